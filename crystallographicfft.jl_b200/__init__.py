@@ -1,0 +1,21 @@
+"""B200-native symmetry-reduced crystallographic FFT (KRFFT) and SCFT diffusion step.
+
+Host-side mirror of CrystallographicFFT.jl's plan/execute API over the C ABI of
+libcfft_b200.so (include/cfft_b200.h).  Importing the package loads the native
+library; there is no CPU fallback.
+"""
+from ._lib import LIB, CFFTError, LIB_PATH  # noqa: F401
+from .symmetry import (  # noqa: F401
+    SymOp, SpectralIndexing, apply_op, auto_L, available_groups, calc_spectral_asu, check_shift_invariance,
+    count_special_positions, detect_centering_type, dual_ops, find_optimal_shift, get_k_vector, get_ops,
+    strip_centering,
+)
+from .plans import (  # noqa: F401
+    DiffusionSolver, KRFFTPlan, PATH_AUTO, PATH_CENTERED, PATH_M2, execute_centered_ikrfft, execute_centered_krfft,
+    execute_centered_scft, execute_krfft, execute_m2_backward, execute_m2_scft, fft_reconstruct,
+    fft_reconstruct_centered, fullgrid_to_subgrid, ifft_unrecon_centered, plan_centered_ikrfft, plan_centered_scft,
+    plan_diffusion, plan_krfft, plan_krfft_centered, plan_m2_backward, plan_m2_scft, step_diffusion,
+    subgrid_to_fullgrid, update_kernel, update_m2_kernel,
+)
+
+__version__ = "0.1.0"

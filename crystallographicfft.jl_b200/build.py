@@ -1,0 +1,74 @@
+"""Build recipe for libcfft_b200.so (sm_100a).
+
+Host C++ (plan layer, space-group table, C ABI) is compiled with g++; the device
+layer with nvcc for sm_100a; the shared library links the CUDA runtime statically
+so it depends only on the driver.  The library is built in-tree next to this file.
+
+    python crystallographicfft.jl_b200/build.py [--force] [--verbose]
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libcfft_b200.so")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CXXFLAGS = ["-O3", "-fPIC", "-std=c++17", "-Wall", "-Wno-unused-function"]
+NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"] + ARCH
+
+HOST_SOURCES = ["spacegroups.cpp", "planner.cpp", "cabi.cpp"]
+DEVICE_SOURCES = ["exec.cu"]
+HEADERS = ["cfft_internal.h", "exec.h"]
+
+
+def _newer(src_paths, target):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(p) > t for p in src_paths)
+
+
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build(force: bool = False, verbose: bool = False, extra_nvflags=None) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "cfft_b200.h")]
+    objs = []
+    for s in HOST_SOURCES:
+        src = os.path.join(CSRC, s)
+        obj = os.path.join(BUILD, s + ".o")
+        if force or _newer([src] + headers, obj):
+            _run(["g++"] + CXXFLAGS + ["-I", INCLUDE, "-I", "/usr/local/cuda/include", "-c", src, "-o", obj], verbose)
+        objs.append(obj)
+    for s in DEVICE_SOURCES:
+        src = os.path.join(CSRC, s)
+        obj = os.path.join(BUILD, s + ".o")
+        if force or _newer([src] + headers, obj):
+            _run([NVCC] + NVFLAGS + list(extra_nvflags or []) + ["-I", INCLUDE, "-c", src, "-o", obj], verbose)
+        objs.append(obj)
+    if force or _newer(objs, LIB):
+        _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static"], verbose)
+    return LIB
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--ptxas-verbose", action="store_true")
+    a = ap.parse_args()
+    extra = ["-Xptxas", "-v"] if a.ptxas_verbose else None
+    print(build(force=a.force or a.ptxas_verbose, verbose=a.verbose, extra_nvflags=extra))
+    sys.exit(0)

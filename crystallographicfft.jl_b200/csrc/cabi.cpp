@@ -1,0 +1,302 @@
+// extern "C" entry points of libcfft_b200 (declared in include/cfft_b200.h).
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/cfft_b200.h"
+#include "exec.h"
+
+using cfft::Status;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+cfft_status ret(Status s, const std::string& msg = std::string()) {
+  if (s != Status::kOk) g_last_error = msg;
+  return static_cast<cfft_status>(static_cast<int>(s));
+}
+
+bool read_ops(int dim, int n_ops, const int32_t* R, const int32_t* t, std::vector<cfft::SymOp>* ops,
+              std::string* err) {
+  if (dim != 2 && dim != 3) { *err = "dim must be 2 or 3"; return false; }
+  if (n_ops < 1 || !R || !t) { *err = "empty or null operation list"; return false; }
+  ops->resize(n_ops);
+  for (int k = 0; k < n_ops; ++k) {
+    cfft::SymOp& op = (*ops)[k];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) op.R[i][j] = R[9 * k + 3 * i + j];
+    for (int i = 0; i < 3; ++i) op.t[i] = t[3 * k + i];
+    for (int d = dim; d < 3; ++d) {
+      op.t[d] = 0;
+      for (int j = 0; j < 3; ++j) op.R[d][j] = op.R[j][d] = (d == j);
+    }
+  }
+  return true;
+}
+
+bool read_N(int dim, const int* N, int* out, std::string* err) {
+  if (!N) { *err = "null grid"; return false; }
+  for (int d = 0; d < 3; ++d) out[d] = d < dim ? N[d] : 1;
+  for (int d = 0; d < dim; ++d)
+    if (out[d] < 1) { *err = "grid edges must be positive"; return false; }
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+cfft_status cfft_get_ops(int sg, int dim, const int* N, int cap, int* n_ops, int32_t* R, int32_t* t) {
+  std::string err;
+  int n[3];
+  if (!n_ops || !read_N(dim, N, n, &err)) return ret(Status::kInvalid, err.empty() ? "null argument" : err);
+  std::vector<cfft::SymOp> ops;
+  Status s = cfft::get_ops(sg, dim, n, &ops, &err);
+  if (s != Status::kOk) return ret(s, err);
+  *n_ops = static_cast<int>(ops.size());
+  if (!R || !t) return CFFT_OK;
+  if (cap < *n_ops) return ret(Status::kInvalid, "capacity too small for the operation list");
+  for (size_t k = 0; k < ops.size(); ++k) {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) R[9 * k + 3 * i + j] = ops[k].R[i][j];
+    for (int i = 0; i < 3; ++i) t[3 * k + i] = ops[k].t[i];
+  }
+  return CFFT_OK;
+}
+
+int cfft_list_groups(int dim, int* out, int cap) { return cfft::list_groups(dim, out, cap); }
+
+cfft_status cfft_find_optimal_shift(int dim, const int* N, int n_ops, const int32_t* R, const int32_t* t,
+                                    double* shift, int32_t* t_shifted) {
+  std::string err;
+  int n[3];
+  std::vector<cfft::SymOp> ops;
+  if (!read_N(dim, N, n, &err) || !read_ops(dim, n_ops, R, t, &ops, &err)) return ret(Status::kInvalid, err);
+  if (!shift || !t_shifted) return ret(Status::kInvalid, "null output");
+  double sh[3];
+  std::vector<cfft::SymOp> out;
+  cfft::find_optimal_shift(ops, n, dim, sh, &out);
+  for (int d = 0; d < dim; ++d) shift[d] = sh[d];
+  for (int k = 0; k < n_ops; ++k)
+    for (int i = 0; i < 3; ++i) t_shifted[3 * k + i] = out[k].t[i];
+  return CFFT_OK;
+}
+
+int cfft_count_special_positions(int dim, const int* N, int n_ops, const int32_t* R, const int32_t* t) {
+  std::string err;
+  int n[3];
+  std::vector<cfft::SymOp> ops;
+  if (!read_N(dim, N, n, &err) || !read_ops(dim, n_ops, R, t, &ops, &err)) { ret(Status::kInvalid, err); return -1; }
+  return cfft::count_special_positions_fast(n, dim, ops);
+}
+
+cfft_status cfft_auto_L(int dim, int n_ops, const int32_t* R, const int32_t* t, int* L) {
+  std::string err;
+  std::vector<cfft::SymOp> ops;
+  if (!read_ops(dim, n_ops, R, t, &ops, &err) || !L) return ret(Status::kInvalid, err.empty() ? "null output" : err);
+  auto l = cfft::auto_L(ops, dim);
+  for (int d = 0; d < 3; ++d) L[d] = l[d];
+  return CFFT_OK;
+}
+
+int cfft_detect_centering(int dim, const int* N, int n_ops, const int32_t* R, const int32_t* t) {
+  std::string err;
+  int n[3];
+  std::vector<cfft::SymOp> ops;
+  if (!read_N(dim, N, n, &err) || !read_ops(dim, n_ops, R, t, &ops, &err)) { ret(Status::kInvalid, err); return -1; }
+  return static_cast<int>(cfft::detect_centering_type(ops, n, dim));
+}
+
+cfft_status cfft_spectral_asu(int dim, const int* N, int n_ops, const int32_t* R, const int32_t* t, int cap,
+                              int* n_spec, int32_t* idx, int32_t* mult) {
+  std::string err;
+  int n[3];
+  std::vector<cfft::SymOp> ops;
+  if (!read_N(dim, N, n, &err) || !read_ops(dim, n_ops, R, t, &ops, &err) || !n_spec)
+    return ret(Status::kInvalid, err.empty() ? "null output" : err);
+  if (static_cast<long>(n[0]) * n[1] * n[2] > (1L << 28)) return ret(Status::kUnsupported, "grid too large");
+  auto pts = cfft::calc_spectral_asu(ops, n, dim);
+  *n_spec = static_cast<int>(pts.size());
+  if (!idx && !mult) return CFFT_OK;
+  if (cap < *n_spec) return ret(Status::kInvalid, "capacity too small for the spectral ASU");
+  for (size_t s = 0; s < pts.size(); ++s) {
+    if (idx)
+      for (int d = 0; d < 3; ++d) idx[3 * s + d] = pts[s].h[d];
+    if (mult) mult[s] = pts[s].mult;
+  }
+  return CFFT_OK;
+}
+
+static cfft_status plan_create_impl(const cfft_desc* desc, cfft_plan* plan, bool device) {
+  if (!desc || !plan) return ret(Status::kInvalid, "null argument");
+  *plan = nullptr;
+  std::string err;
+  int n[3];
+  std::vector<cfft::SymOp> ops;
+  if (!read_N(desc->dim, desc->N, n, &err) || !read_ops(desc->dim, desc->n_ops, desc->R, desc->t, &ops, &err))
+    return ret(Status::kInvalid, err);
+  if (desc->precision != 4 && desc->precision != 8) return ret(Status::kInvalid, "precision must be 4 or 8");
+  if (desc->max_batch < 1) return ret(Status::kInvalid, "max_batch must be positive");
+  if (desc->path < 0 || desc->path > 2) return ret(Status::kInvalid, "unknown path");
+  auto* p = new (std::nothrow) cfft::Plan();
+  if (!p) return ret(Status::kAlloc, "host allocation failed");
+  p->precision = desc->precision;
+  p->max_batch = desc->max_batch;
+  p->ds = desc->ds;
+  std::memcpy(p->lattice, desc->lattice, sizeof(p->lattice));
+  Status s = cfft::build_tables(ops, n, desc->dim, desc->path != CFFT_PATH_M2, &p->T, &err);
+  if (s == Status::kOk && device) s = cfft::plan_device_init(p, &err);
+  if (s == Status::kOk && !device) cfft::compute_kernel(p->T, p->lattice, p->ds, &p->T.K);
+  if (s != Status::kOk) {
+    cfft::plan_device_free(p);
+    delete p;
+    return ret(s, err);
+  }
+  *plan = reinterpret_cast<cfft_plan>(p);
+  return CFFT_OK;
+}
+
+cfft_status cfft_plan_create(const cfft_desc* desc, cfft_plan* plan) { return plan_create_impl(desc, plan, true); }
+cfft_status cfft_plan_create_host(const cfft_desc* desc, cfft_plan* plan) { return plan_create_impl(desc, plan, false); }
+
+cfft_status cfft_plan_destroy(cfft_plan plan) {
+  if (!plan) return CFFT_OK;
+  auto* p = reinterpret_cast<cfft::Plan*>(plan);
+  cfft::plan_device_free(p);
+  delete p;
+  return CFFT_OK;
+}
+
+cfft_status cfft_plan_info(cfft_plan plan, cfft_info* info) {
+  if (!plan || !info) return ret(Status::kInvalid, "null argument");
+  const auto* p = reinterpret_cast<cfft::Plan*>(plan);
+  const auto& T = p->T;
+  for (int d = 0; d < 3; ++d) { info->N[d] = T.N[d]; info->L[d] = T.L[d]; info->M[d] = T.M[d]; info->H[d] = T.H[d]; }
+  info->n_spec = static_cast<int>(T.spec.size());
+  info->n_ops = static_cast<int>(T.ops.size());
+  info->n_rep = T.d;
+  info->centering = static_cast<int>(T.centering);
+  info->centered = T.centered ? 1 : 0;
+  info->n_channels = T.n_ch;
+  info->n_orbits = static_cast<int>(T.orbit_rep.size());
+  info->n_rem_ops = static_cast<int>(T.rem_ops.size());
+  info->precision = p->precision;
+  info->max_batch = p->max_batch;
+  info->P = T.P;
+  info->workspace_bytes = static_cast<int64_t>(p->workspace_bytes);
+  return CFFT_OK;
+}
+
+cfft_status cfft_plan_spectral_asu(cfft_plan plan, int32_t* idx, int32_t* mult) {
+  if (!plan) return ret(Status::kInvalid, "null plan");
+  const auto& T = reinterpret_cast<cfft::Plan*>(plan)->T;
+  for (size_t s = 0; s < T.spec.size(); ++s) {
+    if (idx)
+      for (int d = 0; d < 3; ++d) idx[3 * s + d] = T.spec[s].h[d];
+    if (mult) mult[s] = T.spec[s].mult;
+  }
+  return CFFT_OK;
+}
+
+cfft_status cfft_plan_rep_ops(cfft_plan plan, int32_t* R, int32_t* t) {
+  if (!plan || !R || !t) return ret(Status::kInvalid, "null argument");
+  const auto& T = reinterpret_cast<cfft::Plan*>(plan)->T;
+  for (size_t k = 0; k < T.rep_ops.size(); ++k) {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) R[9 * k + 3 * i + j] = T.rep_ops[k].R[i][j];
+    for (int i = 0; i < 3; ++i) t[3 * k + i] = T.rep_ops[k].t[i];
+  }
+  return CFFT_OK;
+}
+
+cfft_status cfft_plan_backward_tables(cfft_plan plan, int32_t* orbit_rep, int32_t* inv_spec, int32_t* inv_phase) {
+  if (!plan) return ret(Status::kInvalid, "null plan");
+  const auto& T = reinterpret_cast<cfft::Plan*>(plan)->T;
+  if (orbit_rep) std::memcpy(orbit_rep, T.orbit_rep.data(), T.orbit_rep.size() * 4);
+  if (inv_spec) std::memcpy(inv_spec, T.inv_spec.data(), T.inv_spec.size() * 4);
+  if (inv_phase) std::memcpy(inv_phase, T.inv_phase.data(), T.inv_phase.size() * 4);
+  return CFFT_OK;
+}
+
+cfft_status cfft_plan_kernel(cfft_plan plan, double* K) {
+  if (!plan || !K) return ret(Status::kInvalid, "null argument");
+  const auto& T = reinterpret_cast<cfft::Plan*>(plan)->T;
+  std::memcpy(K, T.K.data(), T.K.size() * sizeof(double));
+  return CFFT_OK;
+}
+
+cfft_status cfft_update_kernel(cfft_plan plan, double ds, const double* lattice) {
+  if (!plan) return ret(Status::kInvalid, "null plan");
+  auto* p = reinterpret_cast<cfft::Plan*>(plan);
+  p->ds = ds;
+  if (lattice) std::memcpy(p->lattice, lattice, sizeof(p->lattice));
+  std::string err;
+  if (!p->d_geom) {
+    cfft::compute_kernel(p->T, p->lattice, p->ds, &p->T.K);
+    return CFFT_OK;
+  }
+  return ret(cfft::plan_upload_kernel(p, &err), err);
+}
+
+#define CFFT_EXEC(expr)                                               \
+  do {                                                                \
+    if (!plan) return ret(Status::kInvalid, "null plan");            \
+    auto* p = reinterpret_cast<cfft::Plan*>(plan);                    \
+    if (!p->d_geom) return ret(Status::kInvalid, "plan has no device state (created with cfft_plan_create_host)"); \
+    std::string err;                                                  \
+    Status s_ = (expr);                                               \
+    return ret(s_, err);                                              \
+  } while (0)
+
+cfft_status cfft_forward(cfft_plan plan, const void* f0, void* F, int batch, void* stream) {
+  CFFT_EXEC(cfft::exec_forward(p, f0, F, batch, stream, &err));
+}
+cfft_status cfft_backward(cfft_plan plan, const void* F, void* f0, int batch, void* stream) {
+  CFFT_EXEC(cfft::exec_backward(p, F, f0, batch, stream, &err));
+}
+cfft_status cfft_scft_step(cfft_plan plan, void* f0, int batch, void* stream) {
+  CFFT_EXEC(cfft::exec_scft_step(p, f0, batch, stream, &err));
+}
+cfft_status cfft_step_diffusion(cfft_plan plan, void* q, const void* w, double dt, int n_steps, int batch,
+                                void* stream) {
+  CFFT_EXEC(cfft::exec_step_diffusion(p, q, w, dt, n_steps, batch, stream, &err));
+}
+cfft_status cfft_fullgrid_to_subgrid(cfft_plan plan, const void* u, void* f0, int batch, void* stream) {
+  CFFT_EXEC(cfft::exec_full_to_sub(p, u, f0, batch, stream, &err));
+}
+cfft_status cfft_subgrid_to_fullgrid(cfft_plan plan, const void* f0, void* u, int batch, void* stream) {
+  CFFT_EXEC(cfft::exec_sub_to_full(p, f0, u, batch, stream, &err));
+}
+cfft_status cfft_forward_host(cfft_plan plan, const void* f0_host, void* F_host, int batch) {
+  CFFT_EXEC(cfft::exec_host(p, 0, f0_host, F_host, batch, &err));
+}
+cfft_status cfft_backward_host(cfft_plan plan, const void* F_host, void* f0_host, int batch) {
+  CFFT_EXEC(cfft::exec_host(p, 1, F_host, f0_host, batch, &err));
+}
+cfft_status cfft_scft_step_host(cfft_plan plan, void* f0_host, int batch) {
+  CFFT_EXEC(cfft::exec_host(p, 2, nullptr, f0_host, batch, &err));
+}
+
+const char* cfft_status_string(cfft_status s) {
+  switch (s) {
+    case CFFT_OK: return "ok";
+    case CFFT_ERR_INVALID: return "invalid argument";
+    case CFFT_ERR_CUDA: return "CUDA error";
+    case CFFT_ERR_NOT_COMMENSURATE: return "operation not commensurate with the grid";
+    case CFFT_ERR_UNSUPPORTED: return "unsupported size or group";
+    case CFFT_ERR_TIMEOUT: return "device wait timed out";
+    case CFFT_ERR_ALLOC: return "allocation failed";
+    case CFFT_ERR_NOT_REACHABLE: return "subgrid parity class not reachable";
+  }
+  return "unknown status";
+}
+
+const char* cfft_last_error(void) { return g_last_error.c_str(); }
+
+int cfft_version(void) { return 100; }
+
+int64_t cfft_launch_count(int reset) { return cfft::launch_count(reset != 0); }
+
+}  // extern "C"

@@ -1,0 +1,925 @@
+// Device execution layer of libcfft_b200 (sm_100a).
+//
+// Forward KRFFT per batch of fields (centred fold path; the plain M2 path is the
+// same pipeline with one channel and no fold):
+//   k_plane_fwd   f0 (HBM) -> [fold (WHT8) + twiddle] -> x/y FFT in shared memory
+//                 -> channel workspace   (one CTA per z-plane pair per field)
+//   k_fft_z       z FFT of the channel workspace in place (one CTA per xz-plane)
+//   k_recon       spectral-ASU gather: F(h) = sum_b e^{-2 pi i h.t_b/N} G0(R_b^T h mod M)
+//                 (indices and phases computed on the fly from the representative ops)
+// Backward:
+//   k_inv_recon   G0 at orbit representatives from the aliasing identity
+//                 G0(q) = (1/d) sum_a F(q + M.alpha_a), expanded to the whole orbit
+//                 with G0(R^T q) = e^{2 pi i q.s/M} G0(q)
+//   k_fft_z (inverse), k_plane_bwd (inverse x/y FFT + unfold (inverse WHT / 8) -> f0)
+// The diffusion kernel K multiplies inside k_recon, and e^{-w dt/2} inside the
+// plane kernels, so one SCFT contour step is six launches with no extra passes.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "exec.h"
+
+namespace cfft {
+
+namespace {
+
+thread_local int64_t g_launches = 0;
+
+constexpr int kMaxRem = 192;
+constexpr int kMaxE = 16;  // complex values staged per thread per FFT pass
+
+struct DevGeom {
+  int N[3], M[3], H[3], L[3];
+  int P, d, n_ch, centered;
+  int n_spec, n_orbits, n_rem, n_mask_words;
+  int chan_of_parity[8];
+  int off_idx[8];          // WHT index (o0 + 2 o1 + 4 o2) of each channel
+  int rep_R[8][9];
+  int rep_t[8][3];
+  int rem_R[kMaxRem][9];
+  int rem_s[kMaxRem][3];
+  int nf[3];
+  int radix[3][8];
+  // offsets (in complex elements) into the table buffer
+  int tw_off[3];           // e^{-2 pi i j / H_d}, j < H_d
+  int ftw_off[3];          // e^{-2 pi i j / M_d}, j < H_d  (fold twiddles)
+  int ph_off;              // e^{-2 pi i j / P}, j < P
+};
+
+template <typename T> struct Cx;
+template <> struct Cx<float> { using type = float2; };
+template <> struct Cx<double> { using type = double2; };
+
+template <typename C> __device__ __forceinline__ C mk(decltype(C::x) a, decltype(C::x) b) { C c; c.x = a; c.y = b; return c; }
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return mk<C>(a.x + b.x, a.y + b.y); }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return mk<C>(a.x - b.x, a.y - b.y); }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) { return mk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+template <typename C> __device__ __forceinline__ C cmulc(C a, C b) { return mk<C>(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y); }  // a * conj(b)
+template <typename C> __device__ __forceinline__ C cconj(C a) { return mk<C>(a.x, -a.y); }
+template <typename C> __device__ __forceinline__ C cscale(C a, decltype(C::x) s) { return mk<C>(a.x * s, a.y * s); }
+// multiply by -i (forward) or +i (inverse)
+template <typename C, bool INV> __device__ __forceinline__ C mul_mi(C a) { return INV ? mk<C>(-a.y, a.x) : mk<C>(a.y, -a.x); }
+
+// ---------------------------------------------------------------- small DFTs
+template <typename C, bool INV> __device__ __forceinline__ void dft2(C* v) {
+  C a = v[0], b = v[1];
+  v[0] = cadd(a, b); v[1] = csub(a, b);
+}
+template <typename C, bool INV> __device__ __forceinline__ void dft4(C& x0, C& x1, C& x2, C& x3) {
+  C t0 = cadd(x0, x2), t1 = csub(x0, x2), t2 = cadd(x1, x3), t3 = mul_mi<C, INV>(csub(x1, x3));
+  x0 = cadd(t0, t2); x2 = csub(t0, t2); x1 = cadd(t1, t3); x3 = csub(t1, t3);
+}
+template <typename C, bool INV> __device__ __forceinline__ void dft3(C* v) {
+  using T = decltype(C::x);
+  const T s3 = static_cast<T>(0.86602540378443864676);  // sqrt(3)/2
+  C t = cadd(v[1], v[2]);
+  C u = csub(v[1], v[2]);
+  C m = mk<C>(v[0].x - static_cast<T>(0.5) * t.x, v[0].y - static_cast<T>(0.5) * t.y);
+  C ju = mul_mi<C, INV>(u);  // -i u (forward)
+  v[0] = cadd(v[0], t);
+  v[1] = mk<C>(m.x + s3 * ju.x, m.y + s3 * ju.y);
+  v[2] = mk<C>(m.x - s3 * ju.x, m.y - s3 * ju.y);
+}
+template <typename C, bool INV> __device__ __forceinline__ void dft5(C* v) {
+  using T = decltype(C::x);
+  const T c1 = static_cast<T>(0.30901699437494742410), c2 = static_cast<T>(-0.80901699437494742410);
+  const T s1 = static_cast<T>(0.95105651629515357212), s2 = static_cast<T>(0.58778525229247312917);
+  C a1 = cadd(v[1], v[4]), b1 = csub(v[1], v[4]), a2 = cadd(v[2], v[3]), b2 = csub(v[2], v[3]);
+  C x0 = v[0];
+  C r1 = mk<C>(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
+  C r2 = mk<C>(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
+  C i1 = mul_mi<C, INV>(mk<C>(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y));
+  C i2 = mul_mi<C, INV>(mk<C>(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y));
+  v[0] = cadd(x0, cadd(a1, a2));
+  v[1] = cadd(r1, i1); v[4] = csub(r1, i1);
+  v[2] = cadd(r2, i2); v[3] = csub(r2, i2);
+}
+template <typename C, bool INV> __device__ __forceinline__ void dft8(C* v) {
+  using T = decltype(C::x);
+  const T r = static_cast<T>(0.70710678118654752440);
+  C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  C o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  dft4<C, INV>(e0, e1, e2, e3);
+  dft4<C, INV>(o0, o1, o2, o3);
+  // W8^1 = (1 -/+ i)/sqrt2, W8^2 = -/+ i, W8^3 = (-1 -/+ i)/sqrt2
+  C w1 = INV ? mk<C>(r * (o1.x - o1.y), r * (o1.x + o1.y)) : mk<C>(r * (o1.x + o1.y), r * (o1.y - o1.x));
+  C w2 = mul_mi<C, INV>(o2);
+  C w3 = INV ? mk<C>(-r * (o3.x + o3.y), r * (o3.x - o3.y)) : mk<C>(r * (o3.y - o3.x), -r * (o3.x + o3.y));
+  v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
+  v[1] = cadd(e1, w1); v[5] = csub(e1, w1);
+  v[2] = cadd(e2, w2); v[6] = csub(e2, w2);
+  v[3] = cadd(e3, w3); v[7] = csub(e3, w3);
+}
+template <typename C, bool INV, int R> __device__ __forceinline__ void dftR(C* v) {
+  if constexpr (R == 2) dft2<C, INV>(v);
+  else if constexpr (R == 3) dft3<C, INV>(v);
+  else if constexpr (R == 4) dft4<C, INV>(v[0], v[1], v[2], v[3]);
+  else if constexpr (R == 5) dft5<C, INV>(v);
+  else dft8<C, INV>(v);
+}
+
+// One Stockham autosort pass (radix R, span Ns) over `nlines` lines of length n held
+// in shared memory.  Element i of line l lives at buf[base(l) + i * es] with
+// base(l) = (l / G) * gs + (l % G) * ls.  Every thread stages at most kMaxE/R
+// butterflies, reads them all, synchronises, then writes: the pass is in place.
+template <typename C, bool INV, int R>
+__device__ void stockham_pass(C* buf, int n, int Ns, int nlines, int G, int gs, int ls, int es, const C* tw,
+                              int tid, int nth) {
+  constexpr int MAXB = kMaxE / R;
+  const int nb = n / R;
+  const int total = nb * nlines;
+  C v[MAXB][R];
+#pragma unroll
+  for (int i = 0; i < MAXB; ++i) {
+    const int b = tid + i * nth;
+    if (b < total) {
+      int l, j;
+      if (es == 1) { l = b / nb; j = b - l * nb; } else { j = b / nlines; l = b - j * nlines; }
+      const int base = (l / G) * gs + (l % G) * ls;
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[i][r] = buf[base + (j + r * nb) * es];
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < MAXB; ++i) {
+    const int b = tid + i * nth;
+    if (b < total) {
+      int l, j;
+      if (es == 1) { l = b / nb; j = b - l * nb; } else { j = b / nlines; l = b - j * nlines; }
+      const int base = (l / G) * gs + (l % G) * ls;
+      const int k = j % Ns;
+      const int step = n / (Ns * R);
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        const C w = tw[r * k * step];
+        v[i][r] = INV ? cmulc(v[i][r], w) : cmul(v[i][r], w);
+      }
+      dftR<C, INV, R>(v[i]);
+      const int o = (j / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) buf[base + (o + r * Ns) * es] = v[i][r];
+    }
+  }
+  __syncthreads();
+}
+
+template <typename C, bool INV>
+__device__ void fft_lines(C* buf, int n, int nf, const int* radix, int nlines, int G, int gs, int ls, int es,
+                          const C* tw, int tid, int nth) {
+  int Ns = 1;
+  for (int p = 0; p < nf; ++p) {
+    const int R = radix[p];
+    switch (R) {
+      case 2: stockham_pass<C, INV, 2>(buf, n, Ns, nlines, G, gs, ls, es, tw, tid, nth); break;
+      case 3: stockham_pass<C, INV, 3>(buf, n, Ns, nlines, G, gs, ls, es, tw, tid, nth); break;
+      case 4: stockham_pass<C, INV, 4>(buf, n, Ns, nlines, G, gs, ls, es, tw, tid, nth); break;
+      case 5: stockham_pass<C, INV, 5>(buf, n, Ns, nlines, G, gs, ls, es, tw, tid, nth); break;
+      default: stockham_pass<C, INV, 8>(buf, n, Ns, nlines, G, gs, ls, es, tw, tid, nth); break;
+    }
+    Ns *= R;
+  }
+}
+
+// Walsh-Hadamard transform of 8 values indexed e0 + 2 e1 + 4 e2 (three butterfly stages).
+template <typename T> __device__ __forceinline__ void wht8(T* v) {
+#pragma unroll
+  for (int s = 1; s < 8; s <<= 1)
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      if (!(i & s)) { T a = v[i], b = v[i + s]; v[i] = a + b; v[i + s] = a - b; }
+}
+
+// ---------------------------------------------------------------- plane kernels
+// Forward: build the n_ch channel planes of z-index iz (fold or plain load), x/y FFT,
+// store to the channel workspace W[b][c][iz][y][x].
+template <typename T, bool USE_E>
+__global__ void k_plane_fwd(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                            const T* __restrict__ f0, const T* __restrict__ E, typename Cx<T>::type* __restrict__ W) {
+  using C = typename Cx<T>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int H1 = g->H[0], H2 = g->H[1], H3 = g->H[2];
+  const int M1 = g->M[0], M2 = g->M[1];
+  const int nch = g->n_ch;
+  const int plane = H1 * H2;
+  C* twx = buf + nch * plane;
+  C* twy = twx + H1;
+  const int iz = blockIdx.x, b = blockIdx.y;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  for (int i = tid; i < H1; i += nth) twx[i] = tables[g->tw_off[0] + i];
+  for (int i = tid; i < H2; i += nth) twy[i] = tables[g->tw_off[1] + i];
+  const size_t mvol = static_cast<size_t>(g->M[0]) * g->M[1] * g->M[2];
+  const T* src = f0 + static_cast<size_t>(b) * mvol;
+  const T* Eb = USE_E ? E + static_cast<size_t>(b) * mvol : nullptr;
+  if (!g->centered) {
+    const T* s = src + static_cast<size_t>(iz) * M1 * M2;
+    for (int e = tid; e < plane; e += nth) {
+      T v = s[e];
+      if (USE_E) v *= Eb[static_cast<size_t>(iz) * M1 * M2 + e];
+      buf[e] = mk<C>(v, static_cast<T>(0));
+    }
+  } else {
+    const C* ftx = tables + g->ftw_off[0];
+    const C* fty = tables + g->ftw_off[1];
+    const C ftz = tables[g->ftw_off[2] + iz];
+    for (int e = tid; e < plane; e += nth) {
+      const int ix = e % H1, iy = e / H1;
+      T v[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const size_t idx = (static_cast<size_t>(iz + ((k >> 2) & 1) * H3) * M2 + iy + ((k >> 1) & 1) * H2) * M1 +
+                           ix + (k & 1) * H1;
+        v[k] = src[idx];
+        if (USE_E) v[k] *= Eb[idx];
+      }
+      wht8(v);
+      const C tx = ftx[ix], ty = fty[iy];
+      for (int c = 0; c < nch; ++c) {
+        const int o = g->off_idx[c];
+        C w = mk<C>(static_cast<T>(1), static_cast<T>(0));
+        if (o & 1) w = tx;
+        if (o & 2) w = cmul(w, ty);
+        if (o & 4) w = cmul(w, ftz);
+        buf[c * plane + e] = mk<C>(v[o] * w.x, v[o] * w.y);
+      }
+    }
+  }
+  __syncthreads();
+  // x lines: nch*H2 lines of length H1, contiguous
+  fft_lines<C, false>(buf, H1, g->nf[0], g->radix[0], nch * H2, nch * H2, 0, H1, 1, twx, tid, nth);
+  // y lines: nch*H1 lines of length H2, stride H1
+  fft_lines<C, false>(buf, H2, g->nf[1], g->radix[1], nch * H1, H1, plane, 1, H1, twy, tid, nth);
+  const size_t hvol = static_cast<size_t>(plane) * H3;
+  for (int c = 0; c < nch; ++c) {
+    C* dst = W + (static_cast<size_t>(b) * nch + c) * hvol + static_cast<size_t>(iz) * plane;
+    for (int e = tid; e < plane; e += nth) dst[e] = buf[c * plane + e];
+  }
+}
+
+// Backward: inverse x/y FFT of the n_ch channel planes at z-index iz, then unfold
+// (inverse WHT / 8 after the conjugate twiddle, real part) or take the real part.
+template <typename T, bool USE_E>
+__global__ void k_plane_bwd(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                            const typename Cx<T>::type* __restrict__ W, const T* __restrict__ E, T* __restrict__ f0) {
+  using C = typename Cx<T>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int H1 = g->H[0], H2 = g->H[1], H3 = g->H[2];
+  const int M1 = g->M[0], M2 = g->M[1];
+  const int nch = g->n_ch;
+  const int plane = H1 * H2;
+  C* twx = buf + nch * plane;
+  C* twy = twx + H1;
+  const int iz = blockIdx.x, b = blockIdx.y;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  for (int i = tid; i < H1; i += nth) twx[i] = tables[g->tw_off[0] + i];
+  for (int i = tid; i < H2; i += nth) twy[i] = tables[g->tw_off[1] + i];
+  const size_t hvol = static_cast<size_t>(plane) * H3;
+  for (int c = 0; c < nch; ++c) {
+    const C* s = W + (static_cast<size_t>(b) * nch + c) * hvol + static_cast<size_t>(iz) * plane;
+    for (int e = tid; e < plane; e += nth) buf[c * plane + e] = s[e];
+  }
+  __syncthreads();
+  fft_lines<C, true>(buf, H1, g->nf[0], g->radix[0], nch * H2, nch * H2, 0, H1, 1, twx, tid, nth);
+  fft_lines<C, true>(buf, H2, g->nf[1], g->radix[1], nch * H1, H1, plane, 1, H1, twy, tid, nth);
+  const size_t mvol = static_cast<size_t>(g->M[0]) * g->M[1] * g->M[2];
+  T* dst = f0 + static_cast<size_t>(b) * mvol;
+  const T* Eb = USE_E ? E + static_cast<size_t>(b) * mvol : nullptr;
+  if (!g->centered) {
+    const T scale = static_cast<T>(1.0 / static_cast<double>(mvol));
+    for (int e = tid; e < plane; e += nth) {
+      const size_t idx = static_cast<size_t>(iz) * M1 * M2 + e;
+      T v = buf[e].x * scale;
+      if (USE_E) v *= Eb[idx];
+      dst[idx] = v;
+    }
+  } else {
+    const T scale = static_cast<T>(1.0 / (8.0 * static_cast<double>(hvol)));
+    const C* ftx = tables + g->ftw_off[0];
+    const C* fty = tables + g->ftw_off[1];
+    const C ftz = tables[g->ftw_off[2] + iz];
+    for (int e = tid; e < plane; e += nth) {
+      const int ix = e % H1, iy = e / H1;
+      T v[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v[k] = static_cast<T>(0);
+      const C tx = ftx[ix], ty = fty[iy];
+      for (int c = 0; c < nch; ++c) {
+        const int o = g->off_idx[c];
+        C w = mk<C>(static_cast<T>(1), static_cast<T>(0));
+        if (o & 1) w = tx;
+        if (o & 2) w = cmul(w, ty);
+        if (o & 4) w = cmul(w, ftz);
+        const C x = buf[c * plane + e];
+        v[o] = x.x * w.x + x.y * w.y;  // Re(x * conj(w))
+      }
+      wht8(v);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const size_t idx = (static_cast<size_t>(iz + ((k >> 2) & 1) * H3) * M2 + iy + ((k >> 1) & 1) * H2) * M1 +
+                           ix + (k & 1) * H1;
+        T val = v[k] * scale;
+        if (USE_E) val *= Eb[idx];
+        dst[idx] = val;
+      }
+    }
+  }
+}
+
+// z FFT of the channel workspace: one CTA per (y, channel, field) xz-plane.
+template <typename T, bool INV>
+__global__ void k_fft_z(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                        typename Cx<T>::type* __restrict__ W) {
+  using C = typename Cx<T>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int H1 = g->H[0], H2 = g->H[1], H3 = g->H[2];
+  const int iy = blockIdx.x, c = blockIdx.y, b = blockIdx.z;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  C* twz = buf + H1 * H3;
+  for (int i = tid; i < H3; i += nth) twz[i] = tables[g->tw_off[2] + i];
+  const size_t plane = static_cast<size_t>(H1) * H2;
+  C* base = W + (static_cast<size_t>(b) * g->n_ch + c) * plane * H3 + static_cast<size_t>(iy) * H1;
+  const int tot = H1 * H3;
+  for (int e = tid; e < tot; e += nth) {
+    const int x = e % H1, z = e / H1;
+    buf[e] = base[static_cast<size_t>(z) * plane + x];
+  }
+  __syncthreads();
+  fft_lines<C, INV>(buf, H3, g->nf[2], g->radix[2], H1, H1, 0, 1, H1, twz, tid, nth);
+  for (int e = tid; e < tot; e += nth) {
+    const int x = e % H1, z = e / H1;
+    base[static_cast<size_t>(z) * plane + x] = buf[e];
+  }
+}
+
+// ---------------------------------------------------------------- spectral gathers
+__device__ __forceinline__ int fmod_pos(int a, int n) { int r = a % n; return r < 0 ? r + n : r; }
+
+template <typename T, bool USE_K>
+__global__ void k_recon(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                        const uint32_t* __restrict__ spec_h, const T* __restrict__ K,
+                        const typename Cx<T>::type* __restrict__ W, typename Cx<T>::type* __restrict__ F) {
+  using C = typename Cx<T>::type;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y;
+  if (s >= g->n_spec) return;
+  const uint32_t hp = spec_h[s];
+  const int h[3] = {static_cast<int>(hp & 1023u), static_cast<int>((hp >> 10) & 1023u), static_cast<int>((hp >> 20) & 1023u)};
+  const int H1 = g->H[0], H2 = g->H[1], H3 = g->H[2];
+  const size_t hvol = static_cast<size_t>(H1) * H2 * H3;
+  const C* Wb = W + static_cast<size_t>(b) * g->n_ch * hvol;
+  const C* ph = tables + g->ph_off;
+  const int P = g->P;
+  C acc = mk<C>(static_cast<T>(0), static_cast<T>(0));
+  for (int r = 0; r < g->d; ++r) {
+    int q[3];
+#pragma unroll
+    for (int dd = 0; dd < 3; ++dd) {
+      const int v = g->rep_R[r][0 * 3 + dd] * h[0] + g->rep_R[r][1 * 3 + dd] * h[1] + g->rep_R[r][2 * 3 + dd] * h[2];
+      q[dd] = fmod_pos(v, g->M[dd]);
+    }
+    size_t idx;
+    if (g->centered) {
+      const int c = g->chan_of_parity[(q[0] & 1) + 2 * (q[1] & 1) + 4 * (q[2] & 1)];
+      if (c < 0) continue;
+      idx = static_cast<size_t>(c) * hvol + (static_cast<size_t>(q[2] >> 1) * H2 + (q[1] >> 1)) * H1 + (q[0] >> 1);
+    } else {
+      idx = (static_cast<size_t>(q[2]) * H2 + q[1]) * H1 + q[0];
+    }
+    long long j = 0;
+#pragma unroll
+    for (int dd = 0; dd < 3; ++dd) j += static_cast<long long>(h[dd]) * g->rep_t[r][dd] * (P / g->N[dd]);
+    const int jj = static_cast<int>(((j % P) + P) % P);
+    acc = cadd(acc, cmul(Wb[idx], ph[jj]));
+  }
+  if (USE_K) acc = cscale(acc, K[s]);
+  F[static_cast<size_t>(b) * g->n_spec + s] = acc;
+}
+
+template <typename T>
+__global__ void k_inv_recon(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                            const int32_t* __restrict__ orbit_rep, const int32_t* __restrict__ inv_spec,
+                            const int32_t* __restrict__ inv_phase, const uint32_t* __restrict__ img_mask,
+                            const typename Cx<T>::type* __restrict__ F, typename Cx<T>::type* __restrict__ W) {
+  using C = typename Cx<T>::type;
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = blockIdx.y;
+  if (o >= g->n_orbits) return;
+  const int d = g->d;
+  const C* Fb = F + static_cast<size_t>(b) * g->n_spec;
+  const C* ph = tables + g->ph_off;
+  C acc = mk<C>(static_cast<T>(0), static_cast<T>(0));
+  for (int a = 0; a < d; ++a) {
+    const int s = inv_spec[static_cast<size_t>(o) * d + a];
+    if (s == 0) continue;
+    C f = Fb[(s > 0 ? s : -s) - 1];
+    if (s < 0) f = cconj(f);
+    acc = cadd(acc, cmulc(f, ph[inv_phase[static_cast<size_t>(o) * d + a]]));  // f * e^{+2 pi i j/P}
+  }
+  acc = cscale(acc, static_cast<T>(1.0 / static_cast<double>(d)));
+  const int m = orbit_rep[o];
+  const int M1 = g->M[0], M2 = g->M[1], M3 = g->M[2];
+  const int q[3] = {m % M1, (m / M1) % M2, m / (M1 * M2)};
+  const int H1 = g->H[0], H2 = g->H[1], H3 = g->H[2];
+  const size_t hvol = static_cast<size_t>(H1) * H2 * H3;
+  C* Wb = W + static_cast<size_t>(b) * g->n_ch * hvol;
+  const int P = g->P;
+  const int nw = g->n_mask_words;
+  for (int i = 0; i < g->n_rem; ++i) {
+    if (!((img_mask[static_cast<size_t>(o) * nw + (i >> 5)] >> (i & 31)) & 1u)) continue;
+    int qq[3];
+    long long j = 0;
+#pragma unroll
+    for (int dd = 0; dd < 3; ++dd) {
+      const int v = g->rem_R[i][0 * 3 + dd] * q[0] + g->rem_R[i][1 * 3 + dd] * q[1] + g->rem_R[i][2 * 3 + dd] * q[2];
+      qq[dd] = fmod_pos(v, g->M[dd]);
+      j += static_cast<long long>(q[dd]) * g->rem_s[i][dd] * (P / g->M[dd]);
+    }
+    const int jj = static_cast<int>(((j % P) + P) % P);
+    const C val = cmulc(acc, ph[jj]);  // acc * e^{+2 pi i q.s/M}
+    size_t idx;
+    if (g->centered) {
+      const int c = g->chan_of_parity[(qq[0] & 1) + 2 * (qq[1] & 1) + 4 * (qq[2] & 1)];
+      if (c < 0) continue;  // even-translation images stay in alive classes; guard anyway
+      idx = static_cast<size_t>(c) * hvol + (static_cast<size_t>(qq[2] >> 1) * H2 + (qq[1] >> 1)) * H1 + (qq[0] >> 1);
+    } else {
+      idx = (static_cast<size_t>(qq[2]) * H2 + qq[1]) * H1 + qq[0];
+    }
+    Wb[idx] = val;
+  }
+  (void)M3;
+}
+
+// ---------------------------------------------------------------- elementwise
+template <typename T>
+__global__ void k_interaction(const T* __restrict__ w, T* __restrict__ E, T half_dt, size_t n) {
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n; i += static_cast<size_t>(gridDim.x) * blockDim.x)
+    E[i] = exp(-w[i] * half_dt);
+}
+
+template <typename T>
+__global__ void k_full_to_sub(const T* __restrict__ u, T* __restrict__ f0, int N1, int N2, int L1, int L2, int L3,
+                              int M1, int M2, size_t mvol, size_t nvol, int B) {
+  const size_t tot = mvol * B;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < tot; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const size_t b = i / mvol, r = i % mvol;
+    const size_t x = r % M1, y = (r / M1) % M2, z = r / (static_cast<size_t>(M1) * M2);
+    f0[i] = u[b * nvol + (z * L3 * N2 + y * L2) * N1 + x * L1];
+  }
+}
+
+template <typename T>
+__global__ void k_sub_to_full(const T* __restrict__ f0, const int32_t* __restrict__ fill_map, T* __restrict__ u,
+                              size_t mvol, size_t nvol, int B) {
+  const size_t tot = nvol * B;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < tot; i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const size_t b = i / nvol, r = i % nvol;
+    u[i] = f0[b * mvol + fill_map[r]];
+  }
+}
+
+// ---------------------------------------------------------------- host helpers
+std::string cuda_msg(cudaError_t e, const char* what) {
+  return std::string(what) + ": " + cudaGetErrorString(e);
+}
+
+#define CFFT_CUDA(call, what)                          \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) {                           \
+      *err = cuda_msg(e_, what);                       \
+      return Status::kCuda;                            \
+    }                                                  \
+  } while (0)
+
+bool factor_radices(int n, int* nf, int* radix) {
+  *nf = 0;
+  const int order[5] = {8, 4, 2, 3, 5};
+  for (int r : order)
+    while (n > 1 && n % r == 0) {
+      if (*nf >= 8) return false;
+      radix[(*nf)++] = r;
+      n /= r;
+    }
+  return n == 1;
+}
+
+int round_threads(long elems) {
+  long t = (elems + 14) / 15;
+  t = ((t + 31) / 32) * 32;
+  if (t < 64) t = 64;
+  return static_cast<int>(t);
+}
+
+// Allow the largest dynamic shared memory a CTA may have (227 KB) once per kernel,
+// so plans of different sizes can coexist.
+constexpr int kMaxDynSmem = 227 * 1024;
+template <typename T>
+void set_smem_attrs() {
+  cudaFuncSetAttribute(k_plane_fwd<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_plane_fwd<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_plane_bwd<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_plane_bwd<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_fft_z<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_fft_z<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+}
+
+template <typename T>
+std::vector<unsigned char> make_table_bytes(const Plan& p, DevGeom* g) {
+  using C = typename Cx<T>::type;
+  std::vector<C> tab;
+  auto push = [&](double re, double im) { C c; c.x = static_cast<T>(re); c.y = static_cast<T>(im); tab.push_back(c); };
+  for (int d = 0; d < 3; ++d) {
+    g->tw_off[d] = static_cast<int>(tab.size());
+    const int n = p.T.H[d];
+    for (int j = 0; j < n; ++j) push(std::cos(2.0 * M_PI * j / n), -std::sin(2.0 * M_PI * j / n));
+  }
+  for (int d = 0; d < 3; ++d) {
+    g->ftw_off[d] = static_cast<int>(tab.size());
+    const int m = p.T.M[d];
+    for (int j = 0; j < p.T.H[d]; ++j) push(std::cos(2.0 * M_PI * j / m), -std::sin(2.0 * M_PI * j / m));
+  }
+  g->ph_off = static_cast<int>(tab.size());
+  for (int j = 0; j < p.T.P; ++j) push(std::cos(2.0 * M_PI * j / p.T.P), -std::sin(2.0 * M_PI * j / p.T.P));
+  std::vector<unsigned char> bytes(tab.size() * sizeof(C));
+  std::memcpy(bytes.data(), tab.data(), bytes.size());
+  return bytes;
+}
+
+template <typename T>
+Status launch_forward(Plan* p, const T* f0, typename Cx<T>::type* F, const T* E, bool use_K, int B,
+                      cudaStream_t st, std::string* err) {
+  using C = typename Cx<T>::type;
+  const DevGeom* g = static_cast<const DevGeom*>(p->d_geom);
+  const C* tab = static_cast<const C*>(p->d_tables);
+  C* W = static_cast<C*>(p->d_work_T);
+  const PlanTables& T_ = p->T;
+  if (E)
+    k_plane_fwd<T, true><<<dim3(T_.H[2], B), p->threads_xy, p->smem_xy, st>>>(g, tab, f0, E, W);
+  else
+    k_plane_fwd<T, false><<<dim3(T_.H[2], B), p->threads_xy, p->smem_xy, st>>>(g, tab, f0, nullptr, W);
+  if (T_.H[2] > 1) {
+    k_fft_z<T, false><<<dim3(T_.H[1], T_.n_ch, B), p->threads_z, p->smem_z, st>>>(g, tab, W);
+    ++g_launches;
+  }
+  const int ns = static_cast<int>(T_.spec.size());
+  const dim3 gr((ns + 255) / 256, B);
+  if (use_K)
+    k_recon<T, true><<<gr, 256, 0, st>>>(g, tab, static_cast<const uint32_t*>(p->d_spec_h), static_cast<const T*>(p->d_K), W, F);
+  else
+    k_recon<T, false><<<gr, 256, 0, st>>>(g, tab, static_cast<const uint32_t*>(p->d_spec_h), nullptr, W, F);
+  g_launches += 2;
+  CFFT_CUDA(cudaGetLastError(), "forward launch");
+  return Status::kOk;
+}
+
+template <typename T>
+Status launch_backward(Plan* p, const typename Cx<T>::type* F, T* f0, const T* E, int B, cudaStream_t st,
+                       std::string* err) {
+  using C = typename Cx<T>::type;
+  const DevGeom* g = static_cast<const DevGeom*>(p->d_geom);
+  const C* tab = static_cast<const C*>(p->d_tables);
+  C* W = static_cast<C*>(p->d_work_T);
+  const PlanTables& T_ = p->T;
+  const int no = static_cast<int>(T_.orbit_rep.size());
+  k_inv_recon<T><<<dim3((no + 127) / 128, B), 128, 0, st>>>(
+      g, tab, static_cast<const int32_t*>(p->d_orbit_rep), static_cast<const int32_t*>(p->d_inv_spec),
+      static_cast<const int32_t*>(p->d_inv_phase), static_cast<const uint32_t*>(p->d_img_mask), F, W);
+  if (T_.H[2] > 1) {
+    k_fft_z<T, true><<<dim3(T_.H[1], T_.n_ch, B), p->threads_z, p->smem_z, st>>>(g, tab, W);
+    ++g_launches;
+  }
+  if (E)
+    k_plane_bwd<T, true><<<dim3(T_.H[2], B), p->threads_xy, p->smem_xy, st>>>(g, tab, W, E, f0);
+  else
+    k_plane_bwd<T, false><<<dim3(T_.H[2], B), p->threads_xy, p->smem_xy, st>>>(g, tab, W, nullptr, f0);
+  g_launches += 2;
+  CFFT_CUDA(cudaGetLastError(), "backward launch");
+  return Status::kOk;
+}
+
+Status check_batch(const Plan* p, int B, std::string* err) {
+  if (B < 1 || B > p->max_batch) { *err = "batch must be in [1, max_batch]"; return Status::kInvalid; }
+  return Status::kOk;
+}
+
+}  // namespace
+
+int64_t launch_count(bool reset) {
+  const int64_t v = g_launches;
+  if (reset) g_launches = 0;
+  return v;
+}
+
+Status plan_device_init(Plan* p, std::string* err) {
+  const PlanTables& T = p->T;
+  DevGeom g;
+  std::memset(&g, 0, sizeof(g));
+  for (int d = 0; d < 3; ++d) {
+    g.N[d] = T.N[d]; g.M[d] = T.M[d]; g.H[d] = T.H[d]; g.L[d] = T.L[d];
+    if (!factor_radices(T.H[d], &g.nf[d], g.radix[d])) { *err = "FFT length must factor into 2, 3, 5"; return Status::kUnsupported; }
+  }
+  g.P = T.P; g.d = T.d; g.n_ch = T.n_ch; g.centered = T.centered ? 1 : 0;
+  g.n_spec = static_cast<int>(T.spec.size());
+  g.n_orbits = static_cast<int>(T.orbit_rep.size());
+  g.n_rem = static_cast<int>(T.rem_ops.size());
+  if (g.n_rem > kMaxRem) { *err = "too many even-translation operations"; return Status::kUnsupported; }
+  if (T.d > 8) { *err = "fiber length above 8"; return Status::kUnsupported; }
+  if (T.P > 8192) { *err = "phase denominator lcm(N) above 8192"; return Status::kUnsupported; }
+  p->n_mask_words = (g.n_rem + 31) / 32;
+  g.n_mask_words = p->n_mask_words;
+  for (int k = 0; k < 8; ++k) g.chan_of_parity[k] = T.chan_of_parity[k];
+  for (int c = 0; c < T.n_ch; ++c) g.off_idx[c] = T.offsets[c][0] + 2 * T.offsets[c][1] + 4 * T.offsets[c][2];
+  for (int r = 0; r < T.d; ++r) {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) g.rep_R[r][i * 3 + j] = T.rep_ops[r].R[i][j];
+    for (int i = 0; i < 3; ++i) g.rep_t[r][i] = T.rep_ops[r].t[i];
+  }
+  for (int r = 0; r < g.n_rem; ++r) {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) g.rem_R[r][i * 3 + j] = T.rem_ops[r].R[i][j];
+    for (int i = 0; i < 3; ++i) g.rem_s[r][i] = T.rem_ops[r].t[i];
+  }
+  // distinct-image masks: op i contributes only if no earlier op maps the representative to the same point
+  std::vector<uint32_t> masks(static_cast<size_t>(g.n_orbits) * p->n_mask_words, 0u);
+  for (int o = 0; o < g.n_orbits; ++o) {
+    const int m = T.orbit_rep[o];
+    const int q[3] = {m % T.M[0], (m / T.M[0]) % T.M[1], m / (T.M[0] * T.M[1])};
+    std::vector<long> seen;
+    for (int i = 0; i < g.n_rem; ++i) {
+      long li = 0, stride = 1;
+      for (int dd = 0; dd < 3; ++dd) {
+        long v = 0;
+        for (int d2 = 0; d2 < 3; ++d2) v += static_cast<long>(T.rem_ops[i].R[d2][dd]) * q[d2];
+        li += floor_mod(v, T.M[dd]) * stride;
+        stride *= T.M[dd];
+      }
+      if (std::find(seen.begin(), seen.end(), li) != seen.end()) continue;
+      seen.push_back(li);
+      masks[static_cast<size_t>(o) * p->n_mask_words + (i >> 5)] |= 1u << (i & 31);
+    }
+  }
+  std::vector<uint32_t> hp(T.spec.size());
+  for (size_t s = 0; s < T.spec.size(); ++s)
+    hp[s] = static_cast<uint32_t>(T.spec[s].h[0]) | (static_cast<uint32_t>(T.spec[s].h[1]) << 10) |
+            (static_cast<uint32_t>(T.spec[s].h[2]) << 20);
+  std::vector<unsigned char> tab = p->precision == 8 ? make_table_bytes<double>(*p, &g) : make_table_bytes<float>(*p, &g);
+
+  const size_t rs = p->precision;          // real size
+  const size_t cs = 2 * rs;                // complex size
+  const size_t hvol = static_cast<size_t>(T.H[0]) * T.H[1] * T.H[2];
+  const size_t mvol = static_cast<size_t>(T.M[0]) * T.M[1] * T.M[2];
+  const size_t B = p->max_batch;
+  // launch geometry and shared memory
+  const long pe = static_cast<long>(T.n_ch) * T.H[0] * T.H[1];
+  const long ze = static_cast<long>(T.H[0]) * T.H[2];
+  if (pe > 15 * 1024 || ze > 15 * 1024) { *err = "channel plane too large for one CTA"; return Status::kUnsupported; }
+  p->threads_xy = std::min(1024, round_threads(pe));
+  p->threads_z = std::min(1024, round_threads(ze));
+  p->smem_xy = (pe + T.H[0] + T.H[1]) * cs;
+  p->smem_z = (ze + T.H[2]) * cs;
+  if (p->smem_xy > 227 * 1024 || p->smem_z > 227 * 1024) { *err = "shared memory above 227 KB"; return Status::kUnsupported; }
+
+  auto alloc = [&](void** ptr, size_t bytes, const char* what) -> Status {
+    cudaError_t e = cudaMalloc(ptr, std::max<size_t>(bytes, 16));
+    if (e != cudaSuccess) { *err = cuda_msg(e, what); return Status::kAlloc; }
+    p->workspace_bytes += bytes;
+    return Status::kOk;
+  };
+  Status st;
+  if ((st = alloc(&p->d_geom, sizeof(DevGeom), "geometry")) != Status::kOk) return st;
+  if ((st = alloc(&p->d_tables, tab.size(), "tables")) != Status::kOk) return st;
+  if ((st = alloc(&p->d_spec_h, hp.size() * 4, "spectral points")) != Status::kOk) return st;
+  if ((st = alloc(&p->d_K, T.spec.size() * rs, "kernel")) != Status::kOk) return st;
+  if ((st = alloc(&p->d_orbit_rep, T.orbit_rep.size() * 4, "orbit reps")) != Status::kOk) return st;
+  if ((st = alloc(&p->d_inv_spec, T.inv_spec.size() * 4, "inverse spec")) != Status::kOk) return st;
+  if ((st = alloc(&p->d_inv_phase, T.inv_phase.size() * 4, "inverse phase")) != Status::kOk) return st;
+  if ((st = alloc(&p->d_img_mask, masks.size() * 4, "image masks")) != Status::kOk) return st;
+  if ((st = alloc(&p->d_work_T, B * T.n_ch * hvol * cs, "channel workspace")) != Status::kOk) return st;
+  if ((st = alloc(&p->d_work_F, B * T.spec.size() * cs, "spectrum workspace")) != Status::kOk) return st;
+  if ((st = alloc(&p->d_work_E, B * mvol * rs, "interaction workspace")) != Status::kOk) return st;
+  CFFT_CUDA(cudaMemcpy(p->d_geom, &g, sizeof(g), cudaMemcpyHostToDevice), "upload geometry");
+  CFFT_CUDA(cudaMemcpy(p->d_tables, tab.data(), tab.size(), cudaMemcpyHostToDevice), "upload tables");
+  CFFT_CUDA(cudaMemcpy(p->d_spec_h, hp.data(), hp.size() * 4, cudaMemcpyHostToDevice), "upload spectral points");
+  if (!T.orbit_rep.empty()) {
+    CFFT_CUDA(cudaMemcpy(p->d_orbit_rep, T.orbit_rep.data(), T.orbit_rep.size() * 4, cudaMemcpyHostToDevice), "upload reps");
+    CFFT_CUDA(cudaMemcpy(p->d_inv_spec, T.inv_spec.data(), T.inv_spec.size() * 4, cudaMemcpyHostToDevice), "upload inv spec");
+    CFFT_CUDA(cudaMemcpy(p->d_inv_phase, T.inv_phase.data(), T.inv_phase.size() * 4, cudaMemcpyHostToDevice), "upload inv phase");
+    CFFT_CUDA(cudaMemcpy(p->d_img_mask, masks.data(), masks.size() * 4, cudaMemcpyHostToDevice), "upload masks");
+  }
+  // Orbit expansion writes only alive positions; channel positions never written stay zero.
+  CFFT_CUDA(cudaMemset(p->d_work_T, 0, B * T.n_ch * hvol * cs), "clear workspace");
+  if (p->precision == 8) set_smem_attrs<double>();
+  else set_smem_attrs<float>();
+  CFFT_CUDA(cudaGetLastError(), "set shared-memory attributes");
+  cudaStream_t s;
+  CFFT_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "create stream");
+  p->own_stream = s;
+  return plan_upload_kernel(p, err);
+}
+
+Status plan_upload_kernel(Plan* p, std::string* err) {
+  compute_kernel(p->T, p->lattice, p->ds, &p->T.K);
+  if (p->precision == 8) {
+    CFFT_CUDA(cudaMemcpy(p->d_K, p->T.K.data(), p->T.K.size() * 8, cudaMemcpyHostToDevice), "upload K");
+  } else {
+    std::vector<float> k(p->T.K.begin(), p->T.K.end());
+    CFFT_CUDA(cudaMemcpy(p->d_K, k.data(), k.size() * 4, cudaMemcpyHostToDevice), "upload K");
+  }
+  return Status::kOk;
+}
+
+void plan_device_free(Plan* p) {
+  void** bufs[] = {&p->d_geom, &p->d_tables, &p->d_spec_h, &p->d_K, &p->d_orbit_rep, &p->d_inv_spec,
+                   &p->d_inv_phase, &p->d_img_mask, &p->d_fill_map, &p->d_work_T, &p->d_work_F,
+                   &p->d_work_E, &p->d_stage_in, &p->d_stage_out};
+  for (void** b : bufs)
+    if (*b) { cudaFree(*b); *b = nullptr; }
+  if (p->own_stream) { cudaStreamDestroy(static_cast<cudaStream_t>(p->own_stream)); p->own_stream = nullptr; }
+}
+
+Status exec_forward(Plan* p, const void* f0, void* F, int B, void* stream, std::string* err) {
+  Status st = check_batch(p, B, err);
+  if (st != Status::kOk) return st;
+  if (!f0 || !F) { *err = "null pointer"; return Status::kInvalid; }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (p->precision == 8)
+    return launch_forward<double>(p, static_cast<const double*>(f0), static_cast<double2*>(F), nullptr, false, B, s, err);
+  return launch_forward<float>(p, static_cast<const float*>(f0), static_cast<float2*>(F), nullptr, false, B, s, err);
+}
+
+Status exec_backward(Plan* p, const void* F, void* f0, int B, void* stream, std::string* err) {
+  Status st = check_batch(p, B, err);
+  if (st != Status::kOk) return st;
+  if (!f0 || !F) { *err = "null pointer"; return Status::kInvalid; }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (p->precision == 8)
+    return launch_backward<double>(p, static_cast<const double2*>(F), static_cast<double*>(f0), nullptr, B, s, err);
+  return launch_backward<float>(p, static_cast<const float2*>(F), static_cast<float*>(f0), nullptr, B, s, err);
+}
+
+Status exec_scft_step(Plan* p, void* f0, int B, void* stream, std::string* err) {
+  Status st = check_batch(p, B, err);
+  if (st != Status::kOk) return st;
+  if (!f0) { *err = "null pointer"; return Status::kInvalid; }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (p->precision == 8) {
+    st = launch_forward<double>(p, static_cast<const double*>(f0), static_cast<double2*>(p->d_work_F), nullptr, true, B, s, err);
+    if (st != Status::kOk) return st;
+    return launch_backward<double>(p, static_cast<const double2*>(p->d_work_F), static_cast<double*>(f0), nullptr, B, s, err);
+  }
+  st = launch_forward<float>(p, static_cast<const float*>(f0), static_cast<float2*>(p->d_work_F), nullptr, true, B, s, err);
+  if (st != Status::kOk) return st;
+  return launch_backward<float>(p, static_cast<const float2*>(p->d_work_F), static_cast<float*>(f0), nullptr, B, s, err);
+}
+
+Status exec_step_diffusion(Plan* p, void* q, const void* w, double dt, int n_steps, int B, void* stream,
+                           std::string* err) {
+  Status st = check_batch(p, B, err);
+  if (st != Status::kOk) return st;
+  if (!q || !w || n_steps < 0) { *err = "invalid argument"; return Status::kInvalid; }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t n = static_cast<size_t>(B) * p->T.M[0] * p->T.M[1] * p->T.M[2];
+  const int grid = static_cast<int>(std::min<size_t>((n + 255) / 256, 148 * 16));
+  if (p->precision == 8) {
+    k_interaction<double><<<grid, 256, 0, s>>>(static_cast<const double*>(w), static_cast<double*>(p->d_work_E), dt / 2, n);
+    ++g_launches;
+    for (int i = 0; i < n_steps; ++i) {
+      st = launch_forward<double>(p, static_cast<const double*>(q), static_cast<double2*>(p->d_work_F),
+                                  static_cast<const double*>(p->d_work_E), true, B, s, err);
+      if (st != Status::kOk) return st;
+      st = launch_backward<double>(p, static_cast<const double2*>(p->d_work_F), static_cast<double*>(q),
+                                   static_cast<const double*>(p->d_work_E), B, s, err);
+      if (st != Status::kOk) return st;
+    }
+  } else {
+    k_interaction<float><<<grid, 256, 0, s>>>(static_cast<const float*>(w), static_cast<float*>(p->d_work_E),
+                                              static_cast<float>(dt / 2), n);
+    ++g_launches;
+    for (int i = 0; i < n_steps; ++i) {
+      st = launch_forward<float>(p, static_cast<const float*>(q), static_cast<float2*>(p->d_work_F),
+                                 static_cast<const float*>(p->d_work_E), true, B, s, err);
+      if (st != Status::kOk) return st;
+      st = launch_backward<float>(p, static_cast<const float2*>(p->d_work_F), static_cast<float*>(q),
+                                  static_cast<const float*>(p->d_work_E), B, s, err);
+      if (st != Status::kOk) return st;
+    }
+  }
+  CFFT_CUDA(cudaGetLastError(), "step_diffusion launch");
+  return Status::kOk;
+}
+
+// _build_fill_map (src/q_fused_krfft.jl:733-783): for each grid point the first
+// operation that lands it on the stride-L subgrid.
+static Status ensure_fill_map(Plan* p, std::string* err) {
+  if (p->d_fill_map) return Status::kOk;
+  const PlanTables& T = p->T;
+  const long n1 = T.N[0], n2 = T.N[1], n3 = T.N[2];
+  p->fill_map.assign(n1 * n2 * n3, -1);
+  for (long z = 0; z < n3; ++z)
+    for (long y = 0; y < n2; ++y)
+      for (long x = 0; x < n1; ++x) {
+        const long X[3] = {x, y, z};
+        for (const auto& op : T.ops) {
+          long sub = 0, stride = 1;
+          bool on = true;
+          for (int d = 0; d < 3 && on; ++d) {
+            long v = op.t[d];
+            for (int j = 0; j < 3; ++j) v += static_cast<long>(op.R[d][j]) * X[j];
+            v = floor_mod(v, T.N[d]);
+            if (v % T.L[d] != 0) on = false;
+            sub += (v / T.L[d]) * stride;
+            stride *= T.M[d];
+          }
+          if (on) { p->fill_map[x + n1 * (y + n2 * z)] = static_cast<int32_t>(sub); break; }
+        }
+        if (p->fill_map[x + n1 * (y + n2 * z)] < 0) {
+          *err = "No symmetry operation maps a grid point to the subgrid";
+          return Status::kInvalid;
+        }
+      }
+  CFFT_CUDA(cudaMalloc(&p->d_fill_map, p->fill_map.size() * 4), "alloc fill map");
+  CFFT_CUDA(cudaMemcpy(p->d_fill_map, p->fill_map.data(), p->fill_map.size() * 4, cudaMemcpyHostToDevice), "upload fill map");
+  return Status::kOk;
+}
+
+Status exec_full_to_sub(Plan* p, const void* u, void* f0, int B, void* stream, std::string* err) {
+  Status st = check_batch(p, B, err);
+  if (st != Status::kOk) return st;
+  const PlanTables& T = p->T;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t mvol = static_cast<size_t>(T.M[0]) * T.M[1] * T.M[2];
+  const size_t nvol = static_cast<size_t>(T.N[0]) * T.N[1] * T.N[2];
+  const int grid = static_cast<int>(std::min<size_t>((mvol * B + 255) / 256, 148 * 16));
+  if (p->precision == 8)
+    k_full_to_sub<double><<<grid, 256, 0, s>>>(static_cast<const double*>(u), static_cast<double*>(f0), T.N[0], T.N[1],
+                                               T.L[0], T.L[1], T.L[2], T.M[0], T.M[1], mvol, nvol, B);
+  else
+    k_full_to_sub<float><<<grid, 256, 0, s>>>(static_cast<const float*>(u), static_cast<float*>(f0), T.N[0], T.N[1],
+                                              T.L[0], T.L[1], T.L[2], T.M[0], T.M[1], mvol, nvol, B);
+  ++g_launches;
+  CFFT_CUDA(cudaGetLastError(), "fullgrid_to_subgrid launch");
+  return Status::kOk;
+}
+
+Status exec_sub_to_full(Plan* p, const void* f0, void* u, int B, void* stream, std::string* err) {
+  Status st = check_batch(p, B, err);
+  if (st != Status::kOk) return st;
+  if ((st = ensure_fill_map(p, err)) != Status::kOk) return st;
+  const PlanTables& T = p->T;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t mvol = static_cast<size_t>(T.M[0]) * T.M[1] * T.M[2];
+  const size_t nvol = static_cast<size_t>(T.N[0]) * T.N[1] * T.N[2];
+  const int grid = static_cast<int>(std::min<size_t>((nvol * B + 255) / 256, 148 * 16));
+  if (p->precision == 8)
+    k_sub_to_full<double><<<grid, 256, 0, s>>>(static_cast<const double*>(f0), static_cast<const int32_t*>(p->d_fill_map),
+                                               static_cast<double*>(u), mvol, nvol, B);
+  else
+    k_sub_to_full<float><<<grid, 256, 0, s>>>(static_cast<const float*>(f0), static_cast<const int32_t*>(p->d_fill_map),
+                                              static_cast<float*>(u), mvol, nvol, B);
+  ++g_launches;
+  CFFT_CUDA(cudaGetLastError(), "subgrid_to_fullgrid launch");
+  return Status::kOk;
+}
+
+// which: 0 forward, 1 backward, 2 scft step (in place on the host buffer `out`)
+Status exec_host(Plan* p, int which, const void* in, void* out, int B, std::string* err) {
+  Status st = check_batch(p, B, err);
+  if (st != Status::kOk) return st;
+  const PlanTables& T = p->T;
+  const size_t rs = p->precision, cs = 2 * rs;
+  const size_t fbytes = static_cast<size_t>(B) * T.M[0] * T.M[1] * T.M[2] * rs;
+  const size_t sbytes = static_cast<size_t>(B) * T.spec.size() * cs;
+  const size_t fmax = static_cast<size_t>(p->max_batch) * T.M[0] * T.M[1] * T.M[2] * rs;
+  const size_t smax = static_cast<size_t>(p->max_batch) * T.spec.size() * cs;
+  if (!p->d_stage_in) {
+    CFFT_CUDA(cudaMalloc(&p->d_stage_in, std::max(fmax, smax)), "alloc staging");
+    CFFT_CUDA(cudaMalloc(&p->d_stage_out, std::max(fmax, smax)), "alloc staging");
+    p->workspace_bytes += 2 * std::max(fmax, smax);
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(p->own_stream);
+  if (which == 0) {
+    CFFT_CUDA(cudaMemcpyAsync(p->d_stage_in, in, fbytes, cudaMemcpyHostToDevice, s), "H2D");
+    if ((st = exec_forward(p, p->d_stage_in, p->d_stage_out, B, s, err)) != Status::kOk) return st;
+    CFFT_CUDA(cudaMemcpyAsync(out, p->d_stage_out, sbytes, cudaMemcpyDeviceToHost, s), "D2H");
+  } else if (which == 1) {
+    CFFT_CUDA(cudaMemcpyAsync(p->d_stage_in, in, sbytes, cudaMemcpyHostToDevice, s), "H2D");
+    if ((st = exec_backward(p, p->d_stage_in, p->d_stage_out, B, s, err)) != Status::kOk) return st;
+    CFFT_CUDA(cudaMemcpyAsync(out, p->d_stage_out, fbytes, cudaMemcpyDeviceToHost, s), "D2H");
+  } else {
+    CFFT_CUDA(cudaMemcpyAsync(p->d_stage_in, out, fbytes, cudaMemcpyHostToDevice, s), "H2D");
+    if ((st = exec_scft_step(p, p->d_stage_in, B, s, err)) != Status::kOk) return st;
+    CFFT_CUDA(cudaMemcpyAsync(out, p->d_stage_in, fbytes, cudaMemcpyDeviceToHost, s), "D2H");
+  }
+  CFFT_CUDA(cudaStreamSynchronize(s), "synchronize");
+  return Status::kOk;
+}
+
+}  // namespace cfft

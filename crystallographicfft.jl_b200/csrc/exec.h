@@ -1,0 +1,55 @@
+// Device-side plan object and execution entry points of libcfft_b200.
+#pragma once
+
+#include <string>
+
+#include "cfft_internal.h"
+
+namespace cfft {
+
+struct Plan {
+  PlanTables T;
+  int precision = 4;   // 4 = float, 8 = double
+  int max_batch = 1;
+  double lattice[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  double ds = 0.0;
+  int n_mask_words = 1;
+  std::vector<int32_t> fill_map;  // N-grid -> M-grid linear index (built on first use)
+  // device buffers (owned)
+  void* d_geom = nullptr;       // DevGeom
+  void* d_tables = nullptr;     // twiddles / phases (complex T)
+  void* d_spec_h = nullptr;     // packed h per spectral point
+  void* d_K = nullptr;          // K per spectral point (T)
+  void* d_orbit_rep = nullptr;
+  void* d_inv_spec = nullptr;
+  void* d_inv_phase = nullptr;
+  void* d_img_mask = nullptr;   // distinct-image masks per orbit representative
+  void* d_fill_map = nullptr;
+  void* d_work_T = nullptr;     // B x n_ch x H-grid complex
+  void* d_work_F = nullptr;     // B x n_spec complex
+  void* d_work_E = nullptr;     // B x M-grid real (interaction factors)
+  void* d_stage_in = nullptr;   // host-API staging
+  void* d_stage_out = nullptr;
+  void* own_stream = nullptr;
+  size_t workspace_bytes = 0;
+  // launch geometry
+  int threads_xy = 0, threads_z = 0;
+  size_t smem_xy = 0, smem_z = 0;
+};
+
+Status plan_device_init(Plan* p, std::string* err);
+void plan_device_free(Plan* p);
+Status plan_upload_kernel(Plan* p, std::string* err);
+
+Status exec_forward(Plan* p, const void* f0, void* F, int B, void* stream, std::string* err);
+Status exec_backward(Plan* p, const void* F, void* f0, int B, void* stream, std::string* err);
+Status exec_scft_step(Plan* p, void* f0, int B, void* stream, std::string* err);
+Status exec_step_diffusion(Plan* p, void* q, const void* w, double dt, int n_steps, int B, void* stream,
+                           std::string* err);
+Status exec_full_to_sub(Plan* p, const void* u, void* f0, int B, void* stream, std::string* err);
+Status exec_sub_to_full(Plan* p, const void* f0, void* u, int B, void* stream, std::string* err);
+Status exec_host(Plan* p, int which, const void* in, void* out, int B, std::string* err);
+
+int64_t launch_count(bool reset);
+
+}  // namespace cfft

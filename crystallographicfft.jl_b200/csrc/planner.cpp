@@ -1,0 +1,536 @@
+// Host plan layer: magic shift, spectral ASU, stride-L selection, representative
+// operations, centering detection, backward orbit tables and the diffusion kernel.
+// Each routine follows the reference algorithm cited beside it so that every
+// integer table (spectral-ASU points, multiplicities, L, M, fold offsets) is
+// identical to the reference's.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+#include <set>
+
+#include "cfft_internal.h"
+
+namespace cfft {
+
+long floor_mod(long a, long n) {
+  long r = a % n;
+  return r < 0 ? r + n : r;
+}
+
+static bool is_identity_R(const SymOp& op) {
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      if (op.R[i][j] != (i == j ? 1 : 0)) return false;
+  return true;
+}
+
+// check_shift_invariance (src/symmetry_ops.jl:81-94): delta = (R s - s) .* N must be integral.
+bool check_shift_invariance(const std::vector<SymOp>& ops, const double* shift, const int* N, int dim,
+                            std::vector<std::array<int, 3>>* deltas) {
+  deltas->assign(ops.size(), {0, 0, 0});
+  for (size_t k = 0; k < ops.size(); ++k) {
+    for (int i = 0; i < dim; ++i) {
+      double rs = 0.0;
+      for (int j = 0; j < dim; ++j) rs += ops[k].R[i][j] * shift[j];
+      const double df = (rs - shift[i]) * N[i];
+      const double di = std::nearbyint(df);
+      if (std::fabs(df - di) > 1e-5) return false;
+      (*deltas)[k][i] = static_cast<int>(di);
+    }
+  }
+  return true;
+}
+
+// _count_special_positions_fast (src/asu.jl:372-438): number of orbits shorter than |ops|.
+int count_special_positions_fast(const int* N, int dim, const std::vector<SymOp>& ops) {
+  const int n1 = N[0], n2 = dim > 1 ? N[1] : 1, n3 = dim > 2 ? N[2] : 1;
+  const long total = static_cast<long>(n1) * n2 * n3;
+  std::vector<char> visited(total, 0);
+  std::vector<long> orbit;
+  int sp = 0;
+  const int n[3] = {n1, n2, n3};
+  for (long lin = 0; lin < total; ++lin) {
+    if (visited[lin]) continue;
+    orbit.clear();
+    orbit.push_back(lin);
+    visited[lin] = 1;
+    for (size_t w = 0; w < orbit.size(); ++w) {
+      long rem = orbit[w];
+      int x[3];
+      x[0] = rem % n1; rem /= n1; x[1] = rem % n2; x[2] = rem / n2;
+      for (const auto& op : ops) {
+        long li = 0, stride = 1;
+        for (int d = 0; d < 3; ++d) {
+          long s = (d < dim) ? op.t[d] : 0;
+          for (int j = 0; j < 3; ++j) s += op.R[d][j] * x[j];
+          li += floor_mod(s, n[d]) * stride;
+          stride *= n[d];
+        }
+        if (!visited[li]) { visited[li] = 1; orbit.push_back(li); }
+      }
+    }
+    if (static_cast<long>(orbit.size()) < static_cast<long>(ops.size())) ++sp;
+  }
+  return sp;
+}
+
+static int odd_dims_product(const std::vector<SymOp>& ops, int dim) {
+  int p = 1;
+  for (int d = 0; d < dim; ++d) {
+    bool any = false;
+    for (const auto& op : ops)
+      if (floor_mod(op.t[d], 2) == 1) { any = true; break; }
+    p *= any ? 2 : 1;
+  }
+  return p;
+}
+
+// find_optimal_shift (src/asu.jl:281-347).
+void find_optimal_shift(const std::vector<SymOp>& ops, const int* N, int dim, double* shift_out,
+                        std::vector<SymOp>* shifted) {
+  int Np[3] = {1, 1, 1};
+  for (int d = 0; d < dim; ++d) Np[d] = 12;
+  // _rescale_ops (src/asu.jl:355-363): t_new = t * 12 ÷ N (truncating division)
+  std::vector<SymOp> proxy = ops;
+  for (auto& op : proxy)
+    for (int d = 0; d < dim; ++d) op.t[d] = static_cast<int>((static_cast<long>(op.t[d]) * Np[d]) / N[d]);
+  const double fracs[4] = {0.0, 0.5, 1.0 / 3.0, 0.25};
+  double best_frac = 0.0;
+  int min_sp = INT32_MAX;
+  std::vector<std::array<int, 3>> deltas;
+  for (double frac : fracs) {
+    double s[3] = {0, 0, 0};
+    for (int d = 0; d < dim; ++d) s[d] = frac / Np[d];
+    if (!check_shift_invariance(proxy, s, Np, dim, &deltas)) continue;
+    std::vector<SymOp> cur = proxy;
+    for (size_t k = 0; k < cur.size(); ++k)
+      for (int d = 0; d < dim; ++d) cur[k].t[d] += deltas[k][d];
+    const int sp = count_special_positions_fast(Np, dim, cur);
+    if (sp < min_sp) { min_sp = sp; best_frac = frac; }
+    if (min_sp == 0) break;
+  }
+  double shift[3] = {0, 0, 0};
+  for (int d = 0; d < dim; ++d) shift[d] = best_frac / N[d];
+  std::vector<SymOp> best = ops;
+  if (check_shift_invariance(ops, shift, N, dim, &deltas)) {
+    for (size_t k = 0; k < best.size(); ++k)
+      for (int d = 0; d < dim; ++d) best[k].t[d] += deltas[k][d];
+  } else {
+    for (int d = 0; d < dim; ++d) shift[d] = 0.0;
+  }
+  // Half-grid shift when it raises the number of dimensions with odd translations.
+  double half[3] = {0, 0, 0};
+  for (int d = 0; d < dim; ++d) half[d] = 0.5 / N[d];
+  if (check_shift_invariance(ops, half, N, dim, &deltas)) {
+    std::vector<SymOp> oh = ops;
+    for (size_t k = 0; k < oh.size(); ++k)
+      for (int d = 0; d < dim; ++d) oh[k].t[d] += deltas[k][d];
+    if (odd_dims_product(oh, dim) > odd_dims_product(best, dim)) {
+      for (int d = 0; d < dim; ++d) shift[d] = half[d];
+      best = oh;
+    }
+  }
+  for (int d = 0; d < 3; ++d) shift_out[d] = d < dim ? shift[d] : 0.0;
+  *shifted = best;
+}
+
+// Integer inverse of a unimodular 3x3 matrix.
+static void int_inverse(const int R[3][3], int out[3][3]) {
+  const long det = static_cast<long>(R[0][0]) * (R[1][1] * R[2][2] - R[1][2] * R[2][1]) -
+                   static_cast<long>(R[0][1]) * (R[1][0] * R[2][2] - R[1][2] * R[2][0]) +
+                   static_cast<long>(R[0][2]) * (R[1][0] * R[2][1] - R[1][1] * R[2][0]);
+  int adj[3][3];
+  adj[0][0] = R[1][1] * R[2][2] - R[1][2] * R[2][1];
+  adj[0][1] = R[0][2] * R[2][1] - R[0][1] * R[2][2];
+  adj[0][2] = R[0][1] * R[1][2] - R[0][2] * R[1][1];
+  adj[1][0] = R[1][2] * R[2][0] - R[1][0] * R[2][2];
+  adj[1][1] = R[0][0] * R[2][2] - R[0][2] * R[2][0];
+  adj[1][2] = R[0][2] * R[1][0] - R[0][0] * R[1][2];
+  adj[2][0] = R[1][0] * R[2][1] - R[1][1] * R[2][0];
+  adj[2][1] = R[0][1] * R[2][0] - R[0][0] * R[2][1];
+  adj[2][2] = R[0][0] * R[1][1] - R[0][1] * R[1][0];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) out[i][j] = static_cast<int>(adj[i][j] / det);
+}
+
+// dual_ops (src/symmetry_ops.jl:103-112): R* = (R^-1)^T, t = 0.
+std::vector<SymOp> dual_ops(const std::vector<SymOp>& ops) {
+  std::vector<SymOp> out(ops.size());
+  for (size_t k = 0; k < ops.size(); ++k) {
+    int inv[3][3];
+    int_inverse(ops[k].R, inv);
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) out[k].R[i][j] = inv[j][i];
+    out[k].t[0] = out[k].t[1] = out[k].t[2] = 0;
+  }
+  return out;
+}
+
+// calc_spectral_asu (src/spectral_indexing.jl:22-176): orbit representatives of the
+// dual point group (smallest column-major index), with the stabiliser-phase
+// extinction filter, sorted lexicographically by (h1, h2, h3).
+std::vector<SpecPoint> calc_spectral_asu(const std::vector<SymOp>& ops, const int* N, int dim) {
+  const int n[3] = {N[0], dim > 1 ? N[1] : 1, dim > 2 ? N[2] : 1};
+  const long total = static_cast<long>(n[0]) * n[1] * n[2];
+  const std::vector<SymOp> rec = dual_ops(ops);
+  std::vector<char> visited(total, 0);
+  std::vector<SpecPoint> pts;
+  std::vector<long> work;
+  for (long lin = 0; lin < total; ++lin) {
+    if (visited[lin]) continue;
+    int k[3];
+    long rem = lin;
+    k[0] = rem % n[0]; rem /= n[0]; k[1] = rem % n[1]; k[2] = rem / n[1];
+    visited[lin] = 1;
+    int orbit = 1;
+    long min_lin = lin;
+    work.clear();
+    work.push_back(lin);
+    for (size_t w = 0; w < work.size(); ++w) {
+      long r2 = work[w];
+      int kk[3];
+      kk[0] = r2 % n[0]; r2 /= n[0]; kk[1] = r2 % n[1]; kk[2] = r2 / n[1];
+      for (const auto& op : rec) {
+        long li = 0, stride = 1;
+        for (int d = 0; d < 3; ++d) {
+          long s = 0;
+          for (int j = 0; j < 3; ++j) s += op.R[d][j] * kk[j];
+          li += floor_mod(s, n[d]) * stride;
+          stride *= n[d];
+        }
+        if (!visited[li]) {
+          visited[li] = 1;
+          ++orbit;
+          work.push_back(li);
+          if (li < min_lin) min_lin = li;
+        }
+      }
+    }
+    int kr[3];
+    rem = min_lin;
+    kr[0] = rem % n[0]; rem /= n[0]; kr[1] = rem % n[1]; kr[2] = rem / n[1];
+    // Extinction filter: |sum_{g in Stab(k)} exp(-2 pi i k.t_g / N)| > 1e-5.
+    double sr = 0.0, si = 0.0;
+    for (size_t g = 0; g < rec.size(); ++g) {
+      bool stab = true;
+      for (int d = 0; d < 3 && stab; ++d) {
+        long s = 0;
+        for (int j = 0; j < 3; ++j) s += rec[g].R[d][j] * kr[j];
+        if ((s - kr[d]) % n[d] != 0) stab = false;
+      }
+      if (!stab) continue;
+      double phase = 0.0;
+      for (int d = 0; d < dim; ++d) phase += static_cast<double>(kr[d]) * ops[g].t[d] / n[d];
+      sr += std::cos(2.0 * M_PI * phase);
+      si -= std::sin(2.0 * M_PI * phase);
+    }
+    if (std::hypot(sr, si) > 1e-5) {
+      SpecPoint p;
+      p.h[0] = kr[0]; p.h[1] = kr[1]; p.h[2] = kr[2];
+      p.mult = orbit;
+      pts.push_back(p);
+    }
+  }
+  std::sort(pts.begin(), pts.end(), [](const SpecPoint& a, const SpecPoint& b) {
+    if (a.h[0] != b.h[0]) return a.h[0] < b.h[0];
+    if (a.h[1] != b.h[1]) return a.h[1] < b.h[1];
+    return a.h[2] < b.h[2];
+  });
+  return pts;
+}
+
+// get_k_vector (src/spectral_indexing.jl:195-238): wrap to (-N/2, N/2].
+void get_k_vector(const SpecPoint& p, const int* N, int* k) {
+  for (int d = 0; d < 3; ++d) {
+    const int n = N[d], v = p.h[d];
+    k[d] = (v >= n - n / 2) ? v - n : v;
+  }
+}
+
+// auto_L (src/krfft.jl:225-279).
+std::array<int, 3> auto_L(const std::vector<SymOp>& ops, int dim) {
+  std::array<int, 3> Lmax = {1, 1, 1};
+  for (const auto& op : ops)
+    for (int d = 0; d < dim; ++d)
+      if (floor_mod(op.t[d], 2) == 1) Lmax[d] = 2;
+  const int nsub = Lmax[0] * Lmax[1] * Lmax[2];
+  if (nsub <= 1) return Lmax;
+  auto reach_count = [&](const std::array<int, 3>& L) {
+    std::set<std::array<int, 3>> reach;
+    for (const auto& op : ops)
+      reach.insert({static_cast<int>(floor_mod(op.t[0], L[0])), static_cast<int>(floor_mod(op.t[1], L[1])),
+                    static_cast<int>(floor_mod(op.t[2], L[2]))});
+    return static_cast<int>(reach.size());
+  };
+  if (reach_count(Lmax) == nsub) return Lmax;
+  std::array<int, 3> best = {1, 1, 1};
+  for (int mask = 1; mask < (1 << dim); ++mask) {
+    std::array<int, 3> Lt = {1, 1, 1};
+    for (int d = 0; d < dim; ++d)
+      if (((mask >> d) & 1) && Lmax[d] == 2) Lt[d] = 2;
+    const int ns = Lt[0] * Lt[1] * Lt[2];
+    if (reach_count(Lt) == ns && ns > best[0] * best[1] * best[2]) best = Lt;
+  }
+  return best;
+}
+
+// _select_rep_ops (src/krfft.jl:958-987): one operation per parity class x0 = t mod L,
+// preferring diagonal R with t in {0, N-1}; classes enumerated with x0[0] fastest.
+Status select_rep_ops(const std::vector<SymOp>& ops, const std::array<int, 3>& L, const int* N,
+                      std::vector<SymOp>* rep, std::string* err) {
+  const int d = L[0] * L[1] * L[2];
+  std::vector<int> best(d, -1), quality(d, -1);
+  for (size_t k = 0; k < ops.size(); ++k) {
+    const auto& op = ops[k];
+    const int x0 = static_cast<int>(floor_mod(op.t[0], L[0]) + L[0] * (floor_mod(op.t[1], L[1]) + L[1] * floor_mod(op.t[2], L[2])));
+    bool diag = true;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        if (i != j && op.R[i][j] != 0) diag = false;
+    bool simple = true;
+    for (int dd = 0; dd < 3; ++dd) {
+      const long tm = floor_mod(op.t[dd], N[dd]);
+      if (!(tm == 0 || tm == N[dd] - 1)) simple = false;
+    }
+    const int q = diag ? (simple ? 2 : 1) : 0;
+    if (best[x0] < 0 || q > quality[x0]) { best[x0] = static_cast<int>(k); quality[x0] = q; }
+  }
+  rep->clear();
+  for (int c = 0; c < d; ++c) {
+    if (best[c] < 0) { *err = "subgrid parity class not reachable; auto_L should have prevented this"; return Status::kNotReachable; }
+    rep->push_back(ops[best[c]]);
+  }
+  return Status::kOk;
+}
+
+// detect_centering_type (src/symmetry_ops.jl:133-179).
+Centering detect_centering_type(const std::vector<SymOp>& ops, const int* N, int dim) {
+  bool any = false, xyz = false, x0yz = false, xx0z = false, xy0 = false;
+  for (const auto& op : ops) {
+    if (!is_identity_R(op)) continue;
+    bool zero = true;
+    for (int d = 0; d < dim; ++d)
+      if (op.t[d] != 0) zero = false;
+    if (zero) continue;
+    bool half[3] = {false, false, false};
+    for (int d = 0; d < dim; ++d) half[d] = std::fabs(std::fabs(static_cast<double>(op.t[d])) / N[d] - 0.5) < 0.01;
+    any = true;
+    if (dim < 3) continue;
+    if (half[0] && half[1] && half[2]) xyz = true;
+    if (!half[0] && half[1] && half[2]) x0yz = true;
+    if (half[0] && !half[1] && half[2]) xx0z = true;
+    if (half[0] && half[1] && !half[2]) xy0 = true;
+  }
+  if (!any || dim < 3) return kCentP;
+  if (static_cast<int>(x0yz) + static_cast<int>(xx0z) + static_cast<int>(xy0) >= 2) return kCentF;
+  if (xyz) return kCentI;
+  if (xy0) return kCentC;
+  if (x0yz) return kCentA;
+  if (xx0z) return kCentA;  // B centring is classified as A, as in the reference
+  return kCentP;
+}
+
+// _alive_offsets (src/centering_fold.jl:111-127).
+int alive_offsets(Centering c, std::array<int, 3>* o) {
+  switch (c) {
+    case kCentI: o[0] = {0, 0, 0}; o[1] = {1, 1, 0}; o[2] = {1, 0, 1}; o[3] = {0, 1, 1}; return 4;
+    case kCentF: o[0] = {0, 0, 0}; o[1] = {1, 1, 1}; return 2;
+    case kCentC: o[0] = {0, 0, 0}; o[1] = {1, 1, 0}; o[2] = {0, 0, 1}; o[3] = {1, 1, 1}; return 4;
+    case kCentA: o[0] = {0, 0, 0}; o[1] = {0, 1, 1}; o[2] = {1, 0, 0}; o[3] = {1, 1, 1}; return 4;
+    default: return 0;
+  }
+}
+
+static long lcm_l(long a, long b) { return a / std::gcd(a, b) * b; }
+
+Status build_tables(const std::vector<SymOp>& shifted_ops, const int* N_in, int dim, bool want_centered,
+                    PlanTables* T, std::string* err) {
+  if (shifted_ops.empty()) { *err = "empty operation list"; return Status::kInvalid; }
+  T->dim = dim;
+  for (int d = 0; d < 3; ++d) T->N[d] = d < dim ? N_in[d] : 1;
+  const int* N = T->N;
+  for (int d = 0; d < 3; ++d)
+    if (N[d] < 1 || N[d] > 1024) { *err = "grid edge must be in [1, 1024]"; return Status::kInvalid; }
+  T->ops = shifted_ops;
+  for (auto& op : T->ops)
+    for (int d = dim; d < 3; ++d) {
+      op.t[d] = 0;
+      for (int j = 0; j < 3; ++j) op.R[d][j] = op.R[j][d] = (d == j);
+    }
+  const std::array<int, 3> L = auto_L(T->ops, dim);
+  for (int d = 0; d < 3; ++d) {
+    T->L[d] = L[d];
+    if (N[d] % L[d] != 0) { *err = "Grid size N not divisible by auto L"; return Status::kNotCommensurate; }
+    T->M[d] = N[d] / L[d];
+  }
+  T->d = L[0] * L[1] * L[2];
+  long P = 1;
+  for (int d = 0; d < 3; ++d) P = lcm_l(P, N[d]);
+  if (P > (1 << 20)) { *err = "lcm of grid edges too large"; return Status::kUnsupported; }
+  T->P = static_cast<int>(P);
+  Status st = select_rep_ops(T->ops, L, N, &T->rep_ops, err);
+  if (st != Status::kOk) return st;
+  if (!is_identity_R(T->rep_ops[0]) || T->rep_ops[0].t[0] || T->rep_ops[0].t[1] || T->rep_ops[0].t[2]) {
+    *err = "the identity operation must represent parity class 0";
+    return Status::kInvalid;
+  }
+  T->spec = calc_spectral_asu(T->ops, N, dim);
+  T->centering = detect_centering_type(T->ops, N, dim);
+  // plan_krfft_centered falls back to the plain path for P, L != 2, or odd M
+  // (src/centering_fold.jl:339-352).
+  T->centered = want_centered && T->centering != kCentP && dim == 3 && L[0] == 2 && L[1] == 2 && L[2] == 2 &&
+                T->M[0] % 2 == 0 && T->M[1] % 2 == 0 && T->M[2] % 2 == 0;
+  for (int p = 0; p < 8; ++p) T->chan_of_parity[p] = -1;
+  if (T->centered) {
+    T->n_ch = alive_offsets(T->centering, T->offsets);
+    for (int d = 0; d < 3; ++d) T->H[d] = T->M[d] / 2;
+    for (int c = 0; c < T->n_ch; ++c)
+      T->chan_of_parity[T->offsets[c][0] + 2 * T->offsets[c][1] + 4 * T->offsets[c][2]] = c;
+  } else {
+    T->n_ch = 1;
+    for (int d = 0; d < 3; ++d) T->H[d] = T->M[d];
+    T->offsets[0] = {0, 0, 0};
+  }
+
+  // ---- reverse lookup over the full grid (src/krfft.jl:1183-1255) ----
+  const long n1 = N[0], n2 = N[1], n3 = N[2];
+  const long total = n1 * n2 * n3;
+  std::vector<int32_t> rs(total, 0), rp(total, 0);
+  std::vector<char> rc(total, 0);
+  auto lin = [&](long a, long b, long c) { return a + n1 * (b + n2 * c); };
+  auto phase_num = [&](const int* h, const int* t) {
+    long j = 0;
+    for (int d = 0; d < 3; ++d) j += static_cast<long>(h[d]) * t[d] * (P / N[d]);
+    return static_cast<int32_t>(floor_mod(j, P));
+  };
+  const int nspec = static_cast<int>(T->spec.size());
+  for (int s = 0; s < nspec; ++s) {
+    const int* h = T->spec[s].h;
+    long key = lin(h[0], h[1], h[2]);
+    if (!rs[key]) { rs[key] = s + 1; rp[key] = 0; rc[key] = 0; }
+    for (const auto& op : T->ops) {
+      long hr[3];
+      for (int d = 0; d < 3; ++d) {
+        long v = 0;
+        for (int d2 = 0; d2 < 3; ++d2) v += static_cast<long>(op.R[d2][d]) * h[d2];
+        hr[d] = floor_mod(v, N[d]);
+      }
+      const int32_t ph = phase_num(h, op.t);
+      key = lin(hr[0], hr[1], hr[2]);
+      if (!rs[key]) { rs[key] = s + 1; rp[key] = ph; rc[key] = 0; }
+      key = lin(floor_mod(-hr[0], n1), floor_mod(-hr[1], n2), floor_mod(-hr[2], n3));
+      if (!rs[key]) { rs[key] = s + 1; rp[key] = static_cast<int32_t>(floor_mod(-static_cast<long>(ph), P)); rc[key] = 1; }
+    }
+    key = lin(floor_mod(-h[0], n1), floor_mod(-h[1], n2), floor_mod(-h[2], n3));
+    if (!rs[key]) { rs[key] = s + 1; rp[key] = 0; rc[key] = 1; }
+  }
+
+  // ---- orbit structure on the M-grid under the even-translation subgroup ----
+  // (src/centering_fold.jl:643-687, generalised to any L by s = t / L)
+  T->rem_ops.clear();
+  for (const auto& op : T->ops) {
+    bool ok = true;
+    for (int d = 0; d < 3 && ok; ++d)
+      if (floor_mod(op.t[d], L[d]) != 0) ok = false;
+    SymOp r{};
+    for (int i = 0; i < 3 && ok; ++i)
+      for (int j = 0; j < 3 && ok; ++j) {
+        const long v = static_cast<long>(op.R[i][j]) * L[j];
+        if (v % L[i] != 0) ok = false;
+        r.R[i][j] = static_cast<int>(v / L[i]);
+      }
+    if (!ok) continue;
+    for (int d = 0; d < 3; ++d) r.t[d] = static_cast<int>(floor_mod(op.t[d] / L[d], T->M[d]));
+    T->rem_ops.push_back(r);
+  }
+  const int* M = T->M;
+  const long mtot = static_cast<long>(M[0]) * M[1] * M[2];
+  std::vector<char> seen(mtot, 0);
+  T->orbit_rep.clear();
+  T->inv_spec.clear();
+  T->inv_phase.clear();
+  const int d = T->d;
+  for (long m = 0; m < mtot; ++m) {
+    if (seen[m]) continue;
+    int q[3];
+    long r = m;
+    q[0] = r % M[0]; r /= M[0]; q[1] = r % M[1]; q[2] = r / M[1];
+    const int par = (q[0] & 1) + 2 * (q[1] & 1) + 4 * (q[2] & 1);
+    const bool alive = !T->centered || T->chan_of_parity[par] >= 0;
+    for (const auto& op : T->rem_ops) {
+      long li = 0, stride = 1;
+      for (int dd = 0; dd < 3; ++dd) {
+        long v = 0;
+        for (int d2 = 0; d2 < 3; ++d2) v += static_cast<long>(op.R[d2][dd]) * q[d2];
+        li += floor_mod(v, M[dd]) * stride;
+        stride *= M[dd];
+      }
+      seen[li] = 1;
+    }
+    seen[m] = 1;
+    if (!alive) continue;
+    T->orbit_rep.push_back(static_cast<int32_t>(m));
+    // d aliases h_a = q + M .* alpha_a, alpha enumerated with the first axis fastest.
+    for (int a = 0; a < d; ++a) {
+      int alpha[3];
+      int rem = a;
+      for (int dd = 0; dd < 3; ++dd) { alpha[dd] = rem % L[dd]; rem /= L[dd]; }
+      long hk[3];
+      for (int dd = 0; dd < 3; ++dd) hk[dd] = floor_mod(q[dd] + static_cast<long>(M[dd]) * alpha[dd], N[dd]);
+      const long key = lin(hk[0], hk[1], hk[2]);
+      if (rs[key]) {
+        T->inv_spec.push_back(rc[key] ? -rs[key] : rs[key]);
+        T->inv_phase.push_back(rp[key]);
+      } else {
+        T->inv_spec.push_back(0);
+        T->inv_phase.push_back(0);
+      }
+    }
+  }
+  return Status::kOk;
+}
+
+// K(h) = exp(-ds |2 pi A^-T h_c|^2), h_c = h >= N÷2 ? h - N : h
+// (src/centering_fold.jl:881-891, src/q_fused_krfft.jl:967-974).
+void compute_kernel(const PlanTables& T, const double* lattice, double ds, std::vector<double>* K) {
+  // lattice is column-major 3x3 (lattice vectors in columns), as a Julia Matrix.
+  double A[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) A[i][j] = lattice[i + 3 * j];
+  if (T.dim == 2) {
+    for (int i = 0; i < 3; ++i) { A[i][2] = (i == 2); A[2][i] = (i == 2); }
+  }
+  const double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
+                     A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+                     A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+  double inv[3][3];
+  inv[0][0] = (A[1][1] * A[2][2] - A[1][2] * A[2][1]) / det;
+  inv[0][1] = (A[0][2] * A[2][1] - A[0][1] * A[2][2]) / det;
+  inv[0][2] = (A[0][1] * A[1][2] - A[0][2] * A[1][1]) / det;
+  inv[1][0] = (A[1][2] * A[2][0] - A[1][0] * A[2][2]) / det;
+  inv[1][1] = (A[0][0] * A[2][2] - A[0][2] * A[2][0]) / det;
+  inv[1][2] = (A[0][2] * A[1][0] - A[0][0] * A[1][2]) / det;
+  inv[2][0] = (A[1][0] * A[2][1] - A[1][1] * A[2][0]) / det;
+  inv[2][1] = (A[0][1] * A[2][0] - A[0][0] * A[2][1]) / det;
+  inv[2][2] = (A[0][0] * A[1][1] - A[0][1] * A[1][0]) / det;
+  K->resize(T.spec.size());
+  for (size_t s = 0; s < T.spec.size(); ++s) {
+    double hc[3];
+    for (int d = 0; d < 3; ++d) {
+      const int v = T.spec[s].h[d];
+      hc[d] = (v >= T.N[d] / 2) ? v - T.N[d] : v;
+      if (d >= T.dim) hc[d] = 0.0;
+    }
+    double k2 = 0.0;
+    for (int i = 0; i < 3; ++i) {
+      // recip_B = 2 pi inv(A)^T  =>  k_i = 2 pi sum_j inv[j][i] h_j
+      double k = 0.0;
+      for (int j = 0; j < 3; ++j) k += inv[j][i] * hc[j];
+      k *= 2.0 * M_PI;
+      k2 += k * k;
+    }
+    (*K)[s] = std::exp(-k2 * ds);
+  }
+}
+
+}  // namespace cfft

@@ -1,0 +1,207 @@
+"""Plan-time symmetry and index geometry: the host-side mirror of the reference's
+SymmetryOps / ASU / SpectralIndexing modules (src/symmetry_ops.jl, src/asu.jl,
+src/spectral_indexing.jl) and auto_L (src/krfft.jl:225-279).
+
+The arithmetic runs in libcfft_b200's C++ plan layer; this module only marshals
+arrays.  Operations are integer Seitz pairs in grid units, x' = R x + t (mod N).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from ._lib import LIB, check
+
+CENTERING_NAMES = {0: "P", 1: "C", 2: "A", 3: "I", 4: "F"}
+
+
+@dataclass(frozen=True)
+class SymOp:
+    """SymOp{D} (src/symmetry_ops.jl:17-20)."""
+
+    R: tuple  # row-major D*D
+    t: tuple  # D
+
+    @property
+    def dim(self) -> int:
+        return len(self.t)
+
+    @property
+    def Rm(self) -> np.ndarray:
+        return np.asarray(self.R, dtype=np.int64).reshape(self.dim, self.dim)
+
+    @property
+    def tv(self) -> np.ndarray:
+        return np.asarray(self.t, dtype=np.int64)
+
+
+def _pack(ops):
+    """Pack D-dimensional ops into the C ABI's 3-D slots (R33 = 1, t3 = 0 for D = 2)."""
+    n = len(ops)
+    R = np.zeros((n, 3, 3), dtype=np.int32)
+    t = np.zeros((n, 3), dtype=np.int32)
+    for k, op in enumerate(ops):
+        D = op.dim
+        R[k, :D, :D] = op.Rm
+        for d in range(D, 3):
+            R[k, d, d] = 1
+        t[k, :D] = op.tv
+    return R, t
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def _Nc(N, dim):
+    arr = (ctypes.c_int * 3)(*(list(N) + [1] * (3 - len(N))))
+    return arr
+
+
+def get_ops(sg_num: int, dim: int, N) -> list:
+    """get_ops (src/symmetry_ops.jl:51-53): ITA operations in grid units."""
+    Nc = _Nc(N, dim)
+    n = ctypes.c_int(0)
+    check(LIB.cfft_get_ops(sg_num, dim, Nc, 0, ctypes.byref(n), None, None))
+    R = np.zeros((n.value, 9), dtype=np.int32)
+    t = np.zeros((n.value, 3), dtype=np.int32)
+    check(LIB.cfft_get_ops(sg_num, dim, Nc, n.value, ctypes.byref(n), _ptr(R), _ptr(t)))
+    out = []
+    for k in range(n.value):
+        Rk = R[k].reshape(3, 3)[:dim, :dim]
+        out.append(SymOp(tuple(int(v) for v in Rk.ravel()), tuple(int(v) for v in t[k, :dim])))
+    return out
+
+
+def available_groups(dim: int = 3) -> list:
+    n = LIB.cfft_list_groups(dim, None, 0)
+    buf = (ctypes.c_int * n)()
+    LIB.cfft_list_groups(dim, buf, n)
+    return list(buf)
+
+
+def apply_op(op: SymOp, x, N):
+    """apply_op (src/symmetry_ops.jl:75-78)."""
+    return tuple(int(v) for v in np.mod(op.Rm @ np.asarray(x) + op.tv, np.asarray(N)))
+
+
+def check_shift_invariance(ops, shift, N):
+    """check_shift_invariance (src/symmetry_ops.jl:81-94)."""
+    s = np.asarray(shift, dtype=np.float64)
+    deltas = []
+    for op in ops:
+        df = (op.Rm.astype(np.float64) @ s - s) * np.asarray(N, dtype=np.float64)
+        di = np.rint(df)
+        if not np.all(np.abs(df - di) <= 1e-5):
+            return False, []
+        deltas.append(di.astype(np.int64))
+    return True, deltas
+
+
+def dual_ops(ops):
+    """dual_ops (src/symmetry_ops.jl:103-112)."""
+    out = []
+    for op in ops:
+        Rinv = np.rint(np.linalg.inv(op.Rm.astype(np.float64))).astype(np.int64)
+        out.append(SymOp(tuple(int(v) for v in Rinv.T.ravel()), tuple([0] * op.dim)))
+    return out
+
+
+def find_optimal_shift(ops, N):
+    """find_optimal_shift (src/asu.jl:281-347) -> (shift, shifted_ops)."""
+    dim = ops[0].dim
+    R, t = _pack(ops)
+    shift = np.zeros(3, dtype=np.float64)
+    ts = np.zeros_like(t)
+    check(LIB.cfft_find_optimal_shift(dim, _Nc(N, dim), len(ops), _ptr(R), _ptr(t),
+                                      shift.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), _ptr(ts)))
+    shifted = [SymOp(op.R, tuple(int(v) for v in ts[k, :dim])) for k, op in enumerate(ops)]
+    return shift[:dim], shifted
+
+
+def count_special_positions(N, ops) -> int:
+    """_count_special_positions_fast (src/asu.jl:372-438)."""
+    dim = ops[0].dim
+    R, t = _pack(ops)
+    return int(LIB.cfft_count_special_positions(dim, _Nc(N, dim), len(ops), _ptr(R), _ptr(t)))
+
+
+def auto_L(ops_shifted):
+    """auto_L (src/krfft.jl:225-279)."""
+    dim = ops_shifted[0].dim
+    R, t = _pack(ops_shifted)
+    L = (ctypes.c_int * 3)()
+    check(LIB.cfft_auto_L(dim, len(ops_shifted), _ptr(R), _ptr(t), L))
+    return [int(v) for v in L][:dim]
+
+
+def detect_centering_type(ops, N) -> str:
+    """detect_centering_type (src/symmetry_ops.jl:133-179): 'P', 'C', 'A', 'I' or 'F'."""
+    dim = ops[0].dim
+    R, t = _pack(ops)
+    c = LIB.cfft_detect_centering(dim, _Nc(N, dim), len(ops), _ptr(R), _ptr(t))
+    if c < 0:
+        check(1)
+    return CENTERING_NAMES[c]
+
+
+def strip_centering(ops, centering: str, N):
+    """strip_centering (src/symmetry_ops.jl:192-222)."""
+    D = len(N)
+    if centering in ("I", "F"):
+        halve = [True] * D
+    elif centering == "C":
+        halve = [d < 2 for d in range(D)]
+    elif centering == "A":
+        halve = [d >= 1 for d in range(D)]
+    else:
+        halve = [False] * D
+    Nsub = tuple(N[d] // 2 if halve[d] else N[d] for d in range(D))
+    seen, out = set(), []
+    for op in ops:
+        ts = tuple(int(op.t[d] % Nsub[d]) for d in range(D))
+        if (op.R, ts) not in seen:
+            seen.add((op.R, ts))
+            out.append(SymOp(op.R, ts))
+    return out, Nsub
+
+
+@dataclass
+class SpectralIndexing:
+    """SpectralIndexing (src/spectral_indexing.jl:9-13): sorted orbit representatives."""
+
+    idx: np.ndarray   # (n_spec, D) 0-based frequency indices
+    mult: np.ndarray  # (n_spec,)
+    ops: list         # the direct operations the ASU was built from
+    N: tuple
+
+    @property
+    def n_spec(self) -> int:
+        return int(self.idx.shape[0])
+
+
+def calc_spectral_asu(ops_or_sg, dim: int, N) -> SpectralIndexing:
+    """calc_spectral_asu (src/spectral_indexing.jl:22-176, 184-187)."""
+    ops = get_ops(ops_or_sg, dim, N) if isinstance(ops_or_sg, (int, np.integer)) else list(ops_or_sg)
+    R, t = _pack(ops)
+    n = ctypes.c_int(0)
+    Nc = _Nc(N, dim)
+    check(LIB.cfft_spectral_asu(dim, Nc, len(ops), _ptr(R), _ptr(t), 0, ctypes.byref(n), None, None))
+    idx = np.zeros((n.value, 3), dtype=np.int32)
+    mult = np.zeros(n.value, dtype=np.int32)
+    check(LIB.cfft_spectral_asu(dim, Nc, len(ops), _ptr(R), _ptr(t), n.value, ctypes.byref(n), _ptr(idx), _ptr(mult)))
+    return SpectralIndexing(idx[:, :dim].astype(np.int64), mult.astype(np.int64), ops, tuple(N))
+
+
+def get_k_vector(spec: SpectralIndexing, i: int):
+    """get_k_vector (src/spectral_indexing.jl:195-238) for the 0-based point i:
+    frequencies wrapped to (-N/2, N/2]."""
+    if i < 0 or i >= spec.n_spec:
+        raise IndexError(f"Index {i} out of bounds for SpectralIndexing with {spec.n_spec} points")
+    out = []
+    for d, n in enumerate(spec.N):
+        v = int(spec.idx[i, d])
+        out.append(v - n if v >= n - n // 2 else v)
+    return out

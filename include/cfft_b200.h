@@ -1,0 +1,185 @@
+/*
+ * libcfft_b200 — C ABI of the B200 (sm_100a) symmetry-reduced crystallographic FFT
+ * (KRFFT) and SCFT pseudo-spectral diffusion step.
+ *
+ * The entry points replace the plan/execute surface of CrystallographicFFT.jl for
+ * the hot path; each declaration names the reference function it stands in for
+ * (file:line within the reference project).  A Julia caller binds them with
+ * `ccall`.
+ *
+ * Conventions
+ *  - Grids are column-major, x fastest (Julia Array layout == C [z][y][x]).
+ *  - Real fields are float (precision 4) or double (precision 8); spectra are
+ *    interleaved complex of the same precision, in spectral-ASU order (sorted
+ *    lexicographically by (h1, h2, h3), as calc_spectral_asu returns them).
+ *  - A batch of B fields is B contiguous fields (f0: B * M1*M2*M3 reals,
+ *    spectra: B * n_spec complex).
+ *  - Operations: R is row-major int32[9] (x'_i = sum_j R[3i+j] x_j + t_i), t is
+ *    int32[3] in grid units; a 2-D problem passes dim = 2 and 4-entry R / 2-entry t
+ *    packed into the 3-D slots with R33 = 1, t3 = 0 (N3 = 1).
+ *  - Execute calls take device pointers owned by the caller and a cudaStream_t
+ *    passed as void*; they are stream-ordered and never alias outputs.
+ *  - Plans are not thread-safe (as in the reference); use one plan per stream.
+ *  - Every call returns a cfft_status; cfft_last_error() gives a message.
+ */
+#ifndef CFFT_B200_H
+#define CFFT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum cfft_status {
+  CFFT_OK = 0,
+  CFFT_ERR_INVALID = 1,          /* bad argument / size mismatch */
+  CFFT_ERR_CUDA = 2,             /* CUDA runtime error (message in cfft_last_error) */
+  CFFT_ERR_NOT_COMMENSURATE = 3, /* translation not commensurate with the grid */
+  CFFT_ERR_UNSUPPORTED = 4,      /* size / group outside what the library handles */
+  CFFT_ERR_TIMEOUT = 5,          /* a bounded device wait gave up */
+  CFFT_ERR_ALLOC = 6,            /* device or host allocation failed */
+  CFFT_ERR_NOT_REACHABLE = 7     /* a subgrid parity class has no operation */
+} cfft_status;
+
+typedef enum cfft_path {
+  CFFT_PATH_AUTO = 0,     /* centred fold when applicable, else M2 (plan_krfft_centered) */
+  CFFT_PATH_M2 = 1,       /* plain stride-L path: plan_krfft + plan_m2_backward */
+  CFFT_PATH_CENTERED = 2  /* same as AUTO: plan_krfft_centered falls back to M2 itself */
+} cfft_path;
+
+typedef enum cfft_centering {
+  CFFT_CENT_P = 0, CFFT_CENT_C = 1, CFFT_CENT_A = 2, CFFT_CENT_I = 3, CFFT_CENT_F = 4
+} cfft_centering;
+
+typedef struct cfft_desc {
+  int dim;               /* 2 or 3 */
+  int N[3];              /* full grid (N[2] ignored for dim = 2) */
+  int n_ops;
+  const int32_t* R;      /* n_ops * 9 */
+  const int32_t* t;      /* n_ops * 3, shifted operations (find_optimal_shift) */
+  double lattice[9];     /* lattice vectors in columns, column-major */
+  double ds;             /* Δs of K(h) = exp(-Δs |2π A^-T h|^2) */
+  int precision;         /* 4 (float) or 8 (double) */
+  int max_batch;         /* largest batch any call will pass */
+  int path;              /* cfft_path */
+} cfft_desc;
+
+typedef struct cfft_plan_s* cfft_plan;
+
+typedef struct cfft_info {
+  int N[3], L[3], M[3], H[3];
+  int n_spec;            /* spectral-ASU size */
+  int n_ops;             /* shifted operations held by the plan */
+  int n_rep;             /* prod(L): representative operations (fiber length d) */
+  int centering;         /* cfft_centering */
+  int centered;          /* 1 if the centring fold is used */
+  int n_channels;        /* alive parity channels (1 on the M2 path) */
+  int n_orbits;          /* backward orbit representatives */
+  int n_rem_ops;         /* even-translation operations used for orbit expansion */
+  int precision;
+  int max_batch;
+  int P;                 /* lcm(N): phase denominator */
+  int64_t workspace_bytes;
+} cfft_info;
+
+/* ---------------- plan-time functions (host only, no GPU needed) ---------------- */
+
+/* get_ops(sg, dim, N) (src/symmetry_ops.jl:51-53): operations of space group `sg`
+ * (plane group for dim = 2) in ITA order, converted to grid units like convert_op
+ * (src/symmetry_ops.jl:38-46).  Call with R = t = NULL to query *n_ops. */
+cfft_status cfft_get_ops(int sg, int dim, const int* N, int cap, int* n_ops, int32_t* R, int32_t* t);
+
+/* Space-group numbers the built-in table holds for `dim` (query with out = NULL). */
+int cfft_list_groups(int dim, int* out, int cap);
+
+/* find_optimal_shift(ops, N) (src/asu.jl:281-347): writes the fractional shift
+ * (dim doubles) and the shifted translations (n_ops * 3). */
+cfft_status cfft_find_optimal_shift(int dim, const int* N, int n_ops, const int32_t* R, const int32_t* t,
+                                    double* shift, int32_t* t_shifted);
+
+/* _count_special_positions_fast (src/asu.jl:372-438). */
+int cfft_count_special_positions(int dim, const int* N, int n_ops, const int32_t* R, const int32_t* t);
+
+/* auto_L(ops_shifted) (src/krfft.jl:225-279): writes L[3]. */
+cfft_status cfft_auto_L(int dim, int n_ops, const int32_t* R, const int32_t* t, int* L);
+
+/* detect_centering_type(ops, N) (src/symmetry_ops.jl:133-179): returns cfft_centering. */
+int cfft_detect_centering(int dim, const int* N, int n_ops, const int32_t* R, const int32_t* t);
+
+/* calc_spectral_asu(ops, dim, N) (src/spectral_indexing.jl:22-176): representatives
+ * (n_spec * 3, 0-based) and multiplicities.  Query with idx = mult = NULL. */
+cfft_status cfft_spectral_asu(int dim, const int* N, int n_ops, const int32_t* R, const int32_t* t, int cap,
+                              int* n_spec, int32_t* idx, int32_t* mult);
+
+/* ---------------- plans ---------------- */
+
+/* plan_krfft_centered(spec, ops) / plan_krfft(spec, ops) + plan_m2_backward /
+ * plan_centered_ikrfft / plan_centered_scft / plan_m2_scft
+ * (src/centering_fold.jl:328,630,868; src/krfft.jl:301,1101; src/q_fused_krfft.jl:948):
+ * one plan holds the forward, backward and diffusion-step state for a batch. */
+cfft_status cfft_plan_create(const cfft_desc* desc, cfft_plan* plan);
+/* Same plan-time tables without any device state (no GPU needed); execute calls on
+ * such a plan return CFFT_ERR_INVALID.  For table inspection and host tooling. */
+cfft_status cfft_plan_create_host(const cfft_desc* desc, cfft_plan* plan);
+cfft_status cfft_plan_destroy(cfft_plan plan);
+cfft_status cfft_plan_info(cfft_plan plan, cfft_info* info);
+
+/* Host copies of the plan's integer tables for bit-exact checks:
+ * spectral ASU (n_spec*3 idx, n_spec mult), representative ops (n_rep*9, n_rep*3). */
+cfft_status cfft_plan_spectral_asu(cfft_plan plan, int32_t* idx, int32_t* mult);
+cfft_status cfft_plan_rep_ops(cfft_plan plan, int32_t* R, int32_t* t);
+/* Backward orbit tables: orbit_rep (n_orbits), inv_spec and inv_phase (n_orbits * n_rep). */
+cfft_status cfft_plan_backward_tables(cfft_plan plan, int32_t* orbit_rep, int32_t* inv_spec, int32_t* inv_phase);
+/* K_spec (n_spec doubles) as plan_centered_scft computes it. */
+cfft_status cfft_plan_kernel(cfft_plan plan, double* K);
+
+/* update_kernel! / update_m2_kernel! (src/centering_fold.jl:939-953,
+ * src/q_fused_krfft.jl:1036-1052): recompute K for a new Δs (lattice may be NULL
+ * to keep the plan's). */
+cfft_status cfft_update_kernel(cfft_plan plan, double ds, const double* lattice);
+
+/* ---------------- execution (device pointers, stream-ordered) ---------------- */
+
+/* fft_reconstruct_centered! / fft_reconstruct! (src/centering_fold.jl:421-431,
+ * src/krfft.jl:554-562): f0 (B x M-grid real) -> F (B x n_spec complex). */
+cfft_status cfft_forward(cfft_plan plan, const void* f0, void* F, int batch, void* stream);
+
+/* ifft_unrecon_centered! / execute_m2_backward! (src/centering_fold.jl:745-775,
+ * src/krfft.jl:1269-1277): F -> f0 (real part). */
+cfft_status cfft_backward(cfft_plan plan, const void* F, void* f0, int batch, void* stream);
+
+/* execute_centered_scft! / execute_m2_scft! (src/centering_fold.jl:908-931,
+ * src/q_fused_krfft.jl:989-1026): f0 <- IKRFFT(K . KRFFT(f0)), in place. */
+cfft_status cfft_scft_step(cfft_plan plan, void* f0, int batch, void* stream);
+
+/* step_diffusion! (src/diffusion_solver.jl:254-282) applied n_steps times:
+ * q <- e^{-w dt/2} D(e^{-w dt/2} q), D = the plan's diffusion operator.  w has the
+ * layout of q (B x M-grid). */
+cfft_status cfft_step_diffusion(cfft_plan plan, void* q, const void* w, double dt, int n_steps, int batch,
+                                void* stream);
+
+/* fullgrid_to_subgrid! / subgrid_to_fullgrid! (src/q_fused_krfft.jl:681-719):
+ * u (B x N-grid real) <-> f0 (B x M-grid real). */
+cfft_status cfft_fullgrid_to_subgrid(cfft_plan plan, const void* u, void* f0, int batch, void* stream);
+cfft_status cfft_subgrid_to_fullgrid(cfft_plan plan, const void* f0, void* u, int batch, void* stream);
+
+/* Host-buffer forms of the three execute calls (the reference's execute_*! take
+ * host arrays): copy in, run, copy out on the plan's own stream, then synchronise. */
+cfft_status cfft_forward_host(cfft_plan plan, const void* f0_host, void* F_host, int batch);
+cfft_status cfft_backward_host(cfft_plan plan, const void* F_host, void* f0_host, int batch);
+cfft_status cfft_scft_step_host(cfft_plan plan, void* f0_host, int batch);
+
+/* ---------------- diagnostics ---------------- */
+const char* cfft_status_string(cfft_status s);
+const char* cfft_last_error(void);
+int cfft_version(void);
+/* Number of kernel launches this library issued on this thread since the last reset. */
+int64_t cfft_launch_count(int reset);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CFFT_B200_H */
