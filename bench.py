@@ -1,0 +1,344 @@
+"""Benchmark: symmetry-reduced FFT (KRFFT) forward + backward, Im-3m (No. 229) 128^3
+FP32 with the centring fold, batched fields resident in HBM.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl ours|reference]
+
+One step = one forward + backward KRFFT over B fields (f0 -> spectral ASU -> f0).
+Prints ONE JSON line on rank 0.  Under torchrun each rank runs its own batch
+(fields are independent: replicas / weak scaling); the step time is the max over
+ranks.  `--impl reference` times the FP64 CPU restatement of the reference's
+centred path (fft_reconstruct_centered! + ifft_unrecon_centered!) on a bounded
+sample on this host's cores.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import importlib.util
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG_DIR = os.path.join(ROOT, "crystallographicfft.jl_b200")
+SG, NEDGE = 229, 128
+METRIC = "KRFFT fwd+bwd us per field (Im-3m 128^3 FP32, batched, centring fold)"
+UNIT = "us/field"
+
+
+def load_package():
+    name = "crystallographicfft_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(PKG_DIR, "__init__.py"),
+                                                  submodule_search_locations=[PKG_DIR])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def algorithmic_bytes_per_field(M, n_spec, real_bytes=4):
+    """Forward reads f0 and writes the ASU spectrum; backward does the reverse."""
+    return 2 * (real_bytes * int(np.prod(M)) + 2 * real_bytes * n_spec)
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.samples, self.proc, self.idx = [], None, gpu_index
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": len(self.samples)}
+        rows = [r for r in self.samples if len(r) >= 9]
+        if not rows:
+            return out
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        out["sm_mhz"] = float(np.median(sm)) if sm else None
+        out["sm_max_mhz"] = max(mx) if mx else None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for k, n in enumerate(names):
+                if r[5 + k].lower() == "active":
+                    reasons.add(n)
+        out["reasons"] = sorted(reasons)
+        return out
+
+
+# ----------------------------------------------------------------------------- inputs
+def symmetric_fields(cf, torch, ops_s, N, L, B, seed, device):
+    """B seeded fields symmetric under ops_s (averaged over the group on the GPU),
+    returned as the stride-L subgrid batch (B, M3, M2, M1) in x-fastest layout."""
+    g = torch.Generator(device=device).manual_seed(seed)
+    n1, n2, n3 = N
+    z, y, x = torch.meshgrid(torch.arange(n3, device=device), torch.arange(n2, device=device),
+                             torch.arange(n1, device=device), indexing="ij")
+    X = torch.stack([x.reshape(-1), y.reshape(-1), z.reshape(-1)])  # (3, n) in memory order
+    Nv = torch.tensor(N, device=device).view(3, 1)
+    maps = []
+    for op in ops_s:
+        R, t = op.Rm, op.tv
+        Y = [torch.remainder(sum(int(R[i, j]) * X[j] for j in range(3)) + int(t[i]), int(N[i])) for i in range(3)]
+        maps.append(Y[0] + n1 * (Y[1] + n2 * Y[2]))
+    n_base = 4
+    bases = []
+    for _ in range(n_base):
+        u = torch.randn(n1 * n2 * n3, generator=g, device=device, dtype=torch.float64)
+        s = torch.zeros_like(u)
+        for m in maps:
+            s.index_add_(0, m, u)
+        bases.append((s / len(maps)).view(n3, n2, n1))
+    coef = torch.randn(B, n_base, generator=g, device=device, dtype=torch.float64)
+    sub = torch.stack([b[::L[2], ::L[1], ::L[0]] for b in bases])  # (n_base, M3, M2, M1)
+    return torch.einsum("bk,kzyx->bzyx", coef, sub).contiguous()
+
+
+# ----------------------------------------------------------------------------- reference arm
+def cpu_reference_sample(budget_s=12.0):
+    """FP64 CPU restatement of the reference's centred forward + backward on a bounded
+    sample (Im-3m 128^3), single-threaded numpy/pocketfft like FFTW.set_num_threads(1)."""
+    sys.path.insert(0, ROOT)
+    from oracle import krfft_oracle as O
+
+    cf = load_package()
+    N = (NEDGE,) * 3
+    ops = cf.get_ops(SG, 3, N)
+    _, ops_s = cf.find_optimal_shift(ops, N)
+    oops = [O.SymOp(op.R, op.t) for op in ops_s]
+    spec = O.calc_spectral_asu(oops, 3, N)
+    fwd = O.plan_krfft_centered(spec, oops)
+    bwd = O.plan_centered_ikrfft(spec, oops, fwd)
+    rng = np.random.default_rng(0)
+    M = fwd.krfft.M
+    f0 = rng.standard_normal(M)
+    O.execute_centered_ikrfft(bwd, O.fft_reconstruct_centered(fwd, f0))  # warm-up
+    times, t_end = [], time.perf_counter() + budget_s
+    while time.perf_counter() < t_end or len(times) < 3:
+        t0 = time.perf_counter()
+        F = O.fft_reconstruct_centered(fwd, f0)
+        O.execute_centered_ikrfft(bwd, F)
+        times.append(time.perf_counter() - t0)
+        if len(times) >= 50:
+            break
+    us = float(np.median(times)) * 1e6
+    return {"value": us, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{len(times)} single fields of Im-3m 128^3 FP64 (median), numpy/pocketfft single thread"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cb = cpu_reference_sample(budget_s=min(30.0, 2.0 * max(args.steps, 1)))
+    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": cb["value"] / 1000.0, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference", "config": {"workload": "Im-3m (No. 229) centred KRFFT forward+backward 128^3",
+                                             "group": SG, "N": NEDGE, "sample": cb["sample"]},
+            "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------------------- our arm
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    cf = load_package()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    N = (NEDGE,) * 3
+    ops = cf.get_ops(SG, 3, N)
+    _, ops_s = cf.find_optimal_shift(ops, N)
+    spec = cf.calc_spectral_asu(ops_s, 3, N)
+    B = args.batch
+    plan = cf.KRFFTPlan(spec, ops_s, precision=4, max_batch=B, path=cf.PATH_CENTERED)
+    M = plan.M
+    f0 = symmetric_fields(cf, torch, ops_s, N, plan.L, B, seed=1234 + rank, device=dev).float().contiguous()
+    F = torch.empty((B, plan.n_spec), dtype=torch.complex64, device=dev)
+    out = torch.empty_like(f0)
+    stream = torch.cuda.current_stream()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    lib = cf.LIB
+    h = plan.handle
+
+    def step():
+        lib.cfft_forward(h, ctypes.c_void_p(f0.data_ptr()), ctypes.c_void_p(F.data_ptr()), B, sptr)
+        lib.cfft_backward(h, ctypes.c_void_p(F.data_ptr()), ctypes.c_void_p(out.data_ptr()), B, sptr)
+
+    # correctness guard on the real workload: backward(forward(x)) == x
+    step()
+    torch.cuda.synchronize()
+    rt_err = (torch.max(torch.abs(out - f0)) / torch.max(torch.abs(f0))).item()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    lib.cfft_launch_count(1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    launches = int(lib.cfft_launch_count(1))
+    ms_total = e0.elapsed_time(e1)
+    # per-stage device times (events between launches), averaged over a few round trips
+    stage = np.zeros(6)
+    ms_arr = (ctypes.c_float * 8)()
+    nst = ctypes.c_int(0)
+    reps = 5
+    for _ in range(reps):
+        lib.cfft_profile_roundtrip(h, ctypes.c_void_p(f0.data_ptr()), ctypes.c_void_p(F.data_ptr()),
+                                   ctypes.c_void_p(out.data_ptr()), B, sptr, ms_arr, ctypes.byref(nst))
+        stage += np.array([ms_arr[i] for i in range(6)])
+    stage /= reps
+    clk = clocks.stop()
+    t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = t.item()
+    ms_step = ms_max / args.steps
+    fields_total = B * world
+    us_field = ms_step * 1000.0 / fields_total  # whole-job time per field
+    # e2e through the host-buffer C entry points with pinned host memory
+    e2e = None
+    if rank == 0 or world > 1:
+        f0_h = torch.empty(f0.shape, dtype=torch.float32, pin_memory=True)
+        f0_h.copy_(f0.cpu())
+        F_h = torch.empty((B, plan.n_spec), dtype=torch.complex64, pin_memory=True)
+        out_h = torch.empty_like(f0_h)
+
+        def e2e_step():
+            lib.cfft_forward_host(h, ctypes.c_void_p(f0_h.data_ptr()), ctypes.c_void_p(F_h.data_ptr()), B)
+            lib.cfft_backward_host(h, ctypes.c_void_p(F_h.data_ptr()), ctypes.c_void_p(out_h.data_ptr()), B)
+
+        for _ in range(2):
+            e2e_step()
+        ke = max(3, args.steps // 2)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            e2e_step()
+        e2e_s = (time.perf_counter() - t0) / ke
+        te = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e_us = te.item() * 1e6 / fields_total
+        fb = 4 * int(np.prod(M)) * B
+        sb = 8 * plan.n_spec * B
+        e2e = {"value": e2e_us, "unit": UNIT, "h2d_bytes_per_step": fb + sb, "d2h_bytes_per_step": sb + fb,
+               "note": "cfft_forward_host + cfft_backward_host, pinned host buffers, copies inside the timed region"}
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    alg = algorithmic_bytes_per_field(M, plan.n_spec) * B
+    achieved = alg / (ms_step * 1e-3) / 1e9
+    names = ["plane_fwd (fold+xy FFT)", "fft_z fwd", "recon", "inv_recon+expand", "fft_z inv", "plane_bwd (xy IFFT+unfold)"]
+    top = int(np.argmax(stage))
+    line = {
+        "metric": METRIC, "value": us_field, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"Im-3m (No. 229) centred KRFFT forward+backward, 128^3 FP32, {B} fields per GPU",
+                   "group": SG, "N": NEDGE, "batch_per_gpu": B, "fields_total": fields_total,
+                   "n_spec": plan.n_spec, "M": list(M), "channels": plan.n_channels,
+                   "l2": "inputs larger than L2 (f0 batch %.0f MiB + output %.0f MiB)" % (4 * np.prod(M) * B / 2**20, 4 * np.prod(M) * B / 2**20),
+                   "parallelism": f"replicas x{world}", "roundtrip_rel_err": rt_err},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "peak_source": peak_src, "traffic": None,
+                     "scope": "whole forward+backward (6 launches) per batch; algorithmic bytes 2*(4*M^3 + 8*n_spec) per field",
+                     "stage_ms": {n: float(v) for n, v in zip(names, stage)}, "dominant_stage": names[top]},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "e2e": e2e,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_reference_sample(budget_s=12.0)
+        except Exception as exc:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"error": repr(exc)}
+    traffic_file = os.path.join(ROOT, "profiles", "traffic_im3m128.json")
+    if os.path.exists(traffic_file):
+        try:
+            tr = json.load(open(traffic_file))
+            line["roofline"]["traffic"] = tr.get("bytes_per_field", 0) * B
+            line["roofline"]["traffic_note"] = tr.get("note")
+        except (OSError, ValueError):
+            pass
+    plan.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--batch", type=int, default=128)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

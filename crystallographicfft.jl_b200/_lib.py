@@ -86,6 +86,8 @@ def _load():
         "cfft_forward_host": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
         "cfft_backward_host": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
         "cfft_scft_step_host": (c_int, [c_void_p, c_void_p, c_int]),
+        "cfft_profile_roundtrip": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p,
+                                           ctypes.POINTER(ctypes.c_float), c_int_p]),
         "cfft_status_string": (ctypes.c_char_p, [c_int]),
         "cfft_last_error": (ctypes.c_char_p, []),
         "cfft_version": (c_int, []),

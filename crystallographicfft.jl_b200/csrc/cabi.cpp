@@ -279,6 +279,11 @@ cfft_status cfft_scft_step_host(cfft_plan plan, void* f0_host, int batch) {
   CFFT_EXEC(cfft::exec_host(p, 2, nullptr, f0_host, batch, &err));
 }
 
+cfft_status cfft_profile_roundtrip(cfft_plan plan, const void* f0, void* F, void* f0_out, int batch, void* stream,
+                                   float* stage_ms, int* n_stages) {
+  CFFT_EXEC(cfft::exec_profile_roundtrip(p, f0, F, f0_out, batch, stream, stage_ms, n_stages, &err));
+}
+
 const char* cfft_status_string(cfft_status s) {
   switch (s) {
     case CFFT_OK: return "ok";

@@ -31,7 +31,6 @@ namespace {
 thread_local int64_t g_launches = 0;
 
 constexpr int kMaxRem = 192;
-constexpr int kMaxE = 16;  // complex values staged per thread per FFT pass
 
 struct DevGeom {
   int N[3], M[3], H[3], L[3];
@@ -123,67 +122,56 @@ template <typename C, bool INV, int R> __device__ __forceinline__ void dftR(C* v
   else dft8<C, INV>(v);
 }
 
-// One Stockham autosort pass (radix R, span Ns) over `nlines` lines of length n held
-// in shared memory.  Element i of line l lives at buf[base(l) + i * es] with
-// base(l) = (l / G) * gs + (l % G) * ls.  Every thread stages at most kMaxE/R
-// butterflies, reads them all, synchronises, then writes: the pass is in place.
+// One Stockham autosort pass (radix R, span Ns) over `nlines` lines of length n,
+// out of place between two shared-memory buffers.  Element i of line l lives at
+// base(l) + i * es with base(l) = (l / G) * gs + (l % G) * ls in both buffers.
+// Threads loop over butterflies, so any block size works.
 template <typename C, bool INV, int R>
-__device__ void stockham_pass(C* buf, int n, int Ns, int nlines, int G, int gs, int ls, int es, const C* tw,
-                              int tid, int nth) {
-  constexpr int MAXB = kMaxE / R;
+__device__ __forceinline__ void stockham_pass(const C* __restrict__ src, C* __restrict__ dst, int n, int Ns,
+                                              int nlines, int G, int gs, int ls, int es, const C* tw, int tid,
+                                              int nth) {
   const int nb = n / R;
   const int total = nb * nlines;
-  C v[MAXB][R];
+  const int step = n / (Ns * R);
+  for (int b = tid; b < total; b += nth) {
+    int l, j;
+    if (es == 1) { l = b / nb; j = b - l * nb; } else { j = b / nlines; l = b - j * nlines; }
+    const int base = (l / G) * gs + (l % G) * ls;
+    C v[R];
 #pragma unroll
-  for (int i = 0; i < MAXB; ++i) {
-    const int b = tid + i * nth;
-    if (b < total) {
-      int l, j;
-      if (es == 1) { l = b / nb; j = b - l * nb; } else { j = b / nlines; l = b - j * nlines; }
-      const int base = (l / G) * gs + (l % G) * ls;
+    for (int r = 0; r < R; ++r) v[r] = src[base + (j + r * nb) * es];
+    const int k = j % Ns;
 #pragma unroll
-      for (int r = 0; r < R; ++r) v[i][r] = buf[base + (j + r * nb) * es];
+    for (int r = 1; r < R; ++r) {
+      const C w = tw[r * k * step];
+      v[r] = INV ? cmulc(v[r], w) : cmul(v[r], w);
     }
-  }
-  __syncthreads();
+    dftR<C, INV, R>(v);
+    const int o = (j / Ns) * Ns * R + k;
 #pragma unroll
-  for (int i = 0; i < MAXB; ++i) {
-    const int b = tid + i * nth;
-    if (b < total) {
-      int l, j;
-      if (es == 1) { l = b / nb; j = b - l * nb; } else { j = b / nlines; l = b - j * nlines; }
-      const int base = (l / G) * gs + (l % G) * ls;
-      const int k = j % Ns;
-      const int step = n / (Ns * R);
-#pragma unroll
-      for (int r = 1; r < R; ++r) {
-        const C w = tw[r * k * step];
-        v[i][r] = INV ? cmulc(v[i][r], w) : cmul(v[i][r], w);
-      }
-      dftR<C, INV, R>(v[i]);
-      const int o = (j / Ns) * Ns * R + k;
-#pragma unroll
-      for (int r = 0; r < R; ++r) buf[base + (o + r * Ns) * es] = v[i][r];
-    }
+    for (int r = 0; r < R; ++r) dst[base + (o + r * Ns) * es] = v[r];
   }
   __syncthreads();
 }
 
+// Runs all passes; returns the buffer (a or b) that holds the result.
 template <typename C, bool INV>
-__device__ void fft_lines(C* buf, int n, int nf, const int* radix, int nlines, int G, int gs, int ls, int es,
-                          const C* tw, int tid, int nth) {
+__device__ C* fft_lines(C* a, C* b, int n, int nf, const int* radix, int nlines, int G, int gs, int ls, int es,
+                        const C* tw, int tid, int nth) {
   int Ns = 1;
   for (int p = 0; p < nf; ++p) {
     const int R = radix[p];
     switch (R) {
-      case 2: stockham_pass<C, INV, 2>(buf, n, Ns, nlines, G, gs, ls, es, tw, tid, nth); break;
-      case 3: stockham_pass<C, INV, 3>(buf, n, Ns, nlines, G, gs, ls, es, tw, tid, nth); break;
-      case 4: stockham_pass<C, INV, 4>(buf, n, Ns, nlines, G, gs, ls, es, tw, tid, nth); break;
-      case 5: stockham_pass<C, INV, 5>(buf, n, Ns, nlines, G, gs, ls, es, tw, tid, nth); break;
-      default: stockham_pass<C, INV, 8>(buf, n, Ns, nlines, G, gs, ls, es, tw, tid, nth); break;
+      case 2: stockham_pass<C, INV, 2>(a, b, n, Ns, nlines, G, gs, ls, es, tw, tid, nth); break;
+      case 3: stockham_pass<C, INV, 3>(a, b, n, Ns, nlines, G, gs, ls, es, tw, tid, nth); break;
+      case 4: stockham_pass<C, INV, 4>(a, b, n, Ns, nlines, G, gs, ls, es, tw, tid, nth); break;
+      case 5: stockham_pass<C, INV, 5>(a, b, n, Ns, nlines, G, gs, ls, es, tw, tid, nth); break;
+      default: stockham_pass<C, INV, 8>(a, b, n, Ns, nlines, G, gs, ls, es, tw, tid, nth); break;
     }
+    C* t = a; a = b; b = t;
     Ns *= R;
   }
+  return a;
 }
 
 // Walsh-Hadamard transform of 8 values indexed e0 + 2 e1 + 4 e2 (three butterfly stages).
@@ -208,7 +196,8 @@ __global__ void k_plane_fwd(const DevGeom* __restrict__ g, const typename Cx<T>:
   const int M1 = g->M[0], M2 = g->M[1];
   const int nch = g->n_ch;
   const int plane = H1 * H2;
-  C* twx = buf + nch * plane;
+  C* tmp = buf + nch * plane;
+  C* twx = tmp + nch * plane;
   C* twy = twx + H1;
   const int iz = blockIdx.x, b = blockIdx.y;
   const int tid = threadIdx.x, nth = blockDim.x;
@@ -252,13 +241,14 @@ __global__ void k_plane_fwd(const DevGeom* __restrict__ g, const typename Cx<T>:
   }
   __syncthreads();
   // x lines: nch*H2 lines of length H1, contiguous
-  fft_lines<C, false>(buf, H1, g->nf[0], g->radix[0], nch * H2, nch * H2, 0, H1, 1, twx, tid, nth);
+  C* r1 = fft_lines<C, false>(buf, tmp, H1, g->nf[0], g->radix[0], nch * H2, nch * H2, 0, H1, 1, twx, tid, nth);
   // y lines: nch*H1 lines of length H2, stride H1
-  fft_lines<C, false>(buf, H2, g->nf[1], g->radix[1], nch * H1, H1, plane, 1, H1, twy, tid, nth);
+  C* r2 = fft_lines<C, false>(r1, r1 == buf ? tmp : buf, H2, g->nf[1], g->radix[1], nch * H1, H1, plane, 1, H1,
+                              twy, tid, nth);
   const size_t hvol = static_cast<size_t>(plane) * H3;
   for (int c = 0; c < nch; ++c) {
     C* dst = W + (static_cast<size_t>(b) * nch + c) * hvol + static_cast<size_t>(iz) * plane;
-    for (int e = tid; e < plane; e += nth) dst[e] = buf[c * plane + e];
+    for (int e = tid; e < plane; e += nth) dst[e] = r2[c * plane + e];
   }
 }
 
@@ -274,7 +264,8 @@ __global__ void k_plane_bwd(const DevGeom* __restrict__ g, const typename Cx<T>:
   const int M1 = g->M[0], M2 = g->M[1];
   const int nch = g->n_ch;
   const int plane = H1 * H2;
-  C* twx = buf + nch * plane;
+  C* tmp = buf + nch * plane;
+  C* twx = tmp + nch * plane;
   C* twy = twx + H1;
   const int iz = blockIdx.x, b = blockIdx.y;
   const int tid = threadIdx.x, nth = blockDim.x;
@@ -286,8 +277,9 @@ __global__ void k_plane_bwd(const DevGeom* __restrict__ g, const typename Cx<T>:
     for (int e = tid; e < plane; e += nth) buf[c * plane + e] = s[e];
   }
   __syncthreads();
-  fft_lines<C, true>(buf, H1, g->nf[0], g->radix[0], nch * H2, nch * H2, 0, H1, 1, twx, tid, nth);
-  fft_lines<C, true>(buf, H2, g->nf[1], g->radix[1], nch * H1, H1, plane, 1, H1, twy, tid, nth);
+  C* r1 = fft_lines<C, true>(buf, tmp, H1, g->nf[0], g->radix[0], nch * H2, nch * H2, 0, H1, 1, twx, tid, nth);
+  buf = fft_lines<C, true>(r1, r1 == buf ? tmp : buf, H2, g->nf[1], g->radix[1], nch * H1, H1, plane, 1, H1, twy,
+                           tid, nth);
   const size_t mvol = static_cast<size_t>(g->M[0]) * g->M[1] * g->M[2];
   T* dst = f0 + static_cast<size_t>(b) * mvol;
   const T* Eb = USE_E ? E + static_cast<size_t>(b) * mvol : nullptr;
@@ -342,7 +334,8 @@ __global__ void k_fft_z(const DevGeom* __restrict__ g, const typename Cx<T>::typ
   const int H1 = g->H[0], H2 = g->H[1], H3 = g->H[2];
   const int iy = blockIdx.x, c = blockIdx.y, b = blockIdx.z;
   const int tid = threadIdx.x, nth = blockDim.x;
-  C* twz = buf + H1 * H3;
+  C* tmp = buf + H1 * H3;
+  C* twz = tmp + H1 * H3;
   for (int i = tid; i < H3; i += nth) twz[i] = tables[g->tw_off[2] + i];
   const size_t plane = static_cast<size_t>(H1) * H2;
   C* base = W + (static_cast<size_t>(b) * g->n_ch + c) * plane * H3 + static_cast<size_t>(iy) * H1;
@@ -352,10 +345,10 @@ __global__ void k_fft_z(const DevGeom* __restrict__ g, const typename Cx<T>::typ
     buf[e] = base[static_cast<size_t>(z) * plane + x];
   }
   __syncthreads();
-  fft_lines<C, INV>(buf, H3, g->nf[2], g->radix[2], H1, H1, 0, 1, H1, twz, tid, nth);
+  const C* res = fft_lines<C, INV>(buf, tmp, H3, g->nf[2], g->radix[2], H1, H1, 0, 1, H1, twz, tid, nth);
   for (int e = tid; e < tot; e += nth) {
     const int x = e % H1, z = e / H1;
-    base[static_cast<size_t>(z) * plane + x] = buf[e];
+    base[static_cast<size_t>(z) * plane + x] = res[e];
   }
 }
 
@@ -511,11 +504,11 @@ bool factor_radices(int n, int* nf, int* radix) {
   return n == 1;
 }
 
+// One thread per four elements, in whole warps, 64 to 512 threads per CTA.
 int round_threads(long elems) {
-  long t = (elems + 14) / 15;
+  long t = (elems + 3) / 4;
   t = ((t + 31) / 32) * 32;
-  if (t < 64) t = 64;
-  return static_cast<int>(t);
+  return static_cast<int>(std::max(64L, std::min(512L, t)));
 }
 
 // Allow the largest dynamic shared memory a CTA may have (227 KB) once per kernel,
@@ -553,29 +546,57 @@ std::vector<unsigned char> make_table_bytes(const Plan& p, DevGeom* g) {
   return bytes;
 }
 
+// Stages of one forward + backward: 0 plane/fold + x/y FFT, 1 z FFT, 2 reconstruct,
+// 3 inverse reconstruct + orbit expansion, 4 inverse z FFT, 5 inverse x/y FFT + unfold.
 template <typename T>
-Status launch_forward(Plan* p, const T* f0, typename Cx<T>::type* F, const T* E, bool use_K, int B,
-                      cudaStream_t st, std::string* err) {
+void launch_stage(Plan* p, int stage, const T* f0, typename Cx<T>::type* F, const typename Cx<T>::type* Fin,
+                  T* f0_out, const T* E, bool use_K, int B, cudaStream_t st) {
   using C = typename Cx<T>::type;
   const DevGeom* g = static_cast<const DevGeom*>(p->d_geom);
   const C* tab = static_cast<const C*>(p->d_tables);
   C* W = static_cast<C*>(p->d_work_T);
   const PlanTables& T_ = p->T;
-  if (E)
-    k_plane_fwd<T, true><<<dim3(T_.H[2], B), p->threads_xy, p->smem_xy, st>>>(g, tab, f0, E, W);
-  else
-    k_plane_fwd<T, false><<<dim3(T_.H[2], B), p->threads_xy, p->smem_xy, st>>>(g, tab, f0, nullptr, W);
-  if (T_.H[2] > 1) {
-    k_fft_z<T, false><<<dim3(T_.H[1], T_.n_ch, B), p->threads_z, p->smem_z, st>>>(g, tab, W);
-    ++g_launches;
+  switch (stage) {
+    case 0:
+      if (E) k_plane_fwd<T, true><<<dim3(T_.H[2], B), p->threads_xy, p->smem_xy, st>>>(g, tab, f0, E, W);
+      else k_plane_fwd<T, false><<<dim3(T_.H[2], B), p->threads_xy, p->smem_xy, st>>>(g, tab, f0, nullptr, W);
+      break;
+    case 1:
+      if (T_.H[2] <= 1) return;
+      k_fft_z<T, false><<<dim3(T_.H[1], T_.n_ch, B), p->threads_z, p->smem_z, st>>>(g, tab, W);
+      break;
+    case 2: {
+      const int ns = static_cast<int>(T_.spec.size());
+      const dim3 gr((ns + 255) / 256, B);
+      if (use_K)
+        k_recon<T, true><<<gr, 256, 0, st>>>(g, tab, static_cast<const uint32_t*>(p->d_spec_h), static_cast<const T*>(p->d_K), W, F);
+      else
+        k_recon<T, false><<<gr, 256, 0, st>>>(g, tab, static_cast<const uint32_t*>(p->d_spec_h), nullptr, W, F);
+      break;
+    }
+    case 3: {
+      const int no = static_cast<int>(T_.orbit_rep.size());
+      k_inv_recon<T><<<dim3((no + 127) / 128, B), 128, 0, st>>>(
+          g, tab, static_cast<const int32_t*>(p->d_orbit_rep), static_cast<const int32_t*>(p->d_inv_spec),
+          static_cast<const int32_t*>(p->d_inv_phase), static_cast<const uint32_t*>(p->d_img_mask), Fin, W);
+      break;
+    }
+    case 4:
+      if (T_.H[2] <= 1) return;
+      k_fft_z<T, true><<<dim3(T_.H[1], T_.n_ch, B), p->threads_z, p->smem_z, st>>>(g, tab, W);
+      break;
+    default:
+      if (E) k_plane_bwd<T, true><<<dim3(T_.H[2], B), p->threads_xy, p->smem_xy, st>>>(g, tab, W, E, f0_out);
+      else k_plane_bwd<T, false><<<dim3(T_.H[2], B), p->threads_xy, p->smem_xy, st>>>(g, tab, W, nullptr, f0_out);
+      break;
   }
-  const int ns = static_cast<int>(T_.spec.size());
-  const dim3 gr((ns + 255) / 256, B);
-  if (use_K)
-    k_recon<T, true><<<gr, 256, 0, st>>>(g, tab, static_cast<const uint32_t*>(p->d_spec_h), static_cast<const T*>(p->d_K), W, F);
-  else
-    k_recon<T, false><<<gr, 256, 0, st>>>(g, tab, static_cast<const uint32_t*>(p->d_spec_h), nullptr, W, F);
-  g_launches += 2;
+  ++g_launches;
+}
+
+template <typename T>
+Status launch_forward(Plan* p, const T* f0, typename Cx<T>::type* F, const T* E, bool use_K, int B,
+                      cudaStream_t st, std::string* err) {
+  for (int s = 0; s < 3; ++s) launch_stage<T>(p, s, f0, F, nullptr, nullptr, E, use_K, B, st);
   CFFT_CUDA(cudaGetLastError(), "forward launch");
   return Status::kOk;
 }
@@ -583,25 +604,26 @@ Status launch_forward(Plan* p, const T* f0, typename Cx<T>::type* F, const T* E,
 template <typename T>
 Status launch_backward(Plan* p, const typename Cx<T>::type* F, T* f0, const T* E, int B, cudaStream_t st,
                        std::string* err) {
-  using C = typename Cx<T>::type;
-  const DevGeom* g = static_cast<const DevGeom*>(p->d_geom);
-  const C* tab = static_cast<const C*>(p->d_tables);
-  C* W = static_cast<C*>(p->d_work_T);
-  const PlanTables& T_ = p->T;
-  const int no = static_cast<int>(T_.orbit_rep.size());
-  k_inv_recon<T><<<dim3((no + 127) / 128, B), 128, 0, st>>>(
-      g, tab, static_cast<const int32_t*>(p->d_orbit_rep), static_cast<const int32_t*>(p->d_inv_spec),
-      static_cast<const int32_t*>(p->d_inv_phase), static_cast<const uint32_t*>(p->d_img_mask), F, W);
-  if (T_.H[2] > 1) {
-    k_fft_z<T, true><<<dim3(T_.H[1], T_.n_ch, B), p->threads_z, p->smem_z, st>>>(g, tab, W);
-    ++g_launches;
-  }
-  if (E)
-    k_plane_bwd<T, true><<<dim3(T_.H[2], B), p->threads_xy, p->smem_xy, st>>>(g, tab, W, E, f0);
-  else
-    k_plane_bwd<T, false><<<dim3(T_.H[2], B), p->threads_xy, p->smem_xy, st>>>(g, tab, W, nullptr, f0);
-  g_launches += 2;
+  for (int s = 3; s < 6; ++s) launch_stage<T>(p, s, nullptr, nullptr, F, f0, E, false, B, st);
   CFFT_CUDA(cudaGetLastError(), "backward launch");
+  return Status::kOk;
+}
+
+template <typename T>
+Status profile_roundtrip(Plan* p, const T* f0, typename Cx<T>::type* F, T* f0_out, int B, cudaStream_t st,
+                         float* ms, int* n, std::string* err) {
+  cudaEvent_t ev[7];
+  for (int i = 0; i < 7; ++i) CFFT_CUDA(cudaEventCreate(&ev[i]), "event create");
+  CFFT_CUDA(cudaEventRecord(ev[0], st), "event record");
+  for (int s = 0; s < 6; ++s) {
+    launch_stage<T>(p, s, f0, F, F, f0_out, nullptr, false, B, st);
+    CFFT_CUDA(cudaEventRecord(ev[s + 1], st), "event record");
+  }
+  CFFT_CUDA(cudaGetLastError(), "profile launch");
+  CFFT_CUDA(cudaEventSynchronize(ev[6]), "event sync");
+  for (int s = 0; s < 6; ++s) CFFT_CUDA(cudaEventElapsedTime(&ms[s], ev[s], ev[s + 1]), "elapsed");
+  *n = 6;
+  for (int i = 0; i < 7; ++i) cudaEventDestroy(ev[i]);
   return Status::kOk;
 }
 
@@ -680,11 +702,10 @@ Status plan_device_init(Plan* p, std::string* err) {
   // launch geometry and shared memory
   const long pe = static_cast<long>(T.n_ch) * T.H[0] * T.H[1];
   const long ze = static_cast<long>(T.H[0]) * T.H[2];
-  if (pe > 15 * 1024 || ze > 15 * 1024) { *err = "channel plane too large for one CTA"; return Status::kUnsupported; }
-  p->threads_xy = std::min(1024, round_threads(pe));
-  p->threads_z = std::min(1024, round_threads(ze));
-  p->smem_xy = (pe + T.H[0] + T.H[1]) * cs;
-  p->smem_z = (ze + T.H[2]) * cs;
+  p->threads_xy = round_threads(pe);
+  p->threads_z = round_threads(ze);
+  p->smem_xy = (2 * pe + T.H[0] + T.H[1]) * cs;
+  p->smem_z = (2 * ze + T.H[2]) * cs;
   if (p->smem_xy > 227 * 1024 || p->smem_z > 227 * 1024) { *err = "shared memory above 227 KB"; return Status::kUnsupported; }
 
   auto alloc = [&](void** ptr, size_t bytes, const char* what) -> Status {
@@ -753,6 +774,17 @@ Status exec_forward(Plan* p, const void* f0, void* F, int B, void* stream, std::
   if (p->precision == 8)
     return launch_forward<double>(p, static_cast<const double*>(f0), static_cast<double2*>(F), nullptr, false, B, s, err);
   return launch_forward<float>(p, static_cast<const float*>(f0), static_cast<float2*>(F), nullptr, false, B, s, err);
+}
+
+Status exec_profile_roundtrip(Plan* p, const void* f0, void* F, void* f0_out, int B, void* stream, float* ms,
+                              int* n, std::string* err) {
+  Status st = check_batch(p, B, err);
+  if (st != Status::kOk) return st;
+  if (!f0 || !F || !f0_out || !ms || !n) { *err = "null pointer"; return Status::kInvalid; }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (p->precision == 8)
+    return profile_roundtrip<double>(p, static_cast<const double*>(f0), static_cast<double2*>(F), static_cast<double*>(f0_out), B, s, ms, n, err);
+  return profile_roundtrip<float>(p, static_cast<const float*>(f0), static_cast<float2*>(F), static_cast<float*>(f0_out), B, s, ms, n, err);
 }
 
 Status exec_backward(Plan* p, const void* F, void* f0, int B, void* stream, std::string* err) {

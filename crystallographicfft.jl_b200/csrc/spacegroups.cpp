@@ -126,7 +126,7 @@ const GroupEntry kGroups[] = {
     {69, 3, 'F', 32, "-x,-y,z;-x,y,-z;-x,-y,-z"},
     {70, 3, 'F', 32, "-x+3/4,-y+3/4,z;-x+3/4,y,-z+3/4;-x,-y,-z"},
     {71, 3, 'I', 16, "-x,-y,z;-x,y,-z;-x,-y,-z"},
-    {72, 3, 'I', 16, "-x,-y,z;-x,y,-z+1/2;-x,-y,-z"},
+    {72, 3, 'I', 16, "-x,-y,z;-x+1/2,y+1/2,-z;-x,-y,-z"},
     {73, 3, 'I', 16, "-x+1/2,-y,z+1/2;-x,y+1/2,-z+1/2;-x,-y,-z"},
     {74, 3, 'I', 16, "-x,-y+1/2,z;-x,y+1/2,-z;-x,-y,-z"},
     // ---------------- tetragonal (selection) ----------------

@@ -172,6 +172,13 @@ cfft_status cfft_backward_host(cfft_plan plan, const void* F_host, void* f0_host
 cfft_status cfft_scft_step_host(cfft_plan plan, void* f0_host, int batch);
 
 /* ---------------- diagnostics ---------------- */
+/* Forward then backward of one batch with a CUDA event between every launch;
+ * stage_ms receives up to 8 per-stage device times (plane/fold+xy FFT, z FFT,
+ * reconstruct, inverse reconstruct, inverse z FFT, inverse xy FFT + unfold) and
+ * *n_stages their number.  Synchronises the stream.  No reference counterpart:
+ * it backs the per-kernel timing of the benchmark. */
+cfft_status cfft_profile_roundtrip(cfft_plan plan, const void* f0, void* F, void* f0_out, int batch, void* stream,
+                                   float* stage_ms, int* n_stages);
 const char* cfft_status_string(cfft_status s);
 const char* cfft_last_error(void);
 int cfft_version(void);

@@ -1,0 +1,39 @@
+"""The C-ABI library loads without a GPU and exports every symbol include/cfft_b200.h
+declares; host-only entry points return the documented status codes."""
+import ctypes
+import os
+import re
+
+from conftest import PKG_DIR, ROOT
+
+
+def declared_symbols():
+    text = open(os.path.join(ROOT, "include", "cfft_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(cfft_[A-Za-z0-9_]+)\s*\(", text)))
+
+
+def test_header_symbols_exported(cf):
+    lib = ctypes.CDLL(os.path.join(PKG_DIR, "libcfft_b200.so"))
+    syms = declared_symbols()
+    assert len(syms) >= 25
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_status_strings(cf):
+    lib = cf.LIB
+    for code in range(8):
+        assert lib.cfft_status_string(code)
+    assert lib.cfft_version() >= 100
+
+
+def test_invalid_arguments(cf):
+    lib = cf.LIB
+    assert lib.cfft_plan_create(None, None) == 1
+    n = ctypes.c_int(0)
+    N = (ctypes.c_int * 3)(16, 16, 16)
+    assert lib.cfft_get_ops(999, 3, N, 0, ctypes.byref(n), None, None) == 4
+    assert lib.cfft_get_ops(229, 4, N, 0, ctypes.byref(n), None, None) == 1
+    assert lib.cfft_forward(None, None, None, 1, None) == 1
+    assert b"null" in lib.cfft_last_error() or lib.cfft_last_error()

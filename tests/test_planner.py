@@ -1,0 +1,155 @@
+"""Host plan layer (C++ via the C ABI) against the oracle: integer tables must be
+bit-exact (shift, shifted ops, spectral ASU points / multiplicities / order, L,
+centring, representative ops), backward lookup tables must match the oracle's
+M2 inverse table, and the generated space-group tables must agree with the
+reference's Crystalline-derived mirror/glide table (tests/golden/mirror_table.json)."""
+import json
+import os
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+from conftest import to_oracle_ops
+
+GROUPS = [1, 2, 10, 16, 25, 35, 47, 62, 63, 69, 70, 71, 72, 74, 75, 99, 123, 136, 139, 200, 221, 223, 224, 225,
+          227, 229, 230]
+
+EXPECTED_ORDER = {1: 1, 2: 2, 10: 4, 47: 8, 63: 16, 70: 32, 72: 16, 139: 32, 221: 48, 225: 192, 227: 192,
+                  229: 96, 230: 96, 166: 36, 191: 24}
+
+
+def test_group_orders(cf):
+    for sg, n in EXPECTED_ORDER.items():
+        N = (12, 12, 12)
+        assert len(cf.get_ops(sg, 3, N)) == n
+
+
+def test_all_table_groups_close(cf):
+    assert len(cf.available_groups(3)) >= 130
+    for sg in cf.available_groups(3):
+        ops = cf.get_ops(sg, 3, (12, 12, 12))
+        assert ops[0].R == (1, 0, 0, 0, 1, 0, 0, 0, 1) and ops[0].t == (0, 0, 0)
+    for sg in cf.available_groups(2):
+        ops = cf.get_ops(sg, 2, (12, 12))
+        assert ops[0].R == (1, 0, 0, 1)
+
+
+def test_not_commensurate(cf):
+    with pytest.raises(cf.CFFTError) as e:
+        cf.get_ops(227, 3, (10, 10, 10))  # 1/4 translations on a 10-point grid
+    assert e.value.status == 3
+
+
+def test_mirror_table_fixture(cf):
+    table = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "mirror_table.json")))
+    for sg in cf.available_groups(3):
+        ops = cf.get_ops(sg, 3, (12, 12, 12))
+        e = table[str(sg)]
+        cv = {tuple(Fraction(v, 12) for v in op.t) for op in ops
+              if np.array_equal(op.Rm, np.eye(3, dtype=int)) and any(op.t)}
+        assert cv == {tuple(Fraction(x) for x in v) for v in e["centering_vecs"]}, sg
+        for n, tr in zip(e["normals"], e["translations"]):
+            found = None
+            for op in ops:
+                R = op.Rm
+                if not np.array_equal(R @ R, np.eye(3, dtype=int)) or round(np.linalg.det(R)) != -1:
+                    continue
+                A = R + np.eye(3, dtype=int)
+                m = np.cross(A[0], A[1])
+                if not m.any():
+                    m = np.cross(A[0], A[2])
+                if not m.any():
+                    m = np.cross(A[1], A[2])
+                if m.any() and not np.cross(m, np.array(n)).any():
+                    found = op
+                    break
+            assert found is not None, (sg, n)
+            assert tuple(Fraction(v, 12) % 1 for v in found.t) == tuple(Fraction(x) % 1 for x in tr), (sg, n)
+
+
+@pytest.mark.parametrize("sg", GROUPS)
+def test_plan_geometry_bit_exact(cf, O, sg):
+    N = (16, 16, 16)
+    ops = cf.get_ops(sg, 3, N)
+    shift, ops_s = cf.find_optimal_shift(ops, N)
+    oshift, oops_s = O.find_optimal_shift(to_oracle_ops(O, ops), N)
+    assert np.array_equal(shift, oshift)
+    assert [(a.R, a.t) for a in ops_s] == [(b.R, b.t) for b in oops_s]
+    spec = cf.calc_spectral_asu(ops_s, 3, N)
+    ospec = O.calc_spectral_asu(oops_s, 3, N)
+    assert np.array_equal(spec.idx, ospec.idx) and np.array_equal(spec.mult, ospec.mult)
+    assert cf.auto_L(ops_s) == O.auto_L(oops_s)
+    assert cf.detect_centering_type(ops_s, N) == O.detect_centering_type(oops_s, N)
+    assert cf.count_special_positions((12, 12, 12), ops_s[:]) >= 0
+
+
+@pytest.mark.parametrize("sg,N", [(229, (16, 16, 16)), (47, (16, 16, 16)), (230, (16, 16, 16)), (10, (16, 16, 16)),
+                                  (225, (16, 16, 16)), (70, (16, 16, 16)), (221, (24, 24, 24)), (229, (24, 24, 24))])
+def test_plan_tables_vs_oracle(cf, O, sg, N):
+    ops = cf.get_ops(sg, 3, N)
+    _, ops_s = cf.find_optimal_shift(ops, N)
+    spec = cf.calc_spectral_asu(ops_s, 3, N)
+    plan = cf.KRFFTPlan(spec, ops_s, ds=0.05, precision=8, device=False)
+    oops = to_oracle_ops(O, ops_s)
+    ospec = O.calc_spectral_asu(oops, 3, N)
+    idx, mult = plan.spectral_asu()
+    assert np.array_equal(idx, ospec.idx) and np.array_equal(mult, ospec.mult)
+    L = O.auto_L(oops)
+    assert plan.L == L and plan.M == tuple(n // l for n, l in zip(N, L))
+    rep = plan.rep_ops()
+    orep = O.select_rep_ops(oops, L, N)
+    assert [(a.R, a.t) for a in rep] == [(b.R, b.t) for b in orep]
+    # centring-fold metadata (plan_krfft_centered / plan_centering_fold)
+    ofwd = O.plan_krfft_centered(ospec, oops)
+    assert plan.centered == isinstance(ofwd, O.CenteredPlan)
+    if plan.centered:
+        assert plan.n_channels == ofwd.fold.n_channels and plan.H == ofwd.fold.H
+    # backward lookup: per orbit representative and alias, the signed spectral index
+    # and the phase must reproduce the oracle's M2 inverse table entry (weight / (1/d)).
+    reps, s_tab, p_tab = plan.backward_tables()
+    ob = O.plan_m2_backward(ospec, oops)
+    d = ob.d
+    P = plan.info.P
+    for o, q in enumerate(reps):
+        for a in range(d):
+            s = int(s_tab[o, a])
+            if s == 0:
+                assert ob.inv_spec[a, q] < 0
+                continue
+            assert ob.inv_spec[a, q] == abs(s) - 1
+            assert bool(ob.inv_conj[a, q]) == (s < 0)
+            w = np.exp(2j * np.pi * p_tab[o, a] / P) / d
+            assert abs(w - ob.inv_w[a, q]) < 1e-12
+    # diffusion kernel K
+    assert np.allclose(plan.kernel(), O.kernel_spec(ospec, N, 0.05, np.eye(3)), rtol=0, atol=1e-15)
+    plan.close()
+
+
+def test_orbit_representatives_cover_grid(cf, O):
+    """Orbit representatives under the even-translation operations partition the
+    alive channel positions exactly once (the device expansion writes each once)."""
+    for sg in (229, 225, 47, 230):
+        N = (16, 16, 16)
+        _, ops_s = cf.find_optimal_shift(cf.get_ops(sg, 3, N), N)
+        spec = cf.calc_spectral_asu(ops_s, 3, N)
+        plan = cf.KRFFTPlan(spec, ops_s, device=False)
+        reps, _, _ = plan.backward_tables()
+        assert len(np.unique(reps)) == len(reps)
+        assert plan.info.n_orbits == len(reps) > 0
+        plan.close()
+
+
+def test_plan_errors(cf):
+    N = (16, 16, 16)
+    _, ops_s = cf.find_optimal_shift(cf.get_ops(229, 3, N), N)
+    spec = cf.calc_spectral_asu(ops_s, 3, N)
+    with pytest.raises(cf.CFFTError):
+        cf.KRFFTPlan(spec, ops_s, precision=3, device=False)
+    with pytest.raises(cf.CFFTError):
+        cf.KRFFTPlan(spec, ops_s, max_batch=0, device=False)
+    plan = cf.KRFFTPlan(spec, ops_s, device=False)
+    with pytest.raises(cf.CFFTError) as e:
+        plan.forward(np.zeros(plan.M))  # host-only plan has no device state
+    assert e.value.status == 1
+    plan.close()
