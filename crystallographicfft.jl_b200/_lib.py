@@ -88,6 +88,7 @@ def _load():
         "cfft_scft_step_host": (c_int, [c_void_p, c_void_p, c_int]),
         "cfft_profile_roundtrip": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p,
                                            ctypes.POINTER(ctypes.c_float), c_int_p]),
+        "cfft_forward_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
         "cfft_status_string": (ctypes.c_char_p, [c_int]),
         "cfft_last_error": (ctypes.c_char_p, []),
         "cfft_version": (c_int, []),

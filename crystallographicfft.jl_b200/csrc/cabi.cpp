@@ -284,6 +284,12 @@ cfft_status cfft_profile_roundtrip(cfft_plan plan, const void* f0, void* F, void
   CFFT_EXEC(cfft::exec_profile_roundtrip(p, f0, F, f0_out, batch, stream, stage_ms, n_stages, &err));
 }
 
+cfft_status cfft_forward_noalloc(cfft_plan plan, const void* f0, void* F, int batch, void* stream) {
+  if (!plan) return ret(Status::kInvalid, "null plan");
+  std::string err;
+  return ret(cfft::exec_forward_noalloc(reinterpret_cast<cfft::Plan*>(plan), f0, F, batch, stream, &err), err);
+}
+
 const char* cfft_status_string(cfft_status s) {
   switch (s) {
     case CFFT_OK: return "ok";

@@ -954,4 +954,125 @@ Status exec_host(Plan* p, int which, const void* in, void* out, int B, std::stri
   return Status::kOk;
 }
 
+// ---------------------------------------------------------------- allocation-free forward
+// cfft_forward_noalloc: the forward transform for callers that may not allocate
+// device memory (for example a process whose device memory belongs entirely to
+// another allocator, or code that must not call into the driver's allocator while
+// it runs).  The channel workspace, the geometry and the twiddle/phase tables live in
+// one file-scope static device array instead of cudaMalloc'd plan buffers, so a plan
+// built with cfft_plan_create_host (host memory only) is enough.  Every GPU that
+// loads this library holds the array (kNoAllocBytes) until the process exits.
+namespace {
+
+constexpr size_t kNoAllocBytes = static_cast<size_t>(32) << 20;  // 32 MiB per device
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+std::mutex g_noalloc_mu;
+constexpr int kNoAllocMaxDevices = 64;
+unsigned char* g_noalloc_addr[kNoAllocMaxDevices] = {nullptr};
+
+size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+
+// Device address of the static scratch for the current device, looked up once per
+// device (the array's name is only a host-side stand-in in host code).
+Status noalloc_scratch_for_current_device(unsigned char** out, std::string* err) {
+  int dev = 0;
+  CFFT_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  if (dev < 0 || dev >= kNoAllocMaxDevices) { *err = "device ordinal above the supported range"; return Status::kUnsupported; }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* ptr = nullptr;
+    CFFT_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch), "cudaGetSymbolAddress(static scratch)");
+    set_smem_attrs<float>();
+    set_smem_attrs<double>();
+    CFFT_CUDA(cudaGetLastError(), "set shared-memory attributes");
+    g_noalloc_addr[dev] = static_cast<unsigned char*>(ptr);
+  }
+  *out = g_noalloc_addr[dev];
+  return Status::kOk;
+}
+
+template <typename T>
+Status noalloc_forward(const Plan* p, const T* f0, typename Cx<T>::type* F, int B, cudaStream_t st,
+                       std::string* err) {
+  using C = typename Cx<T>::type;
+  const PlanTables& Tb = p->T;
+  DevGeom g;
+  std::memset(&g, 0, sizeof(g));
+  for (int d = 0; d < 3; ++d) {
+    g.N[d] = Tb.N[d]; g.M[d] = Tb.M[d]; g.H[d] = Tb.H[d]; g.L[d] = Tb.L[d];
+    if (!factor_radices(Tb.H[d], &g.nf[d], g.radix[d])) { *err = "FFT length must factor into 2, 3, 5"; return Status::kUnsupported; }
+  }
+  if (Tb.d > 8) { *err = "fiber length above 8"; return Status::kUnsupported; }
+  if (Tb.P > 8192) { *err = "phase denominator lcm(N) above 8192"; return Status::kUnsupported; }
+  g.P = Tb.P; g.d = Tb.d; g.n_ch = Tb.n_ch; g.centered = Tb.centered ? 1 : 0;
+  g.n_spec = static_cast<int>(Tb.spec.size());
+  for (int k = 0; k < 8; ++k) g.chan_of_parity[k] = Tb.chan_of_parity[k];
+  for (int c = 0; c < Tb.n_ch; ++c) g.off_idx[c] = Tb.offsets[c][0] + 2 * Tb.offsets[c][1] + 4 * Tb.offsets[c][2];
+  for (int r = 0; r < Tb.d; ++r) {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) g.rep_R[r][i * 3 + j] = Tb.rep_ops[r].R[i][j];
+    for (int i = 0; i < 3; ++i) g.rep_t[r][i] = Tb.rep_ops[r].t[i];
+  }
+  std::vector<uint32_t> hp(Tb.spec.size());
+  for (size_t s = 0; s < Tb.spec.size(); ++s)
+    hp[s] = static_cast<uint32_t>(Tb.spec[s].h[0]) | (static_cast<uint32_t>(Tb.spec[s].h[1]) << 10) |
+            (static_cast<uint32_t>(Tb.spec[s].h[2]) << 20);
+  const std::vector<unsigned char> tab = make_table_bytes<T>(*p, &g);
+  const size_t cs = sizeof(C);
+  const size_t hvol = static_cast<size_t>(Tb.H[0]) * Tb.H[1] * Tb.H[2];
+  const size_t off_tab = align256(sizeof(DevGeom));
+  const size_t off_spec = off_tab + align256(tab.size());
+  const size_t off_W = off_spec + align256(hp.size() * 4);
+  const size_t per_field = align256(static_cast<size_t>(Tb.n_ch) * hvol * cs);
+  if (off_W + per_field > kNoAllocBytes) {
+    *err = "the allocation-free forward needs " + std::to_string(off_W + per_field) +
+           " bytes of scratch for one field; its static scratch holds " + std::to_string(kNoAllocBytes) + " bytes";
+    return Status::kUnsupported;
+  }
+  const int chunk = static_cast<int>((kNoAllocBytes - off_W) / per_field);
+  const long pe = static_cast<long>(Tb.n_ch) * Tb.H[0] * Tb.H[1];
+  const long ze = static_cast<long>(Tb.H[0]) * Tb.H[2];
+  const int thr_xy = round_threads(pe), thr_z = round_threads(ze);
+  const size_t smem_xy = (2 * pe + Tb.H[0] + Tb.H[1]) * cs, smem_z = (2 * ze + Tb.H[2]) * cs;
+  if (smem_xy > 227 * 1024 || smem_z > 227 * 1024) { *err = "shared memory above 227 KB"; return Status::kUnsupported; }
+
+  unsigned char* base = nullptr;
+  Status s = noalloc_scratch_for_current_device(&base, err);
+  if (s != Status::kOk) return s;
+  // Pageable-source copies return once the host data is staged, so the locals may go.
+  CFFT_CUDA(cudaMemcpyAsync(base, &g, sizeof(g), cudaMemcpyHostToDevice, st), "upload geometry");
+  CFFT_CUDA(cudaMemcpyAsync(base + off_tab, tab.data(), tab.size(), cudaMemcpyHostToDevice, st), "upload tables");
+  CFFT_CUDA(cudaMemcpyAsync(base + off_spec, hp.data(), hp.size() * 4, cudaMemcpyHostToDevice, st), "upload points");
+  const DevGeom* dg = reinterpret_cast<const DevGeom*>(base);
+  const C* dtab = reinterpret_cast<const C*>(base + off_tab);
+  const uint32_t* dspec = reinterpret_cast<const uint32_t*>(base + off_spec);
+  C* W = reinterpret_cast<C*>(base + off_W);
+  const size_t mvol = static_cast<size_t>(Tb.M[0]) * Tb.M[1] * Tb.M[2];
+  const int ns = g.n_spec;
+  for (int b0 = 0; b0 < B; b0 += chunk) {
+    const int nb = std::min(chunk, B - b0);
+    k_plane_fwd<T, false><<<dim3(Tb.H[2], nb), thr_xy, smem_xy, st>>>(dg, dtab, f0 + b0 * mvol, nullptr, W);
+    ++g_launches;
+    if (Tb.H[2] > 1) {
+      k_fft_z<T, false><<<dim3(Tb.H[1], Tb.n_ch, nb), thr_z, smem_z, st>>>(dg, dtab, W);
+      ++g_launches;
+    }
+    k_recon<T, false><<<dim3((ns + 255) / 256, nb), 256, 0, st>>>(dg, dtab, dspec, nullptr, W,
+                                                                    F + static_cast<size_t>(b0) * ns);
+    ++g_launches;
+  }
+  CFFT_CUDA(cudaGetLastError(), "allocation-free forward launch");
+  return Status::kOk;
+}
+
+}  // namespace
+
+Status exec_forward_noalloc(const Plan* p, const void* f0, void* F, int B, void* stream, std::string* err) {
+  if (B < 1 || !f0 || !F) { *err = "invalid argument (batch < 1 or null pointer)"; return Status::kInvalid; }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (p->precision == 8)
+    return noalloc_forward<double>(p, static_cast<const double*>(f0), static_cast<double2*>(F), B, s, err);
+  return noalloc_forward<float>(p, static_cast<const float*>(f0), static_cast<float2*>(F), B, s, err);
+}
+
 }  // namespace cfft

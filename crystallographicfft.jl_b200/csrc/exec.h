@@ -52,6 +52,8 @@ Status exec_host(Plan* p, int which, const void* in, void* out, int B, std::stri
 Status exec_profile_roundtrip(Plan* p, const void* f0, void* F, void* f0_out, int B, void* stream, float* ms,
                               int* n, std::string* err);
 
+Status exec_forward_noalloc(const Plan* p, const void* f0, void* F, int B, void* stream, std::string* err);
+
 int64_t launch_count(bool reset);
 
 }  // namespace cfft

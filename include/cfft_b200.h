@@ -165,6 +165,22 @@ cfft_status cfft_step_diffusion(cfft_plan plan, void* q, const void* w, double d
 cfft_status cfft_fullgrid_to_subgrid(cfft_plan plan, const void* u, void* f0, int batch, void* stream);
 cfft_status cfft_subgrid_to_fullgrid(cfft_plan plan, const void* f0, void* u, int batch, void* stream);
 
+/* Allocation-free forward.  No counterpart in the reference: it exists for callers
+ * that cannot allocate device memory themselves or through this library -- for
+ * example a process whose device memory is owned entirely by another allocator, or
+ * code that must not enter the driver's allocator while it runs.  It computes what
+ * cfft_forward computes, but its workspace, geometry and twiddle tables live in one
+ * static device array of 32 MiB compiled into the library (every GPU that loads the
+ * library holds it until the process exits), so a plan from cfft_plan_create_host is
+ * enough; f0 and F are the caller's device buffers.  Any batch size is processed in
+ * chunks that fit the array; a problem whose single field needs more scratch than
+ * 32 MiB is rejected with CFFT_ERR_UNSUPPORTED.  The first call on each device looks
+ * up the array's device address and sets kernel attributes, so make that first call
+ * before any stream capture.  It never calls cudaMalloc or cudaFree.  All calls share
+ * the one array: calls that overlap on the GPU (other streams, other host threads)
+ * race and must be serialised by the caller. */
+cfft_status cfft_forward_noalloc(cfft_plan plan, const void* f0, void* F, int batch, void* stream);
+
 /* Host-buffer forms of the three execute calls (the reference's execute_*! take
  * host arrays): copy in, run, copy out on the plan's own stream, then synchronise. */
 cfft_status cfft_forward_host(cfft_plan plan, const void* f0_host, void* F_host, int batch);
