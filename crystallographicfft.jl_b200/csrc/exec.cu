@@ -20,6 +20,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <cstdlib>
 #include <mutex>
 
 #include "exec.h"
@@ -48,6 +49,8 @@ struct DevGeom {
   int tw_off[3];           // e^{-2 pi i j / H_d}, j < H_d
   int ftw_off[3];          // e^{-2 pi i j / M_d}, j < H_d  (fold twiddles)
   int ph_off;              // e^{-2 pi i j / P}, j < P
+  int pmask;               // P - 1 when P is a power of two, else -1
+  int rep_tp[8][3];        // t_b,d * (P / N_d): phase numerators per unit frequency
 };
 
 template <typename T> struct Cx;
@@ -386,10 +389,8 @@ __global__ void k_recon(const DevGeom* __restrict__ g, const typename Cx<T>::typ
     } else {
       idx = (static_cast<size_t>(q[2]) * H2 + q[1]) * H1 + q[0];
     }
-    long long j = 0;
-#pragma unroll
-    for (int dd = 0; dd < 3; ++dd) j += static_cast<long long>(h[dd]) * g->rep_t[r][dd] * (P / g->N[dd]);
-    const int jj = static_cast<int>(((j % P) + P) % P);
+    int jj = h[0] * g->rep_tp[r][0] + h[1] * g->rep_tp[r][1] + h[2] * g->rep_tp[r][2];
+    jj = g->pmask >= 0 ? (jj & g->pmask) : ((jj % P) + P) % P;
     acc = cadd(acc, cmul(Wb[idx], ph[jj]));
   }
   if (USE_K) acc = cscale(acc, K[s]);
@@ -448,6 +449,390 @@ __global__ void k_inv_recon(const DevGeom* __restrict__ g, const typename Cx<T>:
     Wb[idx] = val;
   }
   (void)M3;
+}
+
+// ---------------------------------------------------------------- compile-time sized path
+// For cubic channel grids with H in {4, 6, 8, 12, 16, 24, 32, 48} every line FFT is a
+// fully unrolled mixed-radix Stockham in registers (one thread per line), with its
+// twiddles in constant memory, so no runtime division or shared-memory pass remains
+// inside an FFT.  Shared-memory rows are padded to an odd stride (H + 1 complex) so
+// row and column accesses of a warp are bank-conflict free.
+
+constexpr int kTwOff4 = 0, kTwOff6 = 4, kTwOff8 = 10, kTwOff12 = 18, kTwOff16 = 30, kTwOff24 = 46,
+              kTwOff32 = 70, kTwOff48 = 102, kTwTotal = 150;
+__constant__ float2 c_tw_f[kTwTotal];
+__constant__ double2 c_tw_d[kTwTotal];
+
+template <int N> constexpr int tw_offset() {
+  return N == 4 ? kTwOff4 : N == 6 ? kTwOff6 : N == 8 ? kTwOff8 : N == 12 ? kTwOff12 : N == 16 ? kTwOff16
+       : N == 24 ? kTwOff24 : N == 32 ? kTwOff32 : kTwOff48;
+}
+constexpr int pick_radix(int rem) { return rem % 8 == 0 ? 8 : rem % 4 == 0 ? 4 : rem % 2 == 0 ? 2 : rem % 3 == 0 ? 3 : 5; }
+
+template <typename C> __device__ __forceinline__ C ctw(int i);
+template <> __device__ __forceinline__ float2 ctw<float2>(int i) { return c_tw_f[i]; }
+template <> __device__ __forceinline__ double2 ctw<double2>(int i) { return c_tw_d[i]; }
+
+template <typename C, bool INV, int N, int Ns, int Rem>
+struct RegFFT {
+  static __device__ __forceinline__ void run(C* v) {
+    constexpr int R = pick_radix(Rem);
+    constexpr int NB = N / R;
+    constexpr int STEP = N / (Ns * R);
+    C w[N];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+      const int k = j % Ns;
+      C x[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) x[r] = v[j + r * NB];
+      if (k != 0) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          const C t = ctw<C>(tw_offset<N>() + r * k * STEP);
+          x[r] = INV ? cmulc(x[r], t) : cmul(x[r], t);
+        }
+      }
+      dftR<C, INV, R>(x);
+      const int o = (j / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) w[o + r * Ns] = x[r];
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = w[i];
+    RegFFT<C, INV, N, Ns * R, Rem / R>::run(v);
+  }
+};
+template <typename C, bool INV, int N, int Ns>
+struct RegFFT<C, INV, N, Ns, 1> {
+  static __device__ __forceinline__ void run(C*) {}
+};
+template <typename C, bool INV, int N> __device__ __forceinline__ void reg_fft(C* v) { RegFFT<C, INV, N, 1, N>::run(v); }
+
+// FFT of `count` lines of length H in padded shared memory, one thread per line.
+// Line l starts at line_base(l) and has element stride es.
+template <typename C, bool INV, int H>
+__device__ __forceinline__ void smem_lines(C* buf, int count, int group, int gstride, int lstride, int es) {
+  for (int l = threadIdx.x; l < count; l += blockDim.x) {
+    C* p = buf + (l / group) * gstride + (l % group) * lstride;
+    C v[H];
+#pragma unroll
+    for (int i = 0; i < H; ++i) v[i] = p[i * es];
+    reg_fft<C, INV, H>(v);
+#pragma unroll
+    for (int i = 0; i < H; ++i) p[i * es] = v[i];
+  }
+}
+
+// Two real fields share one complex transform on the fast path: slot s of the
+// channel workspace holds g_a + i g_b for fields a = 2s and b = 2s + 1 (b may be
+// absent at the end of a batch).  The forward gather separates them with
+// G_a(p) = (X(p) + conj X(-p)) / 2 and G_b(p) = (X(p) - conj X(-p)) / 2i, the backward
+// builds X = G_a + i G_b and the unfold reads field a from the real part and field b
+// from the imaginary part.  This halves the FFT work and the workspace traffic.
+
+// Forward plane kernel, cubic H: fold (or plain load) of two fields + x FFT + y FFT
+// -> W[slot][c][z][y][x].
+template <typename T, int H, bool USE_E>
+__global__ void k_plane_fwd_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                              const T* __restrict__ f0, const T* __restrict__ E, typename Cx<T>::type* __restrict__ W,
+                              int nfields) {
+  using C = typename Cx<T>::type;
+  constexpr int S = H + 1;
+  constexpr int PL = H * S;  // padded plane
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int nch = g->n_ch;
+  const int iz = blockIdx.x, slot = blockIdx.y;
+  const int fa = 2 * slot;
+  const bool has_b = fa + 1 < nfields;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const size_t mvol = static_cast<size_t>(g->M[0]) * g->M[1] * g->M[2];
+  const T* srca = f0 + static_cast<size_t>(fa) * mvol;
+  const T* srcb = srca + mvol;
+  const T* Ea = USE_E ? E + static_cast<size_t>(fa) * mvol : nullptr;
+  const T* Eb = USE_E ? Ea + mvol : nullptr;
+  const T zero = static_cast<T>(0);
+  if (!g->centered) {
+    const size_t zoff = static_cast<size_t>(iz) * H * H;
+    for (int e = tid; e < H * H; e += nth) {
+      T va = srca[zoff + e];
+      T vb = has_b ? srcb[zoff + e] : zero;
+      if (USE_E) { va *= Ea[zoff + e]; if (has_b) vb *= Eb[zoff + e]; }
+      buf[(e / H) * S + (e % H)] = mk<C>(va, vb);
+    }
+  } else {
+    constexpr int M = 2 * H;
+    const C* ftx = tables + g->ftw_off[0];
+    const C ftz = tables[g->ftw_off[2] + iz];
+    for (int e = tid; e < H * H; e += nth) {
+      const int ix = e % H, iy = e / H;
+      T va[8], vb[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const size_t idx = (static_cast<size_t>(iz + ((k >> 2) & 1) * H) * M + iy + ((k >> 1) & 1) * H) * M + ix + (k & 1) * H;
+        va[k] = srca[idx];
+        vb[k] = has_b ? srcb[idx] : zero;
+        if (USE_E) { va[k] *= Ea[idx]; if (has_b) vb[k] *= Eb[idx]; }
+      }
+      wht8(va);
+      wht8(vb);
+      const C tx = ftx[ix], ty = ftx[iy];  // cubic: the y fold twiddle table equals x's
+      for (int c = 0; c < nch; ++c) {
+        const int o = g->off_idx[c];
+        C w = mk<C>(static_cast<T>(1), zero);
+        if (o & 1) w = tx;
+        if (o & 2) w = cmul(w, ty);
+        if (o & 4) w = cmul(w, ftz);
+        buf[c * PL + iy * S + ix] = cmul(mk<C>(va[o], vb[o]), w);
+      }
+    }
+  }
+  __syncthreads();
+  smem_lines<C, false, H>(buf, nch * H, nch * H, 0, S, 1);   // x lines (rows)
+  __syncthreads();
+  smem_lines<C, false, H>(buf, nch * H, H, PL, 1, S);         // y lines (columns)
+  __syncthreads();
+  const size_t hvol = static_cast<size_t>(H) * H * H;
+  for (int c = 0; c < nch; ++c) {
+    C* dst = W + (static_cast<size_t>(slot) * nch + c) * hvol + static_cast<size_t>(iz) * H * H;
+    for (int e = tid; e < H * H; e += nth) dst[e] = buf[c * PL + (e / H) * S + (e % H)];
+  }
+}
+
+// Backward plane kernel, cubic H: inverse x/y FFT of W[slot][c][iz] + unfold of the two
+// fields (real part -> field a, imaginary part -> field b).
+template <typename T, int H, bool USE_E>
+__global__ void k_plane_bwd_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                              const typename Cx<T>::type* __restrict__ W, const T* __restrict__ E, T* __restrict__ f0,
+                              int nfields) {
+  using C = typename Cx<T>::type;
+  constexpr int S = H + 1;
+  constexpr int PL = H * S;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int nch = g->n_ch;
+  const int iz = blockIdx.x, slot = blockIdx.y;
+  const int fa = 2 * slot;
+  const bool has_b = fa + 1 < nfields;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const size_t hvol = static_cast<size_t>(H) * H * H;
+  for (int c = 0; c < nch; ++c) {
+    const C* s = W + (static_cast<size_t>(slot) * nch + c) * hvol + static_cast<size_t>(iz) * H * H;
+    for (int e = tid; e < H * H; e += nth) buf[c * PL + (e / H) * S + (e % H)] = s[e];
+  }
+  __syncthreads();
+  smem_lines<C, true, H>(buf, nch * H, nch * H, 0, S, 1);
+  __syncthreads();
+  smem_lines<C, true, H>(buf, nch * H, H, PL, 1, S);
+  __syncthreads();
+  const size_t mvol = static_cast<size_t>(g->M[0]) * g->M[1] * g->M[2];
+  T* dsta = f0 + static_cast<size_t>(fa) * mvol;
+  T* dstb = dsta + mvol;
+  const T* Ea = USE_E ? E + static_cast<size_t>(fa) * mvol : nullptr;
+  const T* Eb = USE_E ? Ea + mvol : nullptr;
+  if (!g->centered) {
+    const T scale = static_cast<T>(1.0 / static_cast<double>(mvol));
+    const size_t zoff = static_cast<size_t>(iz) * H * H;
+    for (int e = tid; e < H * H; e += nth) {
+      const C x = buf[(e / H) * S + (e % H)];
+      T va = x.x * scale, vb = x.y * scale;
+      if (USE_E) { va *= Ea[zoff + e]; if (has_b) vb *= Eb[zoff + e]; }
+      dsta[zoff + e] = va;
+      if (has_b) dstb[zoff + e] = vb;
+    }
+  } else {
+    constexpr int M = 2 * H;
+    const T scale = static_cast<T>(1.0 / (8.0 * static_cast<double>(hvol)));
+    const C* ftx = tables + g->ftw_off[0];
+    const C ftz = tables[g->ftw_off[2] + iz];
+    for (int e = tid; e < H * H; e += nth) {
+      const int ix = e % H, iy = e / H;
+      T va[8], vb[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) { va[k] = static_cast<T>(0); vb[k] = static_cast<T>(0); }
+      const C tx = ftx[ix], ty = ftx[iy];
+      for (int c = 0; c < nch; ++c) {
+        const int o = g->off_idx[c];
+        C w = mk<C>(static_cast<T>(1), static_cast<T>(0));
+        if (o & 1) w = tx;
+        if (o & 2) w = cmul(w, ty);
+        if (o & 4) w = cmul(w, ftz);
+        const C y = cmulc(buf[c * PL + iy * S + ix], w);  // x * conj(w)
+        va[o] = y.x;
+        vb[o] = y.y;
+      }
+      wht8(va);
+      wht8(vb);
+#pragma unroll
+      for (int k = 0; k < 8; ++k) {
+        const size_t idx = (static_cast<size_t>(iz + ((k >> 2) & 1) * H) * M + iy + ((k >> 1) & 1) * H) * M + ix + (k & 1) * H;
+        T a = va[k] * scale, bq = vb[k] * scale;
+        if (USE_E) { a *= Ea[idx]; if (has_b) bq *= Eb[idx]; }
+        dsta[idx] = a;
+        if (has_b) dstb[idx] = bq;
+      }
+    }
+  }
+}
+
+constexpr int kZB = 4;  // xz-planes (y values) per CTA in the z kernels
+
+// Forward z FFT, cubic H: W[slot][c][z][y][x] (in) -> WT[slot][c][x][y][z] (z fastest,
+// out, same storage: each CTA reads and writes exactly the same addresses).
+template <typename T, int H>
+__global__ void k_fft_z_fwd_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* W,
+                              typename Cx<T>::type* WT) {
+  using C = typename Cx<T>::type;
+  constexpr int S = H + 1;
+  constexpr int PL = H * S;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);  // [yy][z][x]
+  const int y0 = blockIdx.x * kZB, c = blockIdx.y, slot = blockIdx.z;
+  const int ny = min(kZB, H - y0);
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const size_t hvol = static_cast<size_t>(H) * H * H;
+  const C* src = W + (static_cast<size_t>(slot) * g->n_ch + c) * hvol;
+  for (int e = tid; e < ny * H * H; e += nth) {
+    const int x = e % H, z = (e / H) % H, yy = e / (H * H);
+    buf[yy * PL + z * S + x] = src[(static_cast<size_t>(z) * H + y0 + yy) * H + x];
+  }
+  __syncthreads();
+  smem_lines<C, false, H>(buf, ny * H, H, PL, 1, S);  // z lines: element stride S
+  __syncthreads();
+  C* dst = WT + (static_cast<size_t>(slot) * g->n_ch + c) * hvol;
+  for (int e = tid; e < ny * H * H; e += nth) {
+    const int z = e % H, yy = (e / H) % ny, x = e / (H * ny);
+    dst[(static_cast<size_t>(x) * H + y0 + yy) * H + z] = buf[yy * PL + z * S + x];
+  }
+}
+
+// Backward: expand G0 from orbit representatives (ET table) + inverse z FFT, cubic H:
+// G0R[slot][o] -> W[slot][c][z][y][x].
+template <typename T, int H>
+__global__ void k_expand_ifft_z_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                                  const int2* __restrict__ ET, const typename Cx<T>::type* __restrict__ G0R,
+                                  typename Cx<T>::type* __restrict__ W) {
+  using C = typename Cx<T>::type;
+  constexpr int S = H + 1;
+  constexpr int PL = H * S;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int y0 = blockIdx.x * kZB, c = blockIdx.y, slot = blockIdx.z;
+  const int ny = min(kZB, H - y0);
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const size_t hvol = static_cast<size_t>(H) * H * H;
+  const int2* et = ET + static_cast<size_t>(c) * hvol;
+  const C* rep = G0R + static_cast<size_t>(slot) * g->n_orbits;
+  const C* ph = tables + g->ph_off;
+  for (int e = tid; e < ny * H * H; e += nth) {
+    const int x = e % H, z = (e / H) % H, yy = e / (H * H);
+    const int2 t = et[(static_cast<size_t>(z) * H + y0 + yy) * H + x];
+    buf[yy * PL + z * S + x] = cmulc(rep[t.x], ph[t.y]);  // G0R * e^{+2 pi i j/P}
+  }
+  __syncthreads();
+  smem_lines<C, true, H>(buf, ny * H, H, PL, 1, S);
+  __syncthreads();
+  C* dst = W + (static_cast<size_t>(slot) * g->n_ch + c) * hvol;
+  for (int e = tid; e < ny * H * H; e += nth) {
+    const int x = e % H, z = (e / H) % H, yy = e / (H * H);
+    dst[(static_cast<size_t>(z) * H + y0 + yy) * H + x] = buf[yy * PL + z * S + x];
+  }
+}
+
+// Spectral-ASU gather from the z-fastest packed workspace, cubic M (= 2H centred,
+// = H plain); separates the two fields of the slot on the fly.
+template <typename T, int M, bool USE_K>
+__global__ void k_recon_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                          const uint32_t* __restrict__ spec_h, const T* __restrict__ K,
+                          const typename Cx<T>::type* __restrict__ WT, typename Cx<T>::type* __restrict__ F,
+                          int nfields) {
+  using C = typename Cx<T>::type;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int slot = blockIdx.y;
+  if (s >= g->n_spec) return;
+  const int fa = 2 * slot;
+  const bool has_b = fa + 1 < nfields;
+  const uint32_t hp = spec_h[s];
+  const int h0 = static_cast<int>(hp & 1023u), h1 = static_cast<int>((hp >> 10) & 1023u), h2 = static_cast<int>((hp >> 20) & 1023u);
+  const bool cen = g->centered;
+  const int Hc = cen ? M / 2 : M;
+  const size_t hvol = static_cast<size_t>(Hc) * Hc * Hc;
+  const C* Wb = WT + static_cast<size_t>(slot) * g->n_ch * hvol;
+  const C* ph = tables + g->ph_off;
+  const int P = g->P, pmask = g->pmask;
+  const T half = static_cast<T>(0.5);
+  C acca = mk<C>(static_cast<T>(0), static_cast<T>(0));
+  C accb = acca;
+  for (int r = 0; r < g->d; ++r) {
+    int q[3], qn[3];
+#pragma unroll
+    for (int dd = 0; dd < 3; ++dd) {
+      int v = g->rep_R[r][dd] * h0 + g->rep_R[r][3 + dd] * h1 + g->rep_R[r][6 + dd] * h2;
+      v %= M;
+      q[dd] = v < 0 ? v + M : v;
+      qn[dd] = q[dd] == 0 ? 0 : M - q[dd];
+    }
+    size_t idx, idn;
+    if (cen) {
+      const int c = g->chan_of_parity[(q[0] & 1) + 2 * (q[1] & 1) + 4 * (q[2] & 1)];
+      if (c < 0) continue;
+      idx = static_cast<size_t>(c) * hvol + (static_cast<size_t>(q[0] >> 1) * Hc + (q[1] >> 1)) * Hc + (q[2] >> 1);
+      idn = static_cast<size_t>(c) * hvol + (static_cast<size_t>(qn[0] >> 1) * Hc + (qn[1] >> 1)) * Hc + (qn[2] >> 1);
+    } else {
+      idx = (static_cast<size_t>(q[0]) * Hc + q[1]) * Hc + q[2];
+      idn = (static_cast<size_t>(qn[0]) * Hc + qn[1]) * Hc + qn[2];
+    }
+    const C X = Wb[idx], Xn = Wb[idn];
+    // G_a = (X + conj Xn)/2 ; G_b = (X - conj Xn)/(2i)
+    const C Ga = mk<C>(half * (X.x + Xn.x), half * (X.y - Xn.y));
+    const C Gb = mk<C>(half * (X.y + Xn.y), half * (Xn.x - X.x));
+    int j = h0 * g->rep_tp[r][0] + h1 * g->rep_tp[r][1] + h2 * g->rep_tp[r][2];
+    j = pmask >= 0 ? (j & pmask) : ((j % P) + P) % P;
+    const C w = ph[j];
+    acca = cadd(acca, cmul(Ga, w));
+    accb = cadd(accb, cmul(Gb, w));
+  }
+  if (USE_K) { acca = cscale(acca, K[s]); accb = cscale(accb, K[s]); }
+  F[static_cast<size_t>(fa) * g->n_spec + s] = acca;
+  if (has_b) F[static_cast<size_t>(fa + 1) * g->n_spec + s] = accb;
+}
+
+// G0 at orbit representatives of the two fields of a slot, packed as G_a + i G_b.
+template <typename T>
+__global__ void k_inv_recon_reps(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                                 const int32_t* __restrict__ inv_spec, const int32_t* __restrict__ inv_phase,
+                                 const typename Cx<T>::type* __restrict__ F, typename Cx<T>::type* __restrict__ G0R,
+                                 int nfields) {
+  using C = typename Cx<T>::type;
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  const int slot = blockIdx.y;
+  if (o >= g->n_orbits) return;
+  const int fa = 2 * slot;
+  const bool has_b = fa + 1 < nfields;
+  const int d = g->d;
+  const C* Fa = F + static_cast<size_t>(fa) * g->n_spec;
+  const C* Fb = Fa + g->n_spec;
+  const C* ph = tables + g->ph_off;
+  C acca = mk<C>(static_cast<T>(0), static_cast<T>(0));
+  C accb = acca;
+  for (int a = 0; a < d; ++a) {
+    const int s = inv_spec[static_cast<size_t>(o) * d + a];
+    if (s == 0) continue;
+    const int si = (s > 0 ? s : -s) - 1;
+    const C w = ph[inv_phase[static_cast<size_t>(o) * d + a]];
+    C fa_v = Fa[si];
+    if (s < 0) fa_v = cconj(fa_v);
+    acca = cadd(acca, cmulc(fa_v, w));
+    if (has_b) {
+      C fb_v = Fb[si];
+      if (s < 0) fb_v = cconj(fb_v);
+      accb = cadd(accb, cmulc(fb_v, w));
+    }
+  }
+  const T inv_d = static_cast<T>(1.0 / static_cast<double>(d));
+  // X = G_a + i G_b
+  G0R[static_cast<size_t>(slot) * g->n_orbits + o] = mk<C>(inv_d * (acca.x - accb.y), inv_d * (acca.y + accb.x));
 }
 
 // ---------------------------------------------------------------- elementwise
@@ -546,28 +931,157 @@ std::vector<unsigned char> make_table_bytes(const Plan& p, DevGeom* g) {
   return bytes;
 }
 
+// Compile-time sized kernels are instantiated for these cubic channel-grid edges.
+template <typename T> constexpr bool fast_ok(int H) {
+  return H == 4 || H == 6 || H == 8 || H == 12 || H == 16 || H == 24 || H == 32 || (H == 48 && sizeof(T) == 4);
+}
+
+#define CFFT_FOR_H(H, ...)                                        \
+  switch (H) {                                                     \
+    case 4: { constexpr int HH = 4; __VA_ARGS__; } break;                 \
+    case 6: { constexpr int HH = 6; __VA_ARGS__; } break;                 \
+    case 8: { constexpr int HH = 8; __VA_ARGS__; } break;                 \
+    case 12: { constexpr int HH = 12; __VA_ARGS__; } break;               \
+    case 16: { constexpr int HH = 16; __VA_ARGS__; } break;               \
+    case 24: { constexpr int HH = 24; __VA_ARGS__; } break;               \
+    case 32: { constexpr int HH = 32; __VA_ARGS__; } break;               \
+    default: { constexpr int HH = 48; __VA_ARGS__; } break;               \
+  }
+
+#define CFFT_FOR_M(M, ...)                                        \
+  switch (M) {                                                     \
+    case 4: { constexpr int MM = 4; __VA_ARGS__; } break;                 \
+    case 6: { constexpr int MM = 6; __VA_ARGS__; } break;                 \
+    case 8: { constexpr int MM = 8; __VA_ARGS__; } break;                 \
+    case 12: { constexpr int MM = 12; __VA_ARGS__; } break;               \
+    case 16: { constexpr int MM = 16; __VA_ARGS__; } break;               \
+    case 24: { constexpr int MM = 24; __VA_ARGS__; } break;               \
+    case 32: { constexpr int MM = 32; __VA_ARGS__; } break;               \
+    case 48: { constexpr int MM = 48; __VA_ARGS__; } break;               \
+    case 64: { constexpr int MM = 64; __VA_ARGS__; } break;               \
+    default: { constexpr int MM = 96; __VA_ARGS__; } break;               \
+  }
+
+template <typename T>
+void set_fast_attrs() {
+  for (int H : {4, 6, 8, 12, 16, 24, 32, 48}) {
+    if (!fast_ok<T>(H)) continue;
+    CFFT_FOR_H(H, {
+      cudaFuncSetAttribute(k_plane_fwd_h<T, HH, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+      cudaFuncSetAttribute(k_plane_fwd_h<T, HH, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+      cudaFuncSetAttribute(k_plane_bwd_h<T, HH, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+      cudaFuncSetAttribute(k_plane_bwd_h<T, HH, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+      cudaFuncSetAttribute(k_fft_z_fwd_h<T, HH>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+      cudaFuncSetAttribute(k_expand_ifft_z_h<T, HH>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+    });
+  }
+}
+
+// Constant-memory twiddles e^{-2 pi i j / N} for the register FFTs (FP64 values rounded).
+Status upload_const_twiddles(std::string* err) {
+  static std::mutex mu;
+  static bool done[64] = {false};
+  int dev = 0;
+  CFFT_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && dev < 64 && done[dev]) return Status::kOk;
+  std::vector<float2> tf(kTwTotal);
+  std::vector<double2> td(kTwTotal);
+  const int sizes[8] = {4, 6, 8, 12, 16, 24, 32, 48};
+  const int offs[8] = {kTwOff4, kTwOff6, kTwOff8, kTwOff12, kTwOff16, kTwOff24, kTwOff32, kTwOff48};
+  for (int k = 0; k < 8; ++k)
+    for (int j = 0; j < sizes[k]; ++j) {
+      const double c = std::cos(2.0 * M_PI * j / sizes[k]), sn = -std::sin(2.0 * M_PI * j / sizes[k]);
+      td[offs[k] + j] = make_double2(c, sn);
+      tf[offs[k] + j] = make_float2(static_cast<float>(c), static_cast<float>(sn));
+    }
+  CFFT_CUDA(cudaMemcpyToSymbol(c_tw_f, tf.data(), sizeof(float2) * kTwTotal), "upload twiddles");
+  CFFT_CUDA(cudaMemcpyToSymbol(c_tw_d, td.data(), sizeof(double2) * kTwTotal), "upload twiddles");
+  set_fast_attrs<float>();
+  set_fast_attrs<double>();
+  CFFT_CUDA(cudaGetLastError(), "set shared-memory attributes");
+  if (dev >= 0 && dev < 64) done[dev] = true;
+  return Status::kOk;
+}
+
 // Stages of one forward + backward: 0 plane/fold + x/y FFT, 1 z FFT, 2 reconstruct,
-// 3 inverse reconstruct + orbit expansion, 4 inverse z FFT, 5 inverse x/y FFT + unfold.
+// 3 inverse reconstruct (+ orbit expansion), 4 inverse z FFT, 5 inverse x/y FFT + unfold.
+// `nb` fields starting at the caller's pointers; the workspace holds one chunk.
 template <typename T>
 void launch_stage(Plan* p, int stage, const T* f0, typename Cx<T>::type* F, const typename Cx<T>::type* Fin,
-                  T* f0_out, const T* E, bool use_K, int B, cudaStream_t st) {
+                  T* f0_out, const T* E, bool use_K, int nb, cudaStream_t st) {
   using C = typename Cx<T>::type;
   const DevGeom* g = static_cast<const DevGeom*>(p->d_geom);
   const C* tab = static_cast<const C*>(p->d_tables);
   C* W = static_cast<C*>(p->d_work_T);
   const PlanTables& T_ = p->T;
+  const int H = p->fast_h;
+  const size_t cs = sizeof(C);
+  if (H > 0) {
+    const int nch = T_.n_ch;
+    const int nslots = (nb + 1) / 2;
+    const int thr_plane = std::max(128, ((nch * H + 31) / 32) * 32);
+    const size_t smem_plane = static_cast<size_t>(nch) * H * (H + 1) * cs;
+    const int thr_z = std::max(64, ((kZB * H + 31) / 32) * 32);
+    const size_t smem_z = static_cast<size_t>(kZB) * H * (H + 1) * cs;
+    const dim3 gz((H + kZB - 1) / kZB, nch, nslots);
+    switch (stage) {
+      case 0:
+        CFFT_FOR_H(H, {
+          if (E) k_plane_fwd_h<T, HH, true><<<dim3(H, nslots), thr_plane, smem_plane, st>>>(g, tab, f0, E, W, nb);
+          else k_plane_fwd_h<T, HH, false><<<dim3(H, nslots), thr_plane, smem_plane, st>>>(g, tab, f0, nullptr, W, nb);
+        });
+        break;
+      case 1:
+        CFFT_FOR_H(H, { k_fft_z_fwd_h<T, HH><<<gz, thr_z, smem_z, st>>>(g, W, W); });
+        break;
+      case 2: {
+        const int ns = static_cast<int>(T_.spec.size());
+        const dim3 gr((ns + 255) / 256, nslots);
+        const int M = T_.centered ? 2 * H : H;
+        const T* K = static_cast<const T*>(p->d_K);
+        const uint32_t* sh = static_cast<const uint32_t*>(p->d_spec_h);
+        CFFT_FOR_M(M, {
+          if (use_K) k_recon_h<T, MM, true><<<gr, 256, 0, st>>>(g, tab, sh, K, W, F, nb);
+          else k_recon_h<T, MM, false><<<gr, 256, 0, st>>>(g, tab, sh, nullptr, W, F, nb);
+        });
+        break;
+      }
+      case 3: {
+        const int no = static_cast<int>(T_.orbit_rep.size());
+        k_inv_recon_reps<T><<<dim3((no + 127) / 128, nslots), 128, 0, st>>>(
+            g, tab, static_cast<const int32_t*>(p->d_inv_spec), static_cast<const int32_t*>(p->d_inv_phase), Fin,
+            static_cast<C*>(p->d_g0r), nb);
+        break;
+      }
+      case 4:
+        CFFT_FOR_H(H, {
+          k_expand_ifft_z_h<T, HH><<<gz, thr_z, smem_z, st>>>(g, tab, static_cast<const int2*>(p->d_expand),
+                                                              static_cast<const C*>(p->d_g0r), W);
+        });
+        break;
+      default:
+        CFFT_FOR_H(H, {
+          if (E) k_plane_bwd_h<T, HH, true><<<dim3(H, nslots), thr_plane, smem_plane, st>>>(g, tab, W, E, f0_out, nb);
+          else k_plane_bwd_h<T, HH, false><<<dim3(H, nslots), thr_plane, smem_plane, st>>>(g, tab, W, nullptr, f0_out, nb);
+        });
+        break;
+    }
+    ++g_launches;
+    return;
+  }
   switch (stage) {
     case 0:
-      if (E) k_plane_fwd<T, true><<<dim3(T_.H[2], B), p->threads_xy, p->smem_xy, st>>>(g, tab, f0, E, W);
-      else k_plane_fwd<T, false><<<dim3(T_.H[2], B), p->threads_xy, p->smem_xy, st>>>(g, tab, f0, nullptr, W);
+      if (E) k_plane_fwd<T, true><<<dim3(T_.H[2], nb), p->threads_xy, p->smem_xy, st>>>(g, tab, f0, E, W);
+      else k_plane_fwd<T, false><<<dim3(T_.H[2], nb), p->threads_xy, p->smem_xy, st>>>(g, tab, f0, nullptr, W);
       break;
     case 1:
       if (T_.H[2] <= 1) return;
-      k_fft_z<T, false><<<dim3(T_.H[1], T_.n_ch, B), p->threads_z, p->smem_z, st>>>(g, tab, W);
+      k_fft_z<T, false><<<dim3(T_.H[1], T_.n_ch, nb), p->threads_z, p->smem_z, st>>>(g, tab, W);
       break;
     case 2: {
       const int ns = static_cast<int>(T_.spec.size());
-      const dim3 gr((ns + 255) / 256, B);
+      const dim3 gr((ns + 255) / 256, nb);
       if (use_K)
         k_recon<T, true><<<gr, 256, 0, st>>>(g, tab, static_cast<const uint32_t*>(p->d_spec_h), static_cast<const T*>(p->d_K), W, F);
       else
@@ -576,36 +1090,42 @@ void launch_stage(Plan* p, int stage, const T* f0, typename Cx<T>::type* F, cons
     }
     case 3: {
       const int no = static_cast<int>(T_.orbit_rep.size());
-      k_inv_recon<T><<<dim3((no + 127) / 128, B), 128, 0, st>>>(
+      k_inv_recon<T><<<dim3((no + 127) / 128, nb), 128, 0, st>>>(
           g, tab, static_cast<const int32_t*>(p->d_orbit_rep), static_cast<const int32_t*>(p->d_inv_spec),
           static_cast<const int32_t*>(p->d_inv_phase), static_cast<const uint32_t*>(p->d_img_mask), Fin, W);
       break;
     }
     case 4:
       if (T_.H[2] <= 1) return;
-      k_fft_z<T, true><<<dim3(T_.H[1], T_.n_ch, B), p->threads_z, p->smem_z, st>>>(g, tab, W);
+      k_fft_z<T, true><<<dim3(T_.H[1], T_.n_ch, nb), p->threads_z, p->smem_z, st>>>(g, tab, W);
       break;
     default:
-      if (E) k_plane_bwd<T, true><<<dim3(T_.H[2], B), p->threads_xy, p->smem_xy, st>>>(g, tab, W, E, f0_out);
-      else k_plane_bwd<T, false><<<dim3(T_.H[2], B), p->threads_xy, p->smem_xy, st>>>(g, tab, W, nullptr, f0_out);
+      if (E) k_plane_bwd<T, true><<<dim3(T_.H[2], nb), p->threads_xy, p->smem_xy, st>>>(g, tab, W, E, f0_out);
+      else k_plane_bwd<T, false><<<dim3(T_.H[2], nb), p->threads_xy, p->smem_xy, st>>>(g, tab, W, nullptr, f0_out);
       break;
   }
   ++g_launches;
 }
 
+// Forward and/or backward over B fields in workspace-sized chunks.  F holds the
+// spectra of all B fields (the forward output, the backward input).
 template <typename T>
-Status launch_forward(Plan* p, const T* f0, typename Cx<T>::type* F, const T* E, bool use_K, int B,
-                      cudaStream_t st, std::string* err) {
-  for (int s = 0; s < 3; ++s) launch_stage<T>(p, s, f0, F, nullptr, nullptr, E, use_K, B, st);
-  CFFT_CUDA(cudaGetLastError(), "forward launch");
-  return Status::kOk;
-}
-
-template <typename T>
-Status launch_backward(Plan* p, const typename Cx<T>::type* F, T* f0, const T* E, int B, cudaStream_t st,
-                       std::string* err) {
-  for (int s = 3; s < 6; ++s) launch_stage<T>(p, s, nullptr, nullptr, F, f0, E, false, B, st);
-  CFFT_CUDA(cudaGetLastError(), "backward launch");
+Status run_chunks(Plan* p, bool fwd, bool bwd, const T* f0, typename Cx<T>::type* F, T* f0_out, const T* E,
+                  bool use_K, int B, cudaStream_t st, std::string* err) {
+  const size_t mvol = static_cast<size_t>(p->T.M[0]) * p->T.M[1] * p->T.M[2];
+  const size_t ns = p->T.spec.size();
+  for (int b0 = 0; b0 < B; b0 += p->chunk) {
+    const int nb = std::min(p->chunk, B - b0);
+    const T* fin = f0 ? f0 + b0 * mvol : nullptr;
+    T* fout = f0_out ? f0_out + b0 * mvol : nullptr;
+    const T* Ec = E ? E + b0 * mvol : nullptr;
+    auto* Fc = F + b0 * ns;
+    if (fwd)
+      for (int s = 0; s < 3; ++s) launch_stage<T>(p, s, fin, Fc, nullptr, nullptr, Ec, use_K, nb, st);
+    if (bwd)
+      for (int s = 3; s < 6; ++s) launch_stage<T>(p, s, nullptr, nullptr, Fc, fout, Ec, false, nb, st);
+  }
+  CFFT_CUDA(cudaGetLastError(), fwd ? "forward launch" : "backward launch");
   return Status::kOk;
 }
 
@@ -614,14 +1134,24 @@ Status profile_roundtrip(Plan* p, const T* f0, typename Cx<T>::type* F, T* f0_ou
                          float* ms, int* n, std::string* err) {
   cudaEvent_t ev[7];
   for (int i = 0; i < 7; ++i) CFFT_CUDA(cudaEventCreate(&ev[i]), "event create");
-  CFFT_CUDA(cudaEventRecord(ev[0], st), "event record");
-  for (int s = 0; s < 6; ++s) {
-    launch_stage<T>(p, s, f0, F, F, f0_out, nullptr, false, B, st);
-    CFFT_CUDA(cudaEventRecord(ev[s + 1], st), "event record");
+  for (int s = 0; s < 6; ++s) ms[s] = 0.f;
+  const size_t mvol = static_cast<size_t>(p->T.M[0]) * p->T.M[1] * p->T.M[2];
+  const size_t ns = p->T.spec.size();
+  for (int b0 = 0; b0 < B; b0 += p->chunk) {
+    const int nb = std::min(p->chunk, B - b0);
+    CFFT_CUDA(cudaEventRecord(ev[0], st), "event record");
+    for (int s = 0; s < 6; ++s) {
+      launch_stage<T>(p, s, f0 + b0 * mvol, F + b0 * ns, F + b0 * ns, f0_out + b0 * mvol, nullptr, false, nb, st);
+      CFFT_CUDA(cudaEventRecord(ev[s + 1], st), "event record");
+    }
+    CFFT_CUDA(cudaGetLastError(), "profile launch");
+    CFFT_CUDA(cudaEventSynchronize(ev[6]), "event sync");
+    for (int s = 0; s < 6; ++s) {
+      float t = 0.f;
+      CFFT_CUDA(cudaEventElapsedTime(&t, ev[s], ev[s + 1]), "elapsed");
+      ms[s] += t;
+    }
   }
-  CFFT_CUDA(cudaGetLastError(), "profile launch");
-  CFFT_CUDA(cudaEventSynchronize(ev[6]), "event sync");
-  for (int s = 0; s < 6; ++s) CFFT_CUDA(cudaEventElapsedTime(&ms[s], ev[s], ev[s + 1]), "elapsed");
   *n = 6;
   for (int i = 0; i < 7; ++i) cudaEventDestroy(ev[i]);
   return Status::kOk;
@@ -649,6 +1179,7 @@ Status plan_device_init(Plan* p, std::string* err) {
     if (!factor_radices(T.H[d], &g.nf[d], g.radix[d])) { *err = "FFT length must factor into 2, 3, 5"; return Status::kUnsupported; }
   }
   g.P = T.P; g.d = T.d; g.n_ch = T.n_ch; g.centered = T.centered ? 1 : 0;
+  g.pmask = (T.P & (T.P - 1)) == 0 ? T.P - 1 : -1;
   g.n_spec = static_cast<int>(T.spec.size());
   g.n_orbits = static_cast<int>(T.orbit_rep.size());
   g.n_rem = static_cast<int>(T.rem_ops.size());
@@ -662,32 +1193,61 @@ Status plan_device_init(Plan* p, std::string* err) {
   for (int r = 0; r < T.d; ++r) {
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j) g.rep_R[r][i * 3 + j] = T.rep_ops[r].R[i][j];
-    for (int i = 0; i < 3; ++i) g.rep_t[r][i] = T.rep_ops[r].t[i];
+    for (int i = 0; i < 3; ++i) {
+      g.rep_t[r][i] = T.rep_ops[r].t[i];
+      g.rep_tp[r][i] = T.rep_ops[r].t[i] * (T.P / T.N[i]);
+    }
   }
   for (int r = 0; r < g.n_rem; ++r) {
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j) g.rem_R[r][i * 3 + j] = T.rem_ops[r].R[i][j];
     for (int i = 0; i < 3; ++i) g.rem_s[r][i] = T.rem_ops[r].t[i];
   }
+  // Fast (compile-time sized) path for cubic channel grids.
+  const bool cubic = T.H[0] == T.H[1] && T.H[1] == T.H[2];
+  p->fast_h = (cubic && (p->precision == 8 ? fast_ok<double>(T.H[0]) : fast_ok<float>(T.H[0]))) ? T.H[0] : 0;
+  if (const char* f = std::getenv("CFFT_DISABLE_FAST")) {
+    if (f[0] == '1') p->fast_h = 0;
+  }
   // distinct-image masks: op i contributes only if no earlier op maps the representative to the same point
   std::vector<uint32_t> masks(static_cast<size_t>(g.n_orbits) * p->n_mask_words, 0u);
+  const size_t hvol = static_cast<size_t>(T.H[0]) * T.H[1] * T.H[2];
+  std::vector<int2> expand;
+  if (p->fast_h) expand.assign(static_cast<size_t>(T.n_ch) * hvol, make_int2(-1, 0));
   for (int o = 0; o < g.n_orbits; ++o) {
     const int m = T.orbit_rep[o];
     const int q[3] = {m % T.M[0], (m / T.M[0]) % T.M[1], m / (T.M[0] * T.M[1])};
     std::vector<long> seen;
     for (int i = 0; i < g.n_rem; ++i) {
       long li = 0, stride = 1;
+      int qq[3];
       for (int dd = 0; dd < 3; ++dd) {
         long v = 0;
         for (int d2 = 0; d2 < 3; ++d2) v += static_cast<long>(T.rem_ops[i].R[d2][dd]) * q[d2];
-        li += floor_mod(v, T.M[dd]) * stride;
+        qq[dd] = static_cast<int>(floor_mod(v, T.M[dd]));
+        li += qq[dd] * stride;
         stride *= T.M[dd];
       }
       if (std::find(seen.begin(), seen.end(), li) != seen.end()) continue;
       seen.push_back(li);
       masks[static_cast<size_t>(o) * p->n_mask_words + (i >> 5)] |= 1u << (i & 31);
+      if (p->fast_h) {
+        long j = 0;
+        for (int dd = 0; dd < 3; ++dd) j += static_cast<long>(q[dd]) * T.rem_ops[i].t[dd] * (T.P / T.M[dd]);
+        size_t pos;
+        if (T.centered) {
+          const int c = T.chan_of_parity[(qq[0] & 1) + 2 * (qq[1] & 1) + 4 * (qq[2] & 1)];
+          if (c < 0) { *err = "orbit image outside the alive channels"; return Status::kInvalid; }
+          pos = static_cast<size_t>(c) * hvol + (static_cast<size_t>(qq[2] >> 1) * T.H[1] + (qq[1] >> 1)) * T.H[0] + (qq[0] >> 1);
+        } else {
+          pos = (static_cast<size_t>(qq[2]) * T.H[1] + qq[1]) * T.H[0] + qq[0];
+        }
+        expand[pos] = make_int2(o, static_cast<int>(floor_mod(j, T.P)));
+      }
     }
   }
+  for (const int2& e : expand)
+    if (e.x < 0) { *err = "orbit expansion does not cover the channel grid"; return Status::kInvalid; }
   std::vector<uint32_t> hp(T.spec.size());
   for (size_t s = 0; s < T.spec.size(); ++s)
     hp[s] = static_cast<uint32_t>(T.spec[s].h[0]) | (static_cast<uint32_t>(T.spec[s].h[1]) << 10) |
@@ -696,17 +1256,25 @@ Status plan_device_init(Plan* p, std::string* err) {
 
   const size_t rs = p->precision;          // real size
   const size_t cs = 2 * rs;                // complex size
-  const size_t hvol = static_cast<size_t>(T.H[0]) * T.H[1] * T.H[2];
   const size_t mvol = static_cast<size_t>(T.M[0]) * T.M[1] * T.M[2];
   const size_t B = p->max_batch;
-  // launch geometry and shared memory
+  // Chunk the batch: each chunk's channel workspace is at most `budget` bytes (64 MiB by
+  // default; measured: fewer, larger launches beat keeping the workspace L2-resident).
+  // On the fast path two fields share one workspace slot, and chunks hold whole pairs.
+  size_t budget = static_cast<size_t>(64) << 20;
+  if (const char* cb = std::getenv("CFFT_CHUNK_BYTES")) budget = std::strtoull(cb, nullptr, 10);
+  const size_t per_field = T.n_ch * hvol * cs / (p->fast_h ? 2 : 1);
+  size_t ch = std::max<size_t>(1, std::min<size_t>(B, budget / std::max<size_t>(per_field, 1)));
+  if (p->fast_h && ch < B && ch > 1) ch &= ~static_cast<size_t>(1);
+  p->chunk = static_cast<int>(ch);
+  // launch geometry and shared memory (generic path)
   const long pe = static_cast<long>(T.n_ch) * T.H[0] * T.H[1];
   const long ze = static_cast<long>(T.H[0]) * T.H[2];
   p->threads_xy = round_threads(pe);
   p->threads_z = round_threads(ze);
   p->smem_xy = (2 * pe + T.H[0] + T.H[1]) * cs;
   p->smem_z = (2 * ze + T.H[2]) * cs;
-  if (p->smem_xy > 227 * 1024 || p->smem_z > 227 * 1024) { *err = "shared memory above 227 KB"; return Status::kUnsupported; }
+  if (!p->fast_h && (p->smem_xy > 227 * 1024 || p->smem_z > 227 * 1024)) { *err = "shared memory above 227 KB"; return Status::kUnsupported; }
 
   auto alloc = [&](void** ptr, size_t bytes, const char* what) -> Status {
     cudaError_t e = cudaMalloc(ptr, std::max<size_t>(bytes, 16));
@@ -714,6 +1282,7 @@ Status plan_device_init(Plan* p, std::string* err) {
     p->workspace_bytes += bytes;
     return Status::kOk;
   };
+  const size_t chunk = static_cast<size_t>(p->chunk);
   Status st;
   if ((st = alloc(&p->d_geom, sizeof(DevGeom), "geometry")) != Status::kOk) return st;
   if ((st = alloc(&p->d_tables, tab.size(), "tables")) != Status::kOk) return st;
@@ -723,9 +1292,13 @@ Status plan_device_init(Plan* p, std::string* err) {
   if ((st = alloc(&p->d_inv_spec, T.inv_spec.size() * 4, "inverse spec")) != Status::kOk) return st;
   if ((st = alloc(&p->d_inv_phase, T.inv_phase.size() * 4, "inverse phase")) != Status::kOk) return st;
   if ((st = alloc(&p->d_img_mask, masks.size() * 4, "image masks")) != Status::kOk) return st;
-  if ((st = alloc(&p->d_work_T, B * T.n_ch * hvol * cs, "channel workspace")) != Status::kOk) return st;
+  if ((st = alloc(&p->d_work_T, chunk * T.n_ch * hvol * cs, "channel workspace")) != Status::kOk) return st;
   if ((st = alloc(&p->d_work_F, B * T.spec.size() * cs, "spectrum workspace")) != Status::kOk) return st;
   if ((st = alloc(&p->d_work_E, B * mvol * rs, "interaction workspace")) != Status::kOk) return st;
+  if (p->fast_h) {
+    if ((st = alloc(&p->d_expand, expand.size() * sizeof(int2), "expansion table")) != Status::kOk) return st;
+    if ((st = alloc(&p->d_g0r, chunk * T.orbit_rep.size() * cs, "representative workspace")) != Status::kOk) return st;
+  }
   CFFT_CUDA(cudaMemcpy(p->d_geom, &g, sizeof(g), cudaMemcpyHostToDevice), "upload geometry");
   CFFT_CUDA(cudaMemcpy(p->d_tables, tab.data(), tab.size(), cudaMemcpyHostToDevice), "upload tables");
   CFFT_CUDA(cudaMemcpy(p->d_spec_h, hp.data(), hp.size() * 4, cudaMemcpyHostToDevice), "upload spectral points");
@@ -735,11 +1308,14 @@ Status plan_device_init(Plan* p, std::string* err) {
     CFFT_CUDA(cudaMemcpy(p->d_inv_phase, T.inv_phase.data(), T.inv_phase.size() * 4, cudaMemcpyHostToDevice), "upload inv phase");
     CFFT_CUDA(cudaMemcpy(p->d_img_mask, masks.data(), masks.size() * 4, cudaMemcpyHostToDevice), "upload masks");
   }
+  if (p->fast_h)
+    CFFT_CUDA(cudaMemcpy(p->d_expand, expand.data(), expand.size() * sizeof(int2), cudaMemcpyHostToDevice), "upload expansion");
   // Orbit expansion writes only alive positions; channel positions never written stay zero.
-  CFFT_CUDA(cudaMemset(p->d_work_T, 0, B * T.n_ch * hvol * cs), "clear workspace");
+  CFFT_CUDA(cudaMemset(p->d_work_T, 0, chunk * T.n_ch * hvol * cs), "clear workspace");
   if (p->precision == 8) set_smem_attrs<double>();
   else set_smem_attrs<float>();
   CFFT_CUDA(cudaGetLastError(), "set shared-memory attributes");
+  if ((st = upload_const_twiddles(err)) != Status::kOk) return st;
   cudaStream_t s;
   CFFT_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "create stream");
   p->own_stream = s;
@@ -760,7 +1336,7 @@ Status plan_upload_kernel(Plan* p, std::string* err) {
 void plan_device_free(Plan* p) {
   void** bufs[] = {&p->d_geom, &p->d_tables, &p->d_spec_h, &p->d_K, &p->d_orbit_rep, &p->d_inv_spec,
                    &p->d_inv_phase, &p->d_img_mask, &p->d_fill_map, &p->d_work_T, &p->d_work_F,
-                   &p->d_work_E, &p->d_stage_in, &p->d_stage_out};
+                   &p->d_work_E, &p->d_stage_in, &p->d_stage_out, &p->d_expand, &p->d_g0r};
   for (void** b : bufs)
     if (*b) { cudaFree(*b); *b = nullptr; }
   if (p->own_stream) { cudaStreamDestroy(static_cast<cudaStream_t>(p->own_stream)); p->own_stream = nullptr; }
@@ -772,8 +1348,8 @@ Status exec_forward(Plan* p, const void* f0, void* F, int B, void* stream, std::
   if (!f0 || !F) { *err = "null pointer"; return Status::kInvalid; }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (p->precision == 8)
-    return launch_forward<double>(p, static_cast<const double*>(f0), static_cast<double2*>(F), nullptr, false, B, s, err);
-  return launch_forward<float>(p, static_cast<const float*>(f0), static_cast<float2*>(F), nullptr, false, B, s, err);
+    return run_chunks<double>(p, true, false, static_cast<const double*>(f0), static_cast<double2*>(F), nullptr, nullptr, false, B, s, err);
+  return run_chunks<float>(p, true, false, static_cast<const float*>(f0), static_cast<float2*>(F), nullptr, nullptr, false, B, s, err);
 }
 
 Status exec_profile_roundtrip(Plan* p, const void* f0, void* F, void* f0_out, int B, void* stream, float* ms,
@@ -793,8 +1369,8 @@ Status exec_backward(Plan* p, const void* F, void* f0, int B, void* stream, std:
   if (!f0 || !F) { *err = "null pointer"; return Status::kInvalid; }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (p->precision == 8)
-    return launch_backward<double>(p, static_cast<const double2*>(F), static_cast<double*>(f0), nullptr, B, s, err);
-  return launch_backward<float>(p, static_cast<const float2*>(F), static_cast<float*>(f0), nullptr, B, s, err);
+    return run_chunks<double>(p, false, true, nullptr, const_cast<double2*>(static_cast<const double2*>(F)), static_cast<double*>(f0), nullptr, false, B, s, err);
+  return run_chunks<float>(p, false, true, nullptr, const_cast<float2*>(static_cast<const float2*>(F)), static_cast<float*>(f0), nullptr, false, B, s, err);
 }
 
 Status exec_scft_step(Plan* p, void* f0, int B, void* stream, std::string* err) {
@@ -802,14 +1378,9 @@ Status exec_scft_step(Plan* p, void* f0, int B, void* stream, std::string* err) 
   if (st != Status::kOk) return st;
   if (!f0) { *err = "null pointer"; return Status::kInvalid; }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (p->precision == 8) {
-    st = launch_forward<double>(p, static_cast<const double*>(f0), static_cast<double2*>(p->d_work_F), nullptr, true, B, s, err);
-    if (st != Status::kOk) return st;
-    return launch_backward<double>(p, static_cast<const double2*>(p->d_work_F), static_cast<double*>(f0), nullptr, B, s, err);
-  }
-  st = launch_forward<float>(p, static_cast<const float*>(f0), static_cast<float2*>(p->d_work_F), nullptr, true, B, s, err);
-  if (st != Status::kOk) return st;
-  return launch_backward<float>(p, static_cast<const float2*>(p->d_work_F), static_cast<float*>(f0), nullptr, B, s, err);
+  if (p->precision == 8)
+    return run_chunks<double>(p, true, true, static_cast<const double*>(f0), static_cast<double2*>(p->d_work_F), static_cast<double*>(f0), nullptr, true, B, s, err);
+  return run_chunks<float>(p, true, true, static_cast<const float*>(f0), static_cast<float2*>(p->d_work_F), static_cast<float*>(f0), nullptr, true, B, s, err);
 }
 
 Status exec_step_diffusion(Plan* p, void* q, const void* w, double dt, int n_steps, int B, void* stream,
@@ -824,11 +1395,8 @@ Status exec_step_diffusion(Plan* p, void* q, const void* w, double dt, int n_ste
     k_interaction<double><<<grid, 256, 0, s>>>(static_cast<const double*>(w), static_cast<double*>(p->d_work_E), dt / 2, n);
     ++g_launches;
     for (int i = 0; i < n_steps; ++i) {
-      st = launch_forward<double>(p, static_cast<const double*>(q), static_cast<double2*>(p->d_work_F),
-                                  static_cast<const double*>(p->d_work_E), true, B, s, err);
-      if (st != Status::kOk) return st;
-      st = launch_backward<double>(p, static_cast<const double2*>(p->d_work_F), static_cast<double*>(q),
-                                   static_cast<const double*>(p->d_work_E), B, s, err);
+      st = run_chunks<double>(p, true, true, static_cast<const double*>(q), static_cast<double2*>(p->d_work_F),
+                              static_cast<double*>(q), static_cast<const double*>(p->d_work_E), true, B, s, err);
       if (st != Status::kOk) return st;
     }
   } else {
@@ -836,11 +1404,8 @@ Status exec_step_diffusion(Plan* p, void* q, const void* w, double dt, int n_ste
                                               static_cast<float>(dt / 2), n);
     ++g_launches;
     for (int i = 0; i < n_steps; ++i) {
-      st = launch_forward<float>(p, static_cast<const float*>(q), static_cast<float2*>(p->d_work_F),
-                                 static_cast<const float*>(p->d_work_E), true, B, s, err);
-      if (st != Status::kOk) return st;
-      st = launch_backward<float>(p, static_cast<const float2*>(p->d_work_F), static_cast<float*>(q),
-                                  static_cast<const float*>(p->d_work_E), B, s, err);
+      st = run_chunks<float>(p, true, true, static_cast<const float*>(q), static_cast<float2*>(p->d_work_F),
+                             static_cast<float*>(q), static_cast<const float*>(p->d_work_E), true, B, s, err);
       if (st != Status::kOk) return st;
     }
   }
@@ -1005,13 +1570,17 @@ Status noalloc_forward(const Plan* p, const T* f0, typename Cx<T>::type* F, int 
   if (Tb.d > 8) { *err = "fiber length above 8"; return Status::kUnsupported; }
   if (Tb.P > 8192) { *err = "phase denominator lcm(N) above 8192"; return Status::kUnsupported; }
   g.P = Tb.P; g.d = Tb.d; g.n_ch = Tb.n_ch; g.centered = Tb.centered ? 1 : 0;
+  g.pmask = (Tb.P & (Tb.P - 1)) == 0 ? Tb.P - 1 : -1;
   g.n_spec = static_cast<int>(Tb.spec.size());
   for (int k = 0; k < 8; ++k) g.chan_of_parity[k] = Tb.chan_of_parity[k];
   for (int c = 0; c < Tb.n_ch; ++c) g.off_idx[c] = Tb.offsets[c][0] + 2 * Tb.offsets[c][1] + 4 * Tb.offsets[c][2];
   for (int r = 0; r < Tb.d; ++r) {
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j) g.rep_R[r][i * 3 + j] = Tb.rep_ops[r].R[i][j];
-    for (int i = 0; i < 3; ++i) g.rep_t[r][i] = Tb.rep_ops[r].t[i];
+    for (int i = 0; i < 3; ++i) {
+      g.rep_t[r][i] = Tb.rep_ops[r].t[i];
+      g.rep_tp[r][i] = Tb.rep_ops[r].t[i] * (Tb.P / Tb.N[i]);
+    }
   }
   std::vector<uint32_t> hp(Tb.spec.size());
   for (size_t s = 0; s < Tb.spec.size(); ++s)

@@ -30,10 +30,14 @@ struct Plan {
   void* d_work_E = nullptr;     // B x M-grid real (interaction factors)
   void* d_stage_in = nullptr;   // host-API staging
   void* d_stage_out = nullptr;
+  void* d_expand = nullptr;     // fast path: per channel position (orbit index, phase numerator)
+  void* d_g0r = nullptr;        // fast path: chunk x n_orbits complex (G0 at representatives)
   void* own_stream = nullptr;
   size_t workspace_bytes = 0;
   // launch geometry
   int threads_xy = 0, threads_z = 0;
+  int fast_h = 0;               // cubic channel edge of the compile-time sized kernels (0 = generic)
+  int chunk = 1;                // fields per workspace chunk
   size_t smem_xy = 0, smem_z = 0;
 };
 
