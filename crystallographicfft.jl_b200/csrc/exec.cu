@@ -51,6 +51,10 @@ struct DevGeom {
   int ph_off;              // e^{-2 pi i j / P}, j < P
   int pmask;               // P - 1 when P is a power of two, else -1
   int rep_tp[8][3];        // t_b,d * (P / N_d): phase numerators per unit frequency
+  int rep_perm;            // 1 if every R_b^T is a signed permutation
+  int rep_ps[8][3];        // (R_b^T h)_d = sign * h[src]: packed as src + 4 * (sign < 0)
+  int rep_diag8;           // 1 if d = 8 and the rep ops are the 8 diagonal sign matrices
+  int sign_op[8];          // sign pattern s (bit d = axis d negated) -> representative index
 };
 
 template <typename T> struct Cx;
@@ -531,6 +535,35 @@ __device__ __forceinline__ void smem_lines(C* buf, int count, int group, int gst
 // builds X = G_a + i G_b and the unfold reads field a from the real part and field b
 // from the imaginary part.  This halves the FFT work and the workspace traffic.
 
+// Row / column FFTs of nch padded H x H planes (row stride S = H + 1, plane stride
+// H * S), one thread per line, compile-time strides.
+template <typename C, bool INV, int H>
+__device__ __forceinline__ void smem_rows(C* buf, int nlines) {
+  constexpr int S = H + 1;
+  for (int l = threadIdx.x; l < nlines; l += blockDim.x) {
+    C* p = buf + l * S;
+    C v[H];
+#pragma unroll
+    for (int i = 0; i < H; ++i) v[i] = p[i];
+    reg_fft<C, INV, H>(v);
+#pragma unroll
+    for (int i = 0; i < H; ++i) p[i] = v[i];
+  }
+}
+template <typename C, bool INV, int H>
+__device__ __forceinline__ void smem_cols(C* buf, int nlines) {
+  constexpr int S = H + 1;
+  for (int l = threadIdx.x; l < nlines; l += blockDim.x) {
+    C* p = buf + (l / H) * (H * S) + (l % H);
+    C v[H];
+#pragma unroll
+    for (int i = 0; i < H; ++i) v[i] = p[i * S];
+    reg_fft<C, INV, H>(v);
+#pragma unroll
+    for (int i = 0; i < H; ++i) p[i * S] = v[i];
+  }
+}
+
 // Forward plane kernel, cubic H: fold (or plain load) of two fields + x FFT + y FFT
 // -> W[slot][c][z][y][x].
 template <typename T, int H, bool USE_E>
@@ -589,15 +622,14 @@ __global__ void k_plane_fwd_h(const DevGeom* __restrict__ g, const typename Cx<T
     }
   }
   __syncthreads();
-  smem_lines<C, false, H>(buf, nch * H, nch * H, 0, S, 1);   // x lines (rows)
+  smem_rows<C, false, H>(buf, nch * H);   // x lines
   __syncthreads();
-  smem_lines<C, false, H>(buf, nch * H, H, PL, 1, S);         // y lines (columns)
+  smem_cols<C, false, H>(buf, nch * H);   // y lines
   __syncthreads();
-  const size_t hvol = static_cast<size_t>(H) * H * H;
-  for (int c = 0; c < nch; ++c) {
-    C* dst = W + (static_cast<size_t>(slot) * nch + c) * hvol + static_cast<size_t>(iz) * H * H;
-    for (int e = tid; e < H * H; e += nth) dst[e] = buf[c * PL + (e / H) * S + (e % H)];
-  }
+  constexpr int HV = H * H * H;
+  C* dst0 = W + static_cast<size_t>(slot) * nch * HV + iz * H * H;
+  for (int c = 0; c < nch; ++c)
+    for (int e = tid; e < H * H; e += nth) dst0[c * HV + e] = buf[c * PL + (e / H) * S + (e % H)];
 }
 
 // Backward plane kernel, cubic H: inverse x/y FFT of W[slot][c][iz] + unfold of the two
@@ -617,14 +649,14 @@ __global__ void k_plane_bwd_h(const DevGeom* __restrict__ g, const typename Cx<T
   const bool has_b = fa + 1 < nfields;
   const int tid = threadIdx.x, nth = blockDim.x;
   const size_t hvol = static_cast<size_t>(H) * H * H;
-  for (int c = 0; c < nch; ++c) {
-    const C* s = W + (static_cast<size_t>(slot) * nch + c) * hvol + static_cast<size_t>(iz) * H * H;
-    for (int e = tid; e < H * H; e += nth) buf[c * PL + (e / H) * S + (e % H)] = s[e];
-  }
+  constexpr int HV = H * H * H;
+  const C* src0 = W + static_cast<size_t>(slot) * nch * HV + iz * H * H;
+  for (int c = 0; c < nch; ++c)
+    for (int e = tid; e < H * H; e += nth) buf[c * PL + (e / H) * S + (e % H)] = src0[c * HV + e];
   __syncthreads();
-  smem_lines<C, true, H>(buf, nch * H, nch * H, 0, S, 1);
+  smem_rows<C, true, H>(buf, nch * H);
   __syncthreads();
-  smem_lines<C, true, H>(buf, nch * H, H, PL, 1, S);
+  smem_cols<C, true, H>(buf, nch * H);
   __syncthreads();
   const size_t mvol = static_cast<size_t>(g->M[0]) * g->M[1] * g->M[2];
   T* dsta = f0 + static_cast<size_t>(fa) * mvol;
@@ -679,31 +711,39 @@ __global__ void k_plane_bwd_h(const DevGeom* __restrict__ g, const typename Cx<T
 constexpr int kZB = 4;  // xz-planes (y values) per CTA in the z kernels
 
 // Forward z FFT, cubic H: W[slot][c][z][y][x] (in) -> WT[slot][c][x][y][z] (z fastest,
-// out, same storage: each CTA reads and writes exactly the same addresses).
+// out, same storage: each CTA reads and writes exactly the same addresses).  Thread
+// (yy, x) loads its z line straight into registers (coalesced across x); the
+// transposed store goes through shared memory.
 template <typename T, int H>
 __global__ void k_fft_z_fwd_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* W,
                               typename Cx<T>::type* WT) {
   using C = typename Cx<T>::type;
   constexpr int S = H + 1;
-  constexpr int PL = H * S;
+  constexpr int HV = H * H * H;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* buf = reinterpret_cast<C*>(smem_raw);  // [yy][z][x]
+  C* buf = reinterpret_cast<C*>(smem_raw);  // [yy][x][z] padded
   const int y0 = blockIdx.x * kZB, c = blockIdx.y, slot = blockIdx.z;
   const int ny = min(kZB, H - y0);
-  const int tid = threadIdx.x, nth = blockDim.x;
-  const size_t hvol = static_cast<size_t>(H) * H * H;
-  const C* src = W + (static_cast<size_t>(slot) * g->n_ch + c) * hvol;
-  for (int e = tid; e < ny * H * H; e += nth) {
-    const int x = e % H, z = (e / H) % H, yy = e / (H * H);
-    buf[yy * PL + z * S + x] = src[(static_cast<size_t>(z) * H + y0 + yy) * H + x];
+  const int tid = threadIdx.x;
+  const size_t base = (static_cast<size_t>(slot) * g->n_ch + c) * HV;
+  const int yy = tid / H, x = tid % H;
+  if (yy < ny) {
+    const C* src = W + base + (y0 + yy) * H + x;
+    C v[H];
+#pragma unroll
+    for (int z = 0; z < H; ++z) v[z] = src[z * H * H];
+    reg_fft<C, false, H>(v);
+    C* row = buf + (yy * H + x) * S;
+#pragma unroll
+    for (int z = 0; z < H; ++z) row[z] = v[z];
   }
   __syncthreads();
-  smem_lines<C, false, H>(buf, ny * H, H, PL, 1, S);  // z lines: element stride S
-  __syncthreads();
-  C* dst = WT + (static_cast<size_t>(slot) * g->n_ch + c) * hvol;
-  for (int e = tid; e < ny * H * H; e += nth) {
-    const int z = e % H, yy = (e / H) % ny, x = e / (H * ny);
-    dst[(static_cast<size_t>(x) * H + y0 + yy) * H + z] = buf[yy * PL + z * S + x];
+  C* dst = WT + base;
+  const int run = ny * H;  // contiguous (yy, z) run per x
+  for (int e = tid; e < H * run; e += blockDim.x) {
+    const int xx = e / run, r = e % run;
+    const int y2 = r / H, z = r % H;
+    dst[(xx * H + y0) * H + r] = buf[(y2 * H + xx) * S + z];
   }
 }
 
@@ -740,15 +780,106 @@ __global__ void k_expand_ifft_z_h(const DevGeom* __restrict__ g, const typename 
   }
 }
 
+template <int M> __device__ __forceinline__ int mod_m(int v) {
+  if constexpr ((M & (M - 1)) == 0) {
+    return v & (M - 1);
+  } else {
+    const int r = v % M;
+    return r < 0 ? r + M : r;
+  }
+}
+
 // Spectral-ASU gather from the z-fastest packed workspace, cubic M (= 2H centred,
-// = H plain); separates the two fields of the slot on the fly.
-template <typename T, int M, bool USE_K>
+// = H plain), D representative operations; separates the two fields of the slot on
+// the fly.  The geometry is staged in shared memory once per CTA.
+template <typename T, int M, int D, bool USE_K, bool PERM>
 __global__ void k_recon_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
                           const uint32_t* __restrict__ spec_h, const T* __restrict__ K,
                           const typename Cx<T>::type* __restrict__ WT, typename Cx<T>::type* __restrict__ F,
                           int nfields) {
   using C = typename Cx<T>::type;
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ int sR[D][9];
+  __shared__ int sPS[D][3];
+  __shared__ int sTP[D][3];
+  __shared__ int sCh[8];
+  const int tid = threadIdx.x;
+  if (tid < D * 9) sR[tid / 9][tid % 9] = g->rep_R[tid / 9][tid % 9];
+  if (tid < D * 3) { sPS[tid / 3][tid % 3] = g->rep_ps[tid / 3][tid % 3]; sTP[tid / 3][tid % 3] = g->rep_tp[tid / 3][tid % 3]; }
+  if (tid < 8) sCh[tid] = g->chan_of_parity[tid];
+  __syncthreads();
+  const int s = blockIdx.x * blockDim.x + tid;
+  const int slot = blockIdx.y;
+  if (s >= g->n_spec) return;
+  const int fa = 2 * slot;
+  const bool has_b = fa + 1 < nfields;
+  const uint32_t hp = spec_h[s];
+  const int h[3] = {static_cast<int>(hp & 1023u), static_cast<int>((hp >> 10) & 1023u), static_cast<int>((hp >> 20) & 1023u)};
+  const bool cen = g->centered;
+  constexpr int Hc2 = M / 2;
+  const int Hc = cen ? Hc2 : M;
+  const int ls = cen ? 1 : 0;  // channel coordinate = q >> ls
+  const size_t hvol = static_cast<size_t>(Hc) * Hc * Hc;
+  const C* Wb = WT + static_cast<size_t>(slot) * g->n_ch * hvol;
+  const C* ph = tables + g->ph_off;
+  const int P = g->P, pmask = g->pmask;
+  const T half = static_cast<T>(0.5);
+  C acca = mk<C>(static_cast<T>(0), static_cast<T>(0));
+  C accb = acca;
+#pragma unroll
+  for (int r = 0; r < D; ++r) {
+    int q[3], qn[3];
+#pragma unroll
+    for (int dd = 0; dd < 3; ++dd) {
+      int v;
+      if (PERM) {
+        const int ps = sPS[r][dd];
+        v = h[ps & 3];
+        if (ps & 4) v = -v;
+      } else {
+        v = sR[r][dd] * h[0] + sR[r][3 + dd] * h[1] + sR[r][6 + dd] * h[2];
+      }
+      q[dd] = mod_m<M>(v);
+      qn[dd] = mod_m<M>(M - q[dd]);
+    }
+    int c = 0;
+    if (cen) {
+      c = sCh[(q[0] & 1) + 2 * (q[1] & 1) + 4 * (q[2] & 1)];
+      if (c < 0) continue;
+    }
+    const size_t base = static_cast<size_t>(c) * hvol;
+    const size_t idx = base + (static_cast<size_t>(q[0] >> ls) * Hc + (q[1] >> ls)) * Hc + (q[2] >> ls);
+    const size_t idn = base + (static_cast<size_t>(qn[0] >> ls) * Hc + (qn[1] >> ls)) * Hc + (qn[2] >> ls);
+    const C X = Wb[idx], Xn = Wb[idn];
+    const C Ga = mk<C>(half * (X.x + Xn.x), half * (X.y - Xn.y));   // (X + conj Xn) / 2
+    const C Gb = mk<C>(half * (X.y + Xn.y), half * (Xn.x - X.x));   // (X - conj Xn) / 2i
+    int j = h[0] * sTP[r][0] + h[1] * sTP[r][1] + h[2] * sTP[r][2];
+    j = pmask >= 0 ? (j & pmask) : ((j % P) + P) % P;
+    const C w = ph[j];
+    acca = cadd(acca, cmul(Ga, w));
+    accb = cadd(accb, cmul(Gb, w));
+  }
+  if (USE_K) { const T k = K[s]; acca = cscale(acca, k); accb = cscale(accb, k); }
+  F[static_cast<size_t>(fa) * g->n_spec + s] = acca;
+  if (has_b) F[static_cast<size_t>(fa + 1) * g->n_spec + s] = accb;
+}
+
+// Spectral-ASU gather when the 8 representative operations are the diagonal sign
+// matrices diag(+-1, +-1, +-1) (any translations): the 8 taps read G0 at the sign
+// images s.h of h, which all lie in one parity channel, and the Hermitian partner
+// X(-q) of tap s is tap ~s.  Eight workspace loads per point and slot.
+template <typename T, int M, bool USE_K>
+__global__ void k_recon_diag8(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                              const uint32_t* __restrict__ spec_h, const T* __restrict__ K,
+                              const typename Cx<T>::type* __restrict__ WT, typename Cx<T>::type* __restrict__ F,
+                              int nfields) {
+  using C = typename Cx<T>::type;
+  __shared__ int sTP[8][3];  // indexed by sign pattern
+  __shared__ int sCh[8];
+  const int tid = threadIdx.x;
+  if (tid < 24) sTP[tid / 3][tid % 3] = g->rep_tp[g->sign_op[tid / 3]][tid % 3];
+  if (tid < 8) sCh[tid] = g->chan_of_parity[tid];
+  __syncthreads();
+  const int s = blockIdx.x * blockDim.x + tid;
   const int slot = blockIdx.y;
   if (s >= g->n_spec) return;
   const int fa = 2 * slot;
@@ -757,48 +888,51 @@ __global__ void k_recon_h(const DevGeom* __restrict__ g, const typename Cx<T>::t
   const int h0 = static_cast<int>(hp & 1023u), h1 = static_cast<int>((hp >> 10) & 1023u), h2 = static_cast<int>((hp >> 20) & 1023u);
   const bool cen = g->centered;
   const int Hc = cen ? M / 2 : M;
-  const size_t hvol = static_cast<size_t>(Hc) * Hc * Hc;
-  const C* Wb = WT + static_cast<size_t>(slot) * g->n_ch * hvol;
+  const int ls = cen ? 1 : 0;
+  const int hvol = Hc * Hc * Hc;
+  // per-axis (+h, -h) positions mod M, in channel coordinates
+  const int p0 = mod_m<M>(h0), p1 = mod_m<M>(h1), p2 = mod_m<M>(h2);
+  const int m0 = mod_m<M>(M - p0), m1 = mod_m<M>(M - p1), m2 = mod_m<M>(M - p2);
+  int c = 0;
+  if (cen) c = sCh[(p0 & 1) + 2 * (p1 & 1) + 4 * (p2 & 1)];
+  if (c < 0) {  // extinct parity class: every tap reads zero
+    const C z = mk<C>(static_cast<T>(0), static_cast<T>(0));
+    F[static_cast<size_t>(fa) * g->n_spec + s] = z;
+    if (has_b) F[static_cast<size_t>(fa + 1) * g->n_spec + s] = z;
+    return;
+  }
+  const int X0[2] = {(p0 >> ls) * Hc * Hc, (m0 >> ls) * Hc * Hc};
+  const int X1[2] = {(p1 >> ls) * Hc, (m1 >> ls) * Hc};
+  const int X2[2] = {p2 >> ls, m2 >> ls};
+  const C* Wb = WT + (static_cast<size_t>(slot) * g->n_ch + c) * hvol;
+  C X[8];
+#pragma unroll
+  for (int sg = 0; sg < 8; ++sg) X[sg] = Wb[X0[sg & 1] + X1[(sg >> 1) & 1] + X2[(sg >> 2) & 1]];
   const C* ph = tables + g->ph_off;
   const int P = g->P, pmask = g->pmask;
   const T half = static_cast<T>(0.5);
   C acca = mk<C>(static_cast<T>(0), static_cast<T>(0));
   C accb = acca;
-  for (int r = 0; r < g->d; ++r) {
-    int q[3], qn[3];
 #pragma unroll
-    for (int dd = 0; dd < 3; ++dd) {
-      int v = g->rep_R[r][dd] * h0 + g->rep_R[r][3 + dd] * h1 + g->rep_R[r][6 + dd] * h2;
-      v %= M;
-      q[dd] = v < 0 ? v + M : v;
-      qn[dd] = q[dd] == 0 ? 0 : M - q[dd];
-    }
-    size_t idx, idn;
-    if (cen) {
-      const int c = g->chan_of_parity[(q[0] & 1) + 2 * (q[1] & 1) + 4 * (q[2] & 1)];
-      if (c < 0) continue;
-      idx = static_cast<size_t>(c) * hvol + (static_cast<size_t>(q[0] >> 1) * Hc + (q[1] >> 1)) * Hc + (q[2] >> 1);
-      idn = static_cast<size_t>(c) * hvol + (static_cast<size_t>(qn[0] >> 1) * Hc + (qn[1] >> 1)) * Hc + (qn[2] >> 1);
-    } else {
-      idx = (static_cast<size_t>(q[0]) * Hc + q[1]) * Hc + q[2];
-      idn = (static_cast<size_t>(qn[0]) * Hc + qn[1]) * Hc + qn[2];
-    }
-    const C X = Wb[idx], Xn = Wb[idn];
-    // G_a = (X + conj Xn)/2 ; G_b = (X - conj Xn)/(2i)
-    const C Ga = mk<C>(half * (X.x + Xn.x), half * (X.y - Xn.y));
-    const C Gb = mk<C>(half * (X.y + Xn.y), half * (Xn.x - X.x));
-    int j = h0 * g->rep_tp[r][0] + h1 * g->rep_tp[r][1] + h2 * g->rep_tp[r][2];
+  for (int sg = 0; sg < 8; ++sg) {
+    const C Xs = X[sg], Xn = X[7 - sg];
+    const C Ga = mk<C>(half * (Xs.x + Xn.x), half * (Xs.y - Xn.y));
+    const C Gb = mk<C>(half * (Xs.y + Xn.y), half * (Xn.x - Xs.x));
+    int j = h0 * sTP[sg][0] + h1 * sTP[sg][1] + h2 * sTP[sg][2];
     j = pmask >= 0 ? (j & pmask) : ((j % P) + P) % P;
     const C w = ph[j];
     acca = cadd(acca, cmul(Ga, w));
     accb = cadd(accb, cmul(Gb, w));
   }
-  if (USE_K) { acca = cscale(acca, K[s]); accb = cscale(accb, K[s]); }
+  if (USE_K) { const T k = K[s]; acca = cscale(acca, k); accb = cscale(accb, k); }
   F[static_cast<size_t>(fa) * g->n_spec + s] = acca;
   if (has_b) F[static_cast<size_t>(fa + 1) * g->n_spec + s] = accb;
 }
 
 // G0 at orbit representatives of the two fields of a slot, packed as G_a + i G_b.
+// Each thread serves SPT consecutive slots, reusing the table entries and keeping
+// several independent spectrum gathers in flight.
+constexpr int kRepSlots = 4;
 template <typename T>
 __global__ void k_inv_recon_reps(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
                                  const int32_t* __restrict__ inv_spec, const int32_t* __restrict__ inv_phase,
@@ -806,33 +940,117 @@ __global__ void k_inv_recon_reps(const DevGeom* __restrict__ g, const typename C
                                  int nfields) {
   using C = typename Cx<T>::type;
   const int o = blockIdx.x * blockDim.x + threadIdx.x;
-  const int slot = blockIdx.y;
   if (o >= g->n_orbits) return;
-  const int fa = 2 * slot;
-  const bool has_b = fa + 1 < nfields;
+  const int slot0 = blockIdx.y * kRepSlots;
+  const int nslots = (nfields + 1) / 2;
   const int d = g->d;
-  const C* Fa = F + static_cast<size_t>(fa) * g->n_spec;
-  const C* Fb = Fa + g->n_spec;
+  const int ns = g->n_spec;
   const C* ph = tables + g->ph_off;
-  C acca = mk<C>(static_cast<T>(0), static_cast<T>(0));
-  C accb = acca;
+  C acc[2 * kRepSlots];
+#pragma unroll
+  for (int k = 0; k < 2 * kRepSlots; ++k) acc[k] = mk<C>(static_cast<T>(0), static_cast<T>(0));
   for (int a = 0; a < d; ++a) {
     const int s = inv_spec[static_cast<size_t>(o) * d + a];
     if (s == 0) continue;
     const int si = (s > 0 ? s : -s) - 1;
     const C w = ph[inv_phase[static_cast<size_t>(o) * d + a]];
-    C fa_v = Fa[si];
-    if (s < 0) fa_v = cconj(fa_v);
-    acca = cadd(acca, cmulc(fa_v, w));
-    if (has_b) {
-      C fb_v = Fb[si];
-      if (s < 0) fb_v = cconj(fb_v);
-      accb = cadd(accb, cmulc(fb_v, w));
+#pragma unroll
+    for (int k = 0; k < 2 * kRepSlots; ++k) {
+      const int f = 2 * slot0 + k;
+      if (f < nfields) {
+        C v = F[static_cast<size_t>(f) * ns + si];
+        if (s < 0) v = cconj(v);
+        acc[k] = cadd(acc[k], cmulc(v, w));
+      }
     }
   }
   const T inv_d = static_cast<T>(1.0 / static_cast<double>(d));
-  // X = G_a + i G_b
-  G0R[static_cast<size_t>(slot) * g->n_orbits + o] = mk<C>(inv_d * (acca.x - accb.y), inv_d * (acca.y + accb.x));
+#pragma unroll
+  for (int k = 0; k < kRepSlots; ++k) {
+    const int slot = slot0 + k;
+    if (slot < nslots) {
+      const C a = acc[2 * k], b = acc[2 * k + 1];
+      G0R[static_cast<size_t>(slot) * g->n_orbits + o] = mk<C>(inv_d * (a.x - b.y), inv_d * (a.y + b.x));
+    }
+  }
+}
+
+// G0 at orbit representatives for one field, with the field's whole spectrum staged
+// in shared memory (one CTA per field and representative range): every alias gather
+// is a shared-memory read.  Aliases are packed as spec+1 (bits 0-19), conjugation
+// (bit 20) and phase numerator (bits 21-31); with d = 8 a thread reads its
+// representative's 8 entries as two 16-byte loads.  Output layout: G0RP[slot][o][f&1].
+template <typename T, int D>
+__global__ void k_inv_recon_reps_smem(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                                      const uint32_t* __restrict__ inv_pk, const typename Cx<T>::type* __restrict__ F,
+                                      typename Cx<T>::type* __restrict__ G0RP, int reps_per_part) {
+  using C = typename Cx<T>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sF = reinterpret_cast<C*>(smem_raw);
+  const int ns = g->n_spec;
+  const int f = blockIdx.y;
+  const C* Ff = F + static_cast<size_t>(f) * ns;
+  for (int i = threadIdx.x; i < ns; i += blockDim.x) sF[i] = Ff[i];
+  __syncthreads();
+  const C* ph = tables + g->ph_off;
+  const T inv_d = static_cast<T>(1.0 / static_cast<double>(D));
+  const int o0 = blockIdx.x * reps_per_part;
+  const int o1 = min(g->n_orbits, o0 + reps_per_part);
+  C* out = G0RP + static_cast<size_t>(f >> 1) * g->n_orbits * 2 + (f & 1);
+  for (int o = o0 + threadIdx.x; o < o1; o += blockDim.x) {
+    uint32_t e[D];
+    if constexpr (D == 8) {
+      const uint4* p4 = reinterpret_cast<const uint4*>(inv_pk + static_cast<size_t>(o) * 8);
+      const uint4 u0 = p4[0], u1 = p4[1];
+      e[0] = u0.x; e[1] = u0.y; e[2] = u0.z; e[3] = u0.w; e[4] = u1.x; e[5] = u1.y; e[6] = u1.z; e[7] = u1.w;
+    } else {
+#pragma unroll
+      for (int a = 0; a < D; ++a) e[a] = inv_pk[static_cast<size_t>(o) * D + a];
+    }
+    C acc = mk<C>(static_cast<T>(0), static_cast<T>(0));
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      const uint32_t sp = e[a] & 0xFFFFFu;
+      if (sp == 0) continue;
+      C v = sF[sp - 1];
+      if (e[a] & (1u << 20)) v = cconj(v);
+      acc = cadd(acc, cmulc(v, ph[e[a] >> 21]));
+    }
+    out[static_cast<size_t>(o) * 2] = cscale(acc, inv_d);
+  }
+}
+
+// Backward expansion from per-field representatives (G0RP[slot][o][a|b]) + inverse z
+// FFT: thread (yy, x) assembles its z line X = (G_a + i G_b) e^{+2 pi i j/P} in
+// registers, transforms it and stores it coalesced across x.  No shared memory.
+template <typename T, int H>
+__global__ void k_expand2_ifft_z_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                                   const int2* __restrict__ ET, const typename Cx<T>::type* __restrict__ G0RF,
+                                   typename Cx<T>::type* __restrict__ W, int nfields) {
+  using C = typename Cx<T>::type;
+  constexpr int HV = H * H * H;
+  const int y0 = blockIdx.x * kZB, c = blockIdx.y, slot = blockIdx.z;
+  const int ny = min(kZB, H - y0);
+  const int tid = threadIdx.x;
+  const int yy = tid / H, x = tid % H;
+  if (yy >= ny) return;
+  const int y = y0 + yy;
+  const int2* et = ET + static_cast<size_t>(c) * HV + y * H + x;
+  const bool has_b = 2 * slot + 1 < nfields;
+  const C* rp = G0RF + static_cast<size_t>(slot) * g->n_orbits * 2;
+  const C* ph = tables + g->ph_off;
+  C v[H];
+#pragma unroll
+  for (int z = 0; z < H; ++z) {
+    const int2 t = et[z * H * H];
+    const C a = rp[2 * t.x];
+    const C b = has_b ? rp[2 * t.x + 1] : mk<C>(static_cast<T>(0), static_cast<T>(0));
+    v[z] = cmulc(mk<C>(a.x - b.y, a.y + b.x), ph[t.y]);
+  }
+  reg_fft<C, true, H>(v);
+  C* dst = W + (static_cast<size_t>(slot) * g->n_ch + c) * HV + y * H + x;
+#pragma unroll
+  for (int z = 0; z < H; ++z) dst[z * H * H] = v[z];
 }
 
 // ---------------------------------------------------------------- elementwise
@@ -975,6 +1193,10 @@ void set_fast_attrs() {
       cudaFuncSetAttribute(k_expand_ifft_z_h<T, HH>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
     });
   }
+  cudaFuncSetAttribute(k_inv_recon_reps_smem<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_inv_recon_reps_smem<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_inv_recon_reps_smem<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
+  cudaFuncSetAttribute(k_inv_recon_reps_smem<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmem);
 }
 
 // Constant-memory twiddles e^{-2 pi i j / N} for the register FFTs (FP64 values rounded).
@@ -1041,23 +1263,61 @@ void launch_stage(Plan* p, int stage, const T* f0, typename Cx<T>::type* F, cons
         const int M = T_.centered ? 2 * H : H;
         const T* K = static_cast<const T*>(p->d_K);
         const uint32_t* sh = static_cast<const uint32_t*>(p->d_spec_h);
-        CFFT_FOR_M(M, {
-          if (use_K) k_recon_h<T, MM, true><<<gr, 256, 0, st>>>(g, tab, sh, K, W, F, nb);
-          else k_recon_h<T, MM, false><<<gr, 256, 0, st>>>(g, tab, sh, nullptr, W, F, nb);
-        });
+        const bool perm = p->rep_perm;
+        if (p->rep_diag8) {
+          CFFT_FOR_M(M, {
+            if (use_K) k_recon_diag8<T, MM, true><<<gr, 256, 0, st>>>(g, tab, sh, K, W, F, nb);
+            else k_recon_diag8<T, MM, false><<<gr, 256, 0, st>>>(g, tab, sh, nullptr, W, F, nb);
+          });
+          break;
+        }
+#define CFFT_RECON_D(DD)                                                                                  \
+  CFFT_FOR_M(M, {                                                                                         \
+    if (use_K) {                                                                                          \
+      if (perm) k_recon_h<T, MM, DD, true, true><<<gr, 256, 0, st>>>(g, tab, sh, K, W, F, nb);            \
+      else k_recon_h<T, MM, DD, true, false><<<gr, 256, 0, st>>>(g, tab, sh, K, W, F, nb);                \
+    } else {                                                                                              \
+      if (perm) k_recon_h<T, MM, DD, false, true><<<gr, 256, 0, st>>>(g, tab, sh, nullptr, W, F, nb);     \
+      else k_recon_h<T, MM, DD, false, false><<<gr, 256, 0, st>>>(g, tab, sh, nullptr, W, F, nb);         \
+    }                                                                                                     \
+  })
+        switch (T_.d) {
+          case 1: CFFT_RECON_D(1); break;
+          case 2: CFFT_RECON_D(2); break;
+          case 4: CFFT_RECON_D(4); break;
+          default: CFFT_RECON_D(8); break;
+        }
+#undef CFFT_RECON_D
         break;
       }
       case 3: {
         const int no = static_cast<int>(T_.orbit_rep.size());
-        k_inv_recon_reps<T><<<dim3((no + 127) / 128, nslots), 128, 0, st>>>(
+        if (p->reps_smem) {
+          const int parts = nb >= 100 ? 1 : std::max(1, std::min((148 + nb - 1) / nb, (no + 1023) / 1024));
+          const int per = (no + parts - 1) / parts;
+          const size_t smem = T_.spec.size() * cs;
+          const uint32_t* pk = static_cast<const uint32_t*>(p->d_inv_pk);
+          switch (T_.d) {
+            case 1: k_inv_recon_reps_smem<T, 1><<<dim3(parts, nb), 1024, smem, st>>>(g, tab, pk, Fin, static_cast<C*>(p->d_g0r), per); break;
+            case 2: k_inv_recon_reps_smem<T, 2><<<dim3(parts, nb), 1024, smem, st>>>(g, tab, pk, Fin, static_cast<C*>(p->d_g0r), per); break;
+            case 4: k_inv_recon_reps_smem<T, 4><<<dim3(parts, nb), 1024, smem, st>>>(g, tab, pk, Fin, static_cast<C*>(p->d_g0r), per); break;
+            default: k_inv_recon_reps_smem<T, 8><<<dim3(parts, nb), 1024, smem, st>>>(g, tab, pk, Fin, static_cast<C*>(p->d_g0r), per); break;
+          }
+          break;
+        }
+        k_inv_recon_reps<T><<<dim3((no + 127) / 128, (nslots + kRepSlots - 1) / kRepSlots), 128, 0, st>>>(
             g, tab, static_cast<const int32_t*>(p->d_inv_spec), static_cast<const int32_t*>(p->d_inv_phase), Fin,
             static_cast<C*>(p->d_g0r), nb);
         break;
       }
       case 4:
         CFFT_FOR_H(H, {
-          k_expand_ifft_z_h<T, HH><<<gz, thr_z, smem_z, st>>>(g, tab, static_cast<const int2*>(p->d_expand),
-                                                              static_cast<const C*>(p->d_g0r), W);
+          if (p->reps_smem)
+            k_expand2_ifft_z_h<T, HH><<<gz, thr_z, 0, st>>>(g, tab, static_cast<const int2*>(p->d_expand),
+                                                            static_cast<const C*>(p->d_g0r), W, nb);
+          else
+            k_expand_ifft_z_h<T, HH><<<gz, thr_z, smem_z, st>>>(g, tab, static_cast<const int2*>(p->d_expand),
+                                                                static_cast<const C*>(p->d_g0r), W);
         });
         break;
       default:
@@ -1203,6 +1463,37 @@ Status plan_device_init(Plan* p, std::string* err) {
       for (int j = 0; j < 3; ++j) g.rem_R[r][i * 3 + j] = T.rem_ops[r].R[i][j];
     for (int i = 0; i < 3; ++i) g.rem_s[r][i] = T.rem_ops[r].t[i];
   }
+  // Signed-permutation form of R_b^T (column dd of R_b holds a single +-1).
+  g.rep_perm = 1;
+  for (int r = 0; r < T.d && g.rep_perm; ++r)
+    for (int dd = 0; dd < 3; ++dd) {
+      int nz = 0, src = 0, neg = 0;
+      for (int d2 = 0; d2 < 3; ++d2) {
+        const int v = T.rep_ops[r].R[d2][dd];
+        if (v == 0) continue;
+        ++nz; src = d2; neg = v < 0;
+        if (v != 1 && v != -1) nz = 9;
+      }
+      if (nz != 1) { g.rep_perm = 0; break; }
+      g.rep_ps[r][dd] = src + 4 * neg;
+    }
+  p->rep_perm = g.rep_perm != 0;
+  // The 8 representatives are exactly the 8 diagonal sign matrices?
+  g.rep_diag8 = T.d == 8 ? 1 : 0;
+  for (int k = 0; k < 8; ++k) g.sign_op[k] = -1;
+  for (int r = 0; r < T.d && g.rep_diag8; ++r) {
+    int sg = 0;
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        const int v = T.rep_ops[r].R[i][j];
+        if (i != j && v != 0) g.rep_diag8 = 0;
+        if (i == j && v != 1 && v != -1) g.rep_diag8 = 0;
+        if (i == j && v == -1) sg |= 1 << i;
+      }
+    if (g.rep_diag8 && g.sign_op[sg] >= 0) g.rep_diag8 = 0;
+    if (g.rep_diag8) g.sign_op[sg] = r;
+  }
+  p->rep_diag8 = g.rep_diag8 != 0;
   // Fast (compile-time sized) path for cubic channel grids.
   const bool cubic = T.H[0] == T.H[1] && T.H[1] == T.H[2];
   p->fast_h = (cubic && (p->precision == 8 ? fast_ok<double>(T.H[0]) : fast_ok<float>(T.H[0]))) ? T.H[0] : 0;
@@ -1295,9 +1586,21 @@ Status plan_device_init(Plan* p, std::string* err) {
   if ((st = alloc(&p->d_work_T, chunk * T.n_ch * hvol * cs, "channel workspace")) != Status::kOk) return st;
   if ((st = alloc(&p->d_work_F, B * T.spec.size() * cs, "spectrum workspace")) != Status::kOk) return st;
   if ((st = alloc(&p->d_work_E, B * mvol * rs, "interaction workspace")) != Status::kOk) return st;
+  // Per-field representative gather from a shared-memory copy of the spectrum.
+  std::vector<uint32_t> inv_pk;
+  p->reps_smem = p->fast_h && T.spec.size() * cs <= 200 * 1024 && T.spec.size() < (1u << 20) - 1 && T.P <= 2048;
+  if (p->reps_smem) {
+    inv_pk.resize(T.inv_spec.size());
+    for (size_t k = 0; k < inv_pk.size(); ++k) {
+      const int sp = T.inv_spec[k];
+      const uint32_t a = static_cast<uint32_t>(sp < 0 ? -sp : sp);
+      inv_pk[k] = a | (sp < 0 ? (1u << 20) : 0u) | (static_cast<uint32_t>(T.inv_phase[k]) << 21);
+    }
+    if ((st = alloc(&p->d_inv_pk, inv_pk.size() * 4, "packed inverse table")) != Status::kOk) return st;
+  }
   if (p->fast_h) {
     if ((st = alloc(&p->d_expand, expand.size() * sizeof(int2), "expansion table")) != Status::kOk) return st;
-    if ((st = alloc(&p->d_g0r, chunk * T.orbit_rep.size() * cs, "representative workspace")) != Status::kOk) return st;
+    if ((st = alloc(&p->d_g0r, (chunk + 1) * T.orbit_rep.size() * cs, "representative workspace")) != Status::kOk) return st;
   }
   CFFT_CUDA(cudaMemcpy(p->d_geom, &g, sizeof(g), cudaMemcpyHostToDevice), "upload geometry");
   CFFT_CUDA(cudaMemcpy(p->d_tables, tab.data(), tab.size(), cudaMemcpyHostToDevice), "upload tables");
@@ -1310,6 +1613,8 @@ Status plan_device_init(Plan* p, std::string* err) {
   }
   if (p->fast_h)
     CFFT_CUDA(cudaMemcpy(p->d_expand, expand.data(), expand.size() * sizeof(int2), cudaMemcpyHostToDevice), "upload expansion");
+  if (p->reps_smem)
+    CFFT_CUDA(cudaMemcpy(p->d_inv_pk, inv_pk.data(), inv_pk.size() * 4, cudaMemcpyHostToDevice), "upload packed table");
   // Orbit expansion writes only alive positions; channel positions never written stay zero.
   CFFT_CUDA(cudaMemset(p->d_work_T, 0, chunk * T.n_ch * hvol * cs), "clear workspace");
   if (p->precision == 8) set_smem_attrs<double>();
@@ -1336,7 +1641,7 @@ Status plan_upload_kernel(Plan* p, std::string* err) {
 void plan_device_free(Plan* p) {
   void** bufs[] = {&p->d_geom, &p->d_tables, &p->d_spec_h, &p->d_K, &p->d_orbit_rep, &p->d_inv_spec,
                    &p->d_inv_phase, &p->d_img_mask, &p->d_fill_map, &p->d_work_T, &p->d_work_F,
-                   &p->d_work_E, &p->d_stage_in, &p->d_stage_out, &p->d_expand, &p->d_g0r};
+                   &p->d_work_E, &p->d_stage_in, &p->d_stage_out, &p->d_expand, &p->d_g0r, &p->d_inv_pk};
   for (void** b : bufs)
     if (*b) { cudaFree(*b); *b = nullptr; }
   if (p->own_stream) { cudaStreamDestroy(static_cast<cudaStream_t>(p->own_stream)); p->own_stream = nullptr; }

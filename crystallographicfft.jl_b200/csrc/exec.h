@@ -32,12 +32,16 @@ struct Plan {
   void* d_stage_out = nullptr;
   void* d_expand = nullptr;     // fast path: per channel position (orbit index, phase numerator)
   void* d_g0r = nullptr;        // fast path: chunk x n_orbits complex (G0 at representatives)
+  void* d_inv_pk = nullptr;     // fast path: packed alias table for the shared-memory gather
   void* own_stream = nullptr;
   size_t workspace_bytes = 0;
   // launch geometry
   int threads_xy = 0, threads_z = 0;
   int fast_h = 0;               // cubic channel edge of the compile-time sized kernels (0 = generic)
   int chunk = 1;                // fields per workspace chunk
+  bool rep_perm = false;        // representative ops are signed permutations
+  bool rep_diag8 = false;       // representative ops are the 8 diagonal sign matrices
+  bool reps_smem = false;       // representative gather stages the spectrum in shared memory
   size_t smem_xy = 0, smem_z = 0;
 };
 

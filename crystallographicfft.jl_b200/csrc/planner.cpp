@@ -487,6 +487,25 @@ Status build_tables(const std::vector<SymOp>& shifted_ops, const int* N_in, int 
       }
     }
   }
+  // Order the representatives by the spectral index of their first alias so that
+  // neighbouring device threads gather neighbouring spectrum entries.
+  const size_t n_orb = T->orbit_rep.size();
+  std::vector<size_t> perm(n_orb);
+  std::iota(perm.begin(), perm.end(), 0);
+  std::stable_sort(perm.begin(), perm.end(), [&](size_t a, size_t b) {
+    return std::abs(T->inv_spec[a * d]) < std::abs(T->inv_spec[b * d]);
+  });
+  std::vector<int32_t> rep2(n_orb), spec2(n_orb * d), phase2(n_orb * d);
+  for (size_t k = 0; k < n_orb; ++k) {
+    rep2[k] = T->orbit_rep[perm[k]];
+    for (int a = 0; a < d; ++a) {
+      spec2[k * d + a] = T->inv_spec[perm[k] * d + a];
+      phase2[k * d + a] = T->inv_phase[perm[k] * d + a];
+    }
+  }
+  T->orbit_rep.swap(rep2);
+  T->inv_spec.swap(spec2);
+  T->inv_phase.swap(phase2);
   return Status::kOk;
 }
 
