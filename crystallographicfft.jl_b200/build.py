@@ -12,6 +12,7 @@ import argparse
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -25,8 +26,9 @@ CXXFLAGS = ["-O3", "-fPIC", "-std=c++17", "-Wall", "-Wno-unused-function"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"] + ARCH
 
 HOST_SOURCES = ["spacegroups.cpp", "planner.cpp", "cabi.cpp"]
-DEVICE_SOURCES = ["exec.cu"]
-HEADERS = ["cfft_internal.h", "exec.h"]
+# The fast-path kernels are split by stage group and precision so nvcc runs in parallel.
+DEVICE_SOURCES = ["exec.cu", "fast_planes_f32.cu", "fast_planes_f64.cu", "fast_other_f32.cu", "fast_other_f64.cu"]
+HEADERS = ["cfft_internal.h", "exec.h", "device_common.cuh", "fast_api.h", "fast_kernels.cuh"]
 
 
 def _newer(src_paths, target):
@@ -45,19 +47,22 @@ def _run(cmd, verbose):
 def build(force: bool = False, verbose: bool = False, extra_nvflags=None) -> str:
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "cfft_b200.h")]
-    objs = []
+    objs, jobs = [], []
     for s in HOST_SOURCES:
         src = os.path.join(CSRC, s)
         obj = os.path.join(BUILD, s + ".o")
         if force or _newer([src] + headers, obj):
-            _run(["g++"] + CXXFLAGS + ["-I", INCLUDE, "-I", "/usr/local/cuda/include", "-c", src, "-o", obj], verbose)
+            jobs.append(["g++"] + CXXFLAGS + ["-I", INCLUDE, "-I", "/usr/local/cuda/include", "-c", src, "-o", obj])
         objs.append(obj)
     for s in DEVICE_SOURCES:
         src = os.path.join(CSRC, s)
         obj = os.path.join(BUILD, s + ".o")
         if force or _newer([src] + headers, obj):
-            _run([NVCC] + NVFLAGS + list(extra_nvflags or []) + ["-I", INCLUDE, "-c", src, "-o", obj], verbose)
+            jobs.append([NVCC] + NVFLAGS + list(extra_nvflags or []) + ["-I", INCLUDE, "-c", src, "-o", obj])
         objs.append(obj)
+    with ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(_run, j, verbose) for j in jobs]:
+            f.result()
     if force or _newer(objs, LIB):
         _run([NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-cudart", "static"], verbose)
     return LIB

@@ -34,11 +34,17 @@ struct Plan {
   void* d_g0r = nullptr;        // fast path: chunk x n_orbits complex (G0 at representatives)
   void* d_inv_pk = nullptr;     // fast path: packed alias table for the shared-memory gather
   void* own_stream = nullptr;
+  void* lane_stream[2] = {nullptr, nullptr};  // concurrent chunk lanes (fork/join on the caller's stream)
+  void* ev_fork = nullptr;
+  void* ev_join[2] = {nullptr, nullptr};
+  size_t w_lane_bytes = 0, g0r_lane_bytes = 0;
   size_t workspace_bytes = 0;
   // launch geometry
   int threads_xy = 0, threads_z = 0;
   int fast_h = 0;               // cubic channel edge of the compile-time sized kernels (0 = generic)
   int chunk = 1;                // fields per workspace chunk
+  int lanes = 1;                // concurrent chunk lanes
+  int cent_type = 0;            // plane-kernel centring (0 plain, 1 I, 2 F, 3 C, 4 A)
   bool rep_perm = false;        // representative ops are signed permutations
   bool rep_diag8 = false;       // representative ops are the 8 diagonal sign matrices
   bool reps_smem = false;       // representative gather stages the spectrum in shared memory

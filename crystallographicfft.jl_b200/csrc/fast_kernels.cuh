@@ -1,0 +1,882 @@
+// Compile-time sized fast-path kernels of libcfft_b200 (sm_100a).  Included by the four
+// fast_*.cu translation units; each defines CFFT_FAST_T (float/double) and
+// CFFT_FAST_GROUP (0: plane stages 0 and 5, 1: stages 1-4) before including it, so
+// every unit instantiates only its own kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "device_common.cuh"
+#include "fast_api.h"
+
+namespace cfft {
+namespace {
+
+// ---------------------------------------------------------------- compile-time sized path
+// For cubic channel grids with H in {4, 6, 8, 12, 16, 24, 32, 48} every line FFT is a
+// fully unrolled mixed-radix Stockham in registers (one thread per line), with its
+// twiddles in constant memory, so no runtime division or shared-memory pass remains
+// inside an FFT.  Shared-memory rows are padded to an odd stride (H + 1 complex) so
+// row and column accesses of a warp are bank-conflict free.
+
+constexpr int kTwOff4 = 0, kTwOff6 = 4, kTwOff8 = 10, kTwOff12 = 18, kTwOff16 = 30, kTwOff24 = 46,
+              kTwOff32 = 70, kTwOff48 = 102, kTwTotal = 150;
+__constant__ float2 c_tw_f[kTwTotal];
+__constant__ double2 c_tw_d[kTwTotal];
+
+template <int N> constexpr int tw_offset() {
+  return N == 4 ? kTwOff4 : N == 6 ? kTwOff6 : N == 8 ? kTwOff8 : N == 12 ? kTwOff12 : N == 16 ? kTwOff16
+       : N == 24 ? kTwOff24 : N == 32 ? kTwOff32 : kTwOff48;
+}
+constexpr int pick_radix(int rem) { return rem % 8 == 0 ? 8 : rem % 4 == 0 ? 4 : rem % 2 == 0 ? 2 : rem % 3 == 0 ? 3 : 5; }
+
+template <typename C> __device__ __forceinline__ C ctw(int i);
+template <> __device__ __forceinline__ float2 ctw<float2>(int i) { return c_tw_f[i]; }
+template <> __device__ __forceinline__ double2 ctw<double2>(int i) { return c_tw_d[i]; }
+
+template <typename C, bool INV, int N, int Ns, int Rem>
+struct RegFFT {
+  static __device__ __forceinline__ void run(C* v) {
+    constexpr int R = pick_radix(Rem);
+    constexpr int NB = N / R;
+    constexpr int STEP = N / (Ns * R);
+    C w[N];
+#pragma unroll
+    for (int j = 0; j < NB; ++j) {
+      const int k = j % Ns;
+      C x[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) x[r] = v[j + r * NB];
+      if (k != 0) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          const C t = ctw<C>(tw_offset<N>() + r * k * STEP);
+          x[r] = INV ? cmulc(x[r], t) : cmul(x[r], t);
+        }
+      }
+      dftR<C, INV, R>(x);
+      const int o = (j / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) w[o + r * Ns] = x[r];
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = w[i];
+    RegFFT<C, INV, N, Ns * R, Rem / R>::run(v);
+  }
+};
+template <typename C, bool INV, int N, int Ns>
+struct RegFFT<C, INV, N, Ns, 1> {
+  static __device__ __forceinline__ void run(C*) {}
+};
+template <typename C, bool INV, int N> __device__ __forceinline__ void reg_fft(C* v) { RegFFT<C, INV, N, 1, N>::run(v); }
+
+// FFT of `count` lines of length H in padded shared memory, one thread per line.
+// Line l starts at line_base(l) and has element stride es.
+template <typename C, bool INV, int H>
+__device__ __forceinline__ void smem_lines(C* buf, int count, int group, int gstride, int lstride, int es) {
+  for (int l = threadIdx.x; l < count; l += blockDim.x) {
+    C* p = buf + (l / group) * gstride + (l % group) * lstride;
+    C v[H];
+#pragma unroll
+    for (int i = 0; i < H; ++i) v[i] = p[i * es];
+    reg_fft<C, INV, H>(v);
+#pragma unroll
+    for (int i = 0; i < H; ++i) p[i * es] = v[i];
+  }
+}
+
+// Alive parity channels per centring (WHT index o = o0 + 2 o1 + 4 o2 of each channel),
+// as compile-time data so channel loops unroll with constant register indices.
+// CT: 0 plain (no fold), 1 I, 2 F, 3 C, 4 A (same order as the plan's offsets).
+template <int CT> struct Cent {
+  static constexpr int n = CT == 0 ? 1 : CT == 2 ? 2 : 4;
+  static __host__ __device__ constexpr int off(int c) {
+    return CT == 1 ? (c == 0 ? 0 : c == 1 ? 3 : c == 2 ? 5 : 6)
+         : CT == 2 ? (c == 0 ? 0 : 7)
+         : CT == 3 ? (c == 0 ? 0 : c == 1 ? 3 : c == 2 ? 4 : 7)
+         : CT == 4 ? (c == 0 ? 0 : c == 1 ? 6 : c == 2 ? 1 : 7) : 0;
+  }
+};
+
+// Two real fields share one complex transform on the fast path: slot s of the
+// channel workspace holds g_a + i g_b for fields a = 2s and b = 2s + 1 (b may be
+// absent at the end of a batch).  The forward gather separates them with
+// G_a(p) = (X(p) + conj X(-p)) / 2 and G_b(p) = (X(p) - conj X(-p)) / 2i, the backward
+// builds X = G_a + i G_b and the unfold reads field a from the real part and field b
+// from the imaginary part.  This halves the FFT work and the workspace traffic.
+
+// Row / column FFTs of nch padded H x H planes (row stride S = H + 1, plane stride
+// H * S), one thread per line, compile-time strides.
+template <typename C, bool INV, int H>
+__device__ __forceinline__ void smem_rows(C* buf, int nlines) {
+  constexpr int S = H + 1;
+  for (int l = threadIdx.x; l < nlines; l += blockDim.x) {
+    C* p = buf + l * S;
+    C v[H];
+#pragma unroll
+    for (int i = 0; i < H; ++i) v[i] = p[i];
+    reg_fft<C, INV, H>(v);
+#pragma unroll
+    for (int i = 0; i < H; ++i) p[i] = v[i];
+  }
+}
+template <typename C, bool INV, int H>
+__device__ __forceinline__ void smem_cols(C* buf, int nlines) {
+  constexpr int S = H + 1;
+  for (int l = threadIdx.x; l < nlines; l += blockDim.x) {
+    C* p = buf + (l / H) * (H * S) + (l % H);
+    C v[H];
+#pragma unroll
+    for (int i = 0; i < H; ++i) v[i] = p[i * S];
+    reg_fft<C, INV, H>(v);
+#pragma unroll
+    for (int i = 0; i < H; ++i) p[i * S] = v[i];
+  }
+}
+
+// Forward plane kernel, cubic H: fold (or plain load) of two fields + x FFT + y FFT
+// -> W[slot][c][z][y][x].
+template <typename T, int H, int CT>
+__global__ void k_plane_fwd_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                              const T* __restrict__ f0, const T* __restrict__ E, typename Cx<T>::type* __restrict__ W,
+                              int nfields) {
+  using C = typename Cx<T>::type;
+  constexpr int S = H + 1;
+  constexpr int PL = H * S;  // padded plane
+  const bool USE_E = E != nullptr;  // warp-uniform
+  constexpr int nch = Cent<CT>::n;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int iz = blockIdx.x, slot = blockIdx.y;
+  const int fa = 2 * slot;
+  const bool has_b = fa + 1 < nfields;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const size_t mvol = static_cast<size_t>(g->M[0]) * g->M[1] * g->M[2];
+  const T* srca = f0 + static_cast<size_t>(fa) * mvol;
+  const T* srcb = srca + mvol;
+  const T* Ea = USE_E ? E + static_cast<size_t>(fa) * mvol : nullptr;
+  const T* Eb = USE_E ? Ea + mvol : nullptr;
+  const T zero = static_cast<T>(0);
+  if constexpr (CT == 0) {
+    const size_t zoff = static_cast<size_t>(iz) * H * H;
+    for (int e = tid; e < H * H; e += nth) {
+      T va = srca[zoff + e];
+      T vb = has_b ? srcb[zoff + e] : zero;
+      if (USE_E) { va *= Ea[zoff + e]; if (has_b) vb *= Eb[zoff + e]; }
+      buf[(e / H) * S + (e % H)] = mk<C>(va, vb);
+    }
+  } else {
+    constexpr int M = 2 * H;
+    constexpr int VW = 16 / static_cast<int>(sizeof(T));  // elements per 16-byte vector
+    using V = typename Vec16<T>::type;
+    const C* ftx = tables + g->ftw_off[0];
+    const C ftz = tables[g->ftw_off[2] + iz];
+    const bool vec = (H % VW == 0) && (reinterpret_cast<uintptr_t>(srca) % 16 == 0) &&
+                     (!USE_E || reinterpret_cast<uintptr_t>(Ea) % 16 == 0);
+    if (vec) {
+      for (int e = tid; e < H * H / VW; e += nth) {
+        const int ix0 = (e % (H / VW)) * VW, iy = e / (H / VW);
+        T va[8][VW], vb[8][VW];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int idx = ((iz + ((k >> 2) & 1) * H) * M + iy + ((k >> 1) & 1) * H) * M + ix0 + (k & 1) * H;
+          vload<T>(va[k], srca + idx);
+          if (has_b) vload<T>(vb[k], srcb + idx);
+          else {
+#pragma unroll
+            for (int l = 0; l < VW; ++l) vb[k][l] = zero;
+          }
+          if (USE_E) {
+            T ea[VW];
+            vload<T>(ea, Ea + idx);
+#pragma unroll
+            for (int l = 0; l < VW; ++l) va[k][l] *= ea[l];
+            if (has_b) {
+              vload<T>(ea, Eb + idx);
+#pragma unroll
+              for (int l = 0; l < VW; ++l) vb[k][l] *= ea[l];
+            }
+          }
+        }
+        const C ty = ftx[iy];
+#pragma unroll
+        for (int l = 0; l < VW; ++l) {
+          T a8[8], b8[8];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) { a8[k] = va[k][l]; b8[k] = vb[k][l]; }
+          wht8(a8);
+          wht8(b8);
+          const int ix = ix0 + l;
+          const C tx = ftx[ix];
+#pragma unroll
+          for (int c = 0; c < nch; ++c) {
+            const int o = Cent<CT>::off(c);
+            C w = mk<C>(static_cast<T>(1), zero);
+            if (o & 1) w = tx;
+            if (o & 2) w = cmul(w, ty);
+            if (o & 4) w = cmul(w, ftz);
+            buf[c * PL + iy * S + ix] = cmul(mk<C>(a8[o], b8[o]), w);
+          }
+        }
+      }
+    } else {
+      for (int e = tid; e < H * H; e += nth) {
+        const int ix = e % H, iy = e / H;
+        T va[8], vb[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int idx = ((iz + ((k >> 2) & 1) * H) * M + iy + ((k >> 1) & 1) * H) * M + ix + (k & 1) * H;
+          va[k] = srca[idx];
+          vb[k] = has_b ? srcb[idx] : zero;
+          if (USE_E) { va[k] *= Ea[idx]; if (has_b) vb[k] *= Eb[idx]; }
+        }
+        wht8(va);
+        wht8(vb);
+        const C tx = ftx[ix], ty = ftx[iy];  // cubic: the y fold twiddle table equals x's
+#pragma unroll
+        for (int c = 0; c < nch; ++c) {
+          const int o = Cent<CT>::off(c);
+          C w = mk<C>(static_cast<T>(1), zero);
+          if (o & 1) w = tx;
+          if (o & 2) w = cmul(w, ty);
+          if (o & 4) w = cmul(w, ftz);
+          buf[c * PL + iy * S + ix] = cmul(mk<C>(va[o], vb[o]), w);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  smem_rows<C, false, H>(buf, nch * H);   // x lines
+  __syncthreads();
+  smem_cols<C, false, H>(buf, nch * H);   // y lines
+  __syncthreads();
+  constexpr int HV = H * H * H;
+  C* dst0 = W + static_cast<size_t>(slot) * nch * HV + iz * H * H;
+  for (int c = 0; c < nch; ++c)
+    for (int e = tid; e < H * H; e += nth) dst0[c * HV + e] = buf[c * PL + (e / H) * S + (e % H)];
+}
+
+// Backward plane kernel, cubic H: inverse x/y FFT of W[slot][c][iz] + unfold of the two
+// fields (real part -> field a, imaginary part -> field b).
+template <typename T, int H, int CT>
+__global__ void k_plane_bwd_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                              const typename Cx<T>::type* __restrict__ W, const T* __restrict__ E, T* __restrict__ f0,
+                              int nfields) {
+  using C = typename Cx<T>::type;
+  constexpr int S = H + 1;
+  constexpr int PL = H * S;
+  const bool USE_E = E != nullptr;  // warp-uniform
+  constexpr int nch = Cent<CT>::n;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int iz = blockIdx.x, slot = blockIdx.y;
+  const int fa = 2 * slot;
+  const bool has_b = fa + 1 < nfields;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const size_t hvol = static_cast<size_t>(H) * H * H;
+  constexpr int HV = H * H * H;
+  const C* src0 = W + static_cast<size_t>(slot) * nch * HV + iz * H * H;
+  for (int c = 0; c < nch; ++c)
+    for (int e = tid; e < H * H; e += nth) buf[c * PL + (e / H) * S + (e % H)] = src0[c * HV + e];
+  __syncthreads();
+  smem_rows<C, true, H>(buf, nch * H);
+  __syncthreads();
+  smem_cols<C, true, H>(buf, nch * H);
+  __syncthreads();
+  const size_t mvol = static_cast<size_t>(g->M[0]) * g->M[1] * g->M[2];
+  T* dsta = f0 + static_cast<size_t>(fa) * mvol;
+  T* dstb = dsta + mvol;
+  const T* Ea = USE_E ? E + static_cast<size_t>(fa) * mvol : nullptr;
+  const T* Eb = USE_E ? Ea + mvol : nullptr;
+  if constexpr (CT == 0) {
+    const T scale = static_cast<T>(1.0 / static_cast<double>(mvol));
+    const size_t zoff = static_cast<size_t>(iz) * H * H;
+    for (int e = tid; e < H * H; e += nth) {
+      const C x = buf[(e / H) * S + (e % H)];
+      T va = x.x * scale, vb = x.y * scale;
+      if (USE_E) { va *= Ea[zoff + e]; if (has_b) vb *= Eb[zoff + e]; }
+      dsta[zoff + e] = va;
+      if (has_b) dstb[zoff + e] = vb;
+    }
+  } else {
+    constexpr int M = 2 * H;
+    const T scale = static_cast<T>(1.0 / (8.0 * static_cast<double>(hvol)));
+    const C* ftx = tables + g->ftw_off[0];
+    const C ftz = tables[g->ftw_off[2] + iz];
+    {
+      for (int e = tid; e < H * H; e += nth) {
+        const int ix = e % H, iy = e / H;
+        T va[8], vb[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) { va[k] = static_cast<T>(0); vb[k] = static_cast<T>(0); }
+        const C tx = ftx[ix], ty = ftx[iy];
+#pragma unroll
+        for (int c = 0; c < nch; ++c) {
+          const int o = Cent<CT>::off(c);
+          C w = mk<C>(static_cast<T>(1), static_cast<T>(0));
+          if (o & 1) w = tx;
+          if (o & 2) w = cmul(w, ty);
+          if (o & 4) w = cmul(w, ftz);
+          const C y = cmulc(buf[c * PL + iy * S + ix], w);  // x * conj(w)
+          va[o] = y.x;
+          vb[o] = y.y;
+        }
+        wht8(va);
+        wht8(vb);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int idx = ((iz + ((k >> 2) & 1) * H) * M + iy + ((k >> 1) & 1) * H) * M + ix + (k & 1) * H;
+          T a = va[k] * scale, bq = vb[k] * scale;
+          if (USE_E) { a *= Ea[idx]; if (has_b) bq *= Eb[idx]; }
+          dsta[idx] = a;
+          if (has_b) dstb[idx] = bq;
+        }
+      }
+    }
+  }
+}
+
+constexpr int kZB = kFastZB;
+
+// Forward z FFT, cubic H: W[slot][c][z][y][x] (in) -> WT[slot][c][x][y][z] (z fastest,
+// out, same storage: each CTA reads and writes exactly the same addresses).  Thread
+// (yy, x) loads its z line straight into registers (coalesced across x); the
+// transposed store goes through shared memory.
+template <typename T, int H>
+__global__ void k_fft_z_fwd_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* W,
+                              typename Cx<T>::type* WT) {
+  using C = typename Cx<T>::type;
+  constexpr int S = H + 1;
+  constexpr int HV = H * H * H;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);  // [yy][x][z] padded
+  const int y0 = blockIdx.x * kZB, c = blockIdx.y, slot = blockIdx.z;
+  const int ny = min(kZB, H - y0);
+  const int tid = threadIdx.x;
+  const size_t base = (static_cast<size_t>(slot) * g->n_ch + c) * HV;
+  const int yy = tid / H, x = tid % H;
+  if (yy < ny) {
+    const C* src = W + base + (y0 + yy) * H + x;
+    C v[H];
+#pragma unroll
+    for (int z = 0; z < H; ++z) v[z] = src[z * H * H];
+    reg_fft<C, false, H>(v);
+    C* row = buf + (yy * H + x) * S;
+#pragma unroll
+    for (int z = 0; z < H; ++z) row[z] = v[z];
+  }
+  __syncthreads();
+  C* dst = WT + base;
+  const int run = ny * H;  // contiguous (yy, z) run per x
+  for (int e = tid; e < H * run; e += blockDim.x) {
+    const int xx = e / run, r = e % run;
+    const int y2 = r / H, z = r % H;
+    dst[(xx * H + y0) * H + r] = buf[(y2 * H + xx) * S + z];
+  }
+}
+
+// Backward: expand G0 from orbit representatives (ET table) + inverse z FFT, cubic H:
+// G0R[slot][o] -> W[slot][c][z][y][x].
+template <typename T, int H>
+__global__ void k_expand_ifft_z_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                                  const int2* __restrict__ ET, const typename Cx<T>::type* __restrict__ G0R,
+                                  typename Cx<T>::type* __restrict__ W) {
+  using C = typename Cx<T>::type;
+  constexpr int S = H + 1;
+  constexpr int PL = H * S;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int y0 = blockIdx.x * kZB, c = blockIdx.y, slot = blockIdx.z;
+  const int ny = min(kZB, H - y0);
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const size_t hvol = static_cast<size_t>(H) * H * H;
+  const int2* et = ET + static_cast<size_t>(c) * hvol;
+  const C* rep = G0R + static_cast<size_t>(slot) * g->n_orbits;
+  const C* ph = tables + g->ph_off;
+  for (int e = tid; e < ny * H * H; e += nth) {
+    const int x = e % H, z = (e / H) % H, yy = e / (H * H);
+    const int2 t = et[(static_cast<size_t>(z) * H + y0 + yy) * H + x];
+    buf[yy * PL + z * S + x] = cmulc(rep[t.x], ph[t.y]);  // G0R * e^{+2 pi i j/P}
+  }
+  __syncthreads();
+  smem_lines<C, true, H>(buf, ny * H, H, PL, 1, S);
+  __syncthreads();
+  C* dst = W + (static_cast<size_t>(slot) * g->n_ch + c) * hvol;
+  for (int e = tid; e < ny * H * H; e += nth) {
+    const int x = e % H, z = (e / H) % H, yy = e / (H * H);
+    dst[(static_cast<size_t>(z) * H + y0 + yy) * H + x] = buf[yy * PL + z * S + x];
+  }
+}
+
+
+// Spectral-ASU gather from the z-fastest packed workspace, cubic M (= 2H centred,
+// = H plain), D representative operations; separates the two fields of the slot on
+// the fly.  The geometry is staged in shared memory once per CTA.
+template <typename T, int M, int D, bool USE_K, bool PERM>
+__global__ void k_recon_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                          const uint32_t* __restrict__ spec_h, const T* __restrict__ K,
+                          const typename Cx<T>::type* __restrict__ WT, typename Cx<T>::type* __restrict__ F,
+                          int nfields) {
+  using C = typename Cx<T>::type;
+  __shared__ int sR[D][9];
+  __shared__ int sPS[D][3];
+  __shared__ int sTP[D][3];
+  __shared__ int sCh[8];
+  const int tid = threadIdx.x;
+  if (tid < D * 9) sR[tid / 9][tid % 9] = g->rep_R[tid / 9][tid % 9];
+  if (tid < D * 3) { sPS[tid / 3][tid % 3] = g->rep_ps[tid / 3][tid % 3]; sTP[tid / 3][tid % 3] = g->rep_tp[tid / 3][tid % 3]; }
+  if (tid < 8) sCh[tid] = g->chan_of_parity[tid];
+  __syncthreads();
+  const int s = blockIdx.x * blockDim.x + tid;
+  const int slot = blockIdx.y;
+  if (s >= g->n_spec) return;
+  const int fa = 2 * slot;
+  const bool has_b = fa + 1 < nfields;
+  const uint32_t hp = spec_h[s];
+  const int h[3] = {static_cast<int>(hp & 1023u), static_cast<int>((hp >> 10) & 1023u), static_cast<int>((hp >> 20) & 1023u)};
+  const bool cen = g->centered;
+  constexpr int Hc2 = M / 2;
+  const int Hc = cen ? Hc2 : M;
+  const int ls = cen ? 1 : 0;  // channel coordinate = q >> ls
+  const size_t hvol = static_cast<size_t>(Hc) * Hc * Hc;
+  const C* Wb = WT + static_cast<size_t>(slot) * g->n_ch * hvol;
+  const C* ph = tables + g->ph_off;
+  const int P = g->P, pmask = g->pmask;
+  const T half = static_cast<T>(0.5);
+  C acca = mk<C>(static_cast<T>(0), static_cast<T>(0));
+  C accb = acca;
+#pragma unroll
+  for (int r = 0; r < D; ++r) {
+    int q[3], qn[3];
+#pragma unroll
+    for (int dd = 0; dd < 3; ++dd) {
+      int v;
+      if (PERM) {
+        const int ps = sPS[r][dd];
+        v = h[ps & 3];
+        if (ps & 4) v = -v;
+      } else {
+        v = sR[r][dd] * h[0] + sR[r][3 + dd] * h[1] + sR[r][6 + dd] * h[2];
+      }
+      q[dd] = mod_m<M>(v);
+      qn[dd] = mod_m<M>(M - q[dd]);
+    }
+    int c = 0;
+    if (cen) {
+      c = sCh[(q[0] & 1) + 2 * (q[1] & 1) + 4 * (q[2] & 1)];
+      if (c < 0) continue;
+    }
+    const size_t base = static_cast<size_t>(c) * hvol;
+    const size_t idx = base + (static_cast<size_t>(q[0] >> ls) * Hc + (q[1] >> ls)) * Hc + (q[2] >> ls);
+    const size_t idn = base + (static_cast<size_t>(qn[0] >> ls) * Hc + (qn[1] >> ls)) * Hc + (qn[2] >> ls);
+    const C X = Wb[idx], Xn = Wb[idn];
+    const C Ga = mk<C>(half * (X.x + Xn.x), half * (X.y - Xn.y));   // (X + conj Xn) / 2
+    const C Gb = mk<C>(half * (X.y + Xn.y), half * (Xn.x - X.x));   // (X - conj Xn) / 2i
+    int j = h[0] * sTP[r][0] + h[1] * sTP[r][1] + h[2] * sTP[r][2];
+    j = pmask >= 0 ? (j & pmask) : ((j % P) + P) % P;
+    const C w = ph[j];
+    acca = cadd(acca, cmul(Ga, w));
+    accb = cadd(accb, cmul(Gb, w));
+  }
+  if (USE_K) { const T k = K[s]; acca = cscale(acca, k); accb = cscale(accb, k); }
+  F[static_cast<size_t>(fa) * g->n_spec + s] = acca;
+  if (has_b) F[static_cast<size_t>(fa + 1) * g->n_spec + s] = accb;
+}
+
+// Spectral-ASU gather when the 8 representative operations are the diagonal sign
+// matrices diag(+-1, +-1, +-1) (any translations): the 8 taps read G0 at the sign
+// images s.h of h, which all lie in one parity channel, and the Hermitian partner
+// X(-q) of tap s is tap ~s.  Eight workspace loads per point and slot.
+template <typename T, int M, bool USE_K>
+__global__ void k_recon_diag8(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                              const uint32_t* __restrict__ spec_h, const T* __restrict__ K,
+                              const typename Cx<T>::type* __restrict__ WT, typename Cx<T>::type* __restrict__ F,
+                              int nfields) {
+  using C = typename Cx<T>::type;
+  __shared__ int sTP[8][3];  // indexed by sign pattern
+  __shared__ int sCh[8];
+  const int tid = threadIdx.x;
+  if (tid < 24) sTP[tid / 3][tid % 3] = g->rep_tp[g->sign_op[tid / 3]][tid % 3];
+  if (tid < 8) sCh[tid] = g->chan_of_parity[tid];
+  __syncthreads();
+  const int s = blockIdx.x * blockDim.x + tid;
+  const int slot = blockIdx.y;
+  if (s >= g->n_spec) return;
+  const int fa = 2 * slot;
+  const bool has_b = fa + 1 < nfields;
+  const uint32_t hp = spec_h[s];
+  const int h0 = static_cast<int>(hp & 1023u), h1 = static_cast<int>((hp >> 10) & 1023u), h2 = static_cast<int>((hp >> 20) & 1023u);
+  const bool cen = g->centered;
+  const int Hc = cen ? M / 2 : M;
+  const int ls = cen ? 1 : 0;
+  const int hvol = Hc * Hc * Hc;
+  // per-axis (+h, -h) positions mod M, in channel coordinates
+  const int p0 = mod_m<M>(h0), p1 = mod_m<M>(h1), p2 = mod_m<M>(h2);
+  const int m0 = mod_m<M>(M - p0), m1 = mod_m<M>(M - p1), m2 = mod_m<M>(M - p2);
+  int c = 0;
+  if (cen) c = sCh[(p0 & 1) + 2 * (p1 & 1) + 4 * (p2 & 1)];
+  if (c < 0) {  // extinct parity class: every tap reads zero
+    const C z = mk<C>(static_cast<T>(0), static_cast<T>(0));
+    F[static_cast<size_t>(fa) * g->n_spec + s] = z;
+    if (has_b) F[static_cast<size_t>(fa + 1) * g->n_spec + s] = z;
+    return;
+  }
+  const int X0[2] = {(p0 >> ls) * Hc * Hc, (m0 >> ls) * Hc * Hc};
+  const int X1[2] = {(p1 >> ls) * Hc, (m1 >> ls) * Hc};
+  const int X2[2] = {p2 >> ls, m2 >> ls};
+  const C* Wb = WT + (static_cast<size_t>(slot) * g->n_ch + c) * hvol;
+  C X[8];
+#pragma unroll
+  for (int sg = 0; sg < 8; ++sg) X[sg] = Wb[X0[sg & 1] + X1[(sg >> 1) & 1] + X2[(sg >> 2) & 1]];
+  const C* ph = tables + g->ph_off;
+  const int P = g->P, pmask = g->pmask;
+  const T half = static_cast<T>(0.5);
+  C acca = mk<C>(static_cast<T>(0), static_cast<T>(0));
+  C accb = acca;
+#pragma unroll
+  for (int sg = 0; sg < 8; ++sg) {
+    const C Xs = X[sg], Xn = X[7 - sg];
+    const C Ga = mk<C>(half * (Xs.x + Xn.x), half * (Xs.y - Xn.y));
+    const C Gb = mk<C>(half * (Xs.y + Xn.y), half * (Xn.x - Xs.x));
+    int j = h0 * sTP[sg][0] + h1 * sTP[sg][1] + h2 * sTP[sg][2];
+    j = pmask >= 0 ? (j & pmask) : ((j % P) + P) % P;
+    const C w = ph[j];
+    acca = cadd(acca, cmul(Ga, w));
+    accb = cadd(accb, cmul(Gb, w));
+  }
+  if (USE_K) { const T k = K[s]; acca = cscale(acca, k); accb = cscale(accb, k); }
+  F[static_cast<size_t>(fa) * g->n_spec + s] = acca;
+  if (has_b) F[static_cast<size_t>(fa + 1) * g->n_spec + s] = accb;
+}
+
+// G0 at orbit representatives of the two fields of a slot, packed as G_a + i G_b.
+// Each thread serves SPT consecutive slots, reusing the table entries and keeping
+// several independent spectrum gathers in flight.
+constexpr int kRepSlots = 4;
+template <typename T>
+__global__ void k_inv_recon_reps(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                                 const int32_t* __restrict__ inv_spec, const int32_t* __restrict__ inv_phase,
+                                 const typename Cx<T>::type* __restrict__ F, typename Cx<T>::type* __restrict__ G0R,
+                                 int nfields) {
+  using C = typename Cx<T>::type;
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= g->n_orbits) return;
+  const int slot0 = blockIdx.y * kRepSlots;
+  const int nslots = (nfields + 1) / 2;
+  const int d = g->d;
+  const int ns = g->n_spec;
+  const C* ph = tables + g->ph_off;
+  C acc[2 * kRepSlots];
+#pragma unroll
+  for (int k = 0; k < 2 * kRepSlots; ++k) acc[k] = mk<C>(static_cast<T>(0), static_cast<T>(0));
+  for (int a = 0; a < d; ++a) {
+    const int s = inv_spec[static_cast<size_t>(o) * d + a];
+    if (s == 0) continue;
+    const int si = (s > 0 ? s : -s) - 1;
+    const C w = ph[inv_phase[static_cast<size_t>(o) * d + a]];
+#pragma unroll
+    for (int k = 0; k < 2 * kRepSlots; ++k) {
+      const int f = 2 * slot0 + k;
+      if (f < nfields) {
+        C v = F[static_cast<size_t>(f) * ns + si];
+        if (s < 0) v = cconj(v);
+        acc[k] = cadd(acc[k], cmulc(v, w));
+      }
+    }
+  }
+  const T inv_d = static_cast<T>(1.0 / static_cast<double>(d));
+#pragma unroll
+  for (int k = 0; k < kRepSlots; ++k) {
+    const int slot = slot0 + k;
+    if (slot < nslots) {
+      const C a = acc[2 * k], b = acc[2 * k + 1];
+      G0R[static_cast<size_t>(slot) * g->n_orbits + o] = mk<C>(inv_d * (a.x - b.y), inv_d * (a.y + b.x));
+    }
+  }
+}
+
+// G0 at orbit representatives for one field, with the field's whole spectrum staged
+// in shared memory (one CTA per field and representative range): every alias gather
+// is a shared-memory read.  Aliases are packed as spec+1 (bits 0-19), conjugation
+// (bit 20) and phase numerator (bits 21-31); with d = 8 a thread reads its
+// representative's 8 entries as two 16-byte loads.  Output layout: G0RP[slot][o][f&1].
+template <typename T, int D>
+__global__ void k_inv_recon_reps_smem(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                                      const uint32_t* __restrict__ inv_pk, const typename Cx<T>::type* __restrict__ F,
+                                      typename Cx<T>::type* __restrict__ G0RP, int reps_per_part) {
+  using C = typename Cx<T>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* sF = reinterpret_cast<C*>(smem_raw);
+  const int ns = g->n_spec;
+  const int f = blockIdx.y;
+  const C* Ff = F + static_cast<size_t>(f) * ns;
+  for (int i = threadIdx.x; i < ns; i += blockDim.x) sF[i] = Ff[i];
+  __syncthreads();
+  const C* ph = tables + g->ph_off;
+  const T inv_d = static_cast<T>(1.0 / static_cast<double>(D));
+  const int o0 = blockIdx.x * reps_per_part;
+  const int o1 = min(g->n_orbits, o0 + reps_per_part);
+  C* out = G0RP + static_cast<size_t>(f >> 1) * g->n_orbits * 2 + (f & 1);
+  for (int o = o0 + threadIdx.x; o < o1; o += blockDim.x) {
+    uint32_t e[D];
+    if constexpr (D == 8) {
+      const uint4* p4 = reinterpret_cast<const uint4*>(inv_pk + static_cast<size_t>(o) * 8);
+      const uint4 u0 = p4[0], u1 = p4[1];
+      e[0] = u0.x; e[1] = u0.y; e[2] = u0.z; e[3] = u0.w; e[4] = u1.x; e[5] = u1.y; e[6] = u1.z; e[7] = u1.w;
+    } else {
+#pragma unroll
+      for (int a = 0; a < D; ++a) e[a] = inv_pk[static_cast<size_t>(o) * D + a];
+    }
+    C acc = mk<C>(static_cast<T>(0), static_cast<T>(0));
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+      const uint32_t sp = e[a] & 0xFFFFFu;
+      if (sp == 0) continue;
+      C v = sF[sp - 1];
+      if (e[a] & (1u << 20)) v = cconj(v);
+      acc = cadd(acc, cmulc(v, ph[e[a] >> 21]));
+    }
+    out[static_cast<size_t>(o) * 2] = cscale(acc, inv_d);
+  }
+}
+
+// Backward expansion from per-field representatives (G0RP[slot][o][a|b]) + inverse z
+// FFT: thread (yy, x) assembles its z line X = (G_a + i G_b) e^{+2 pi i j/P} in
+// registers, transforms it and stores it coalesced across x.  No shared memory.
+template <typename T, int H>
+__global__ void k_expand2_ifft_z_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                                   const int2* __restrict__ ET, const typename Cx<T>::type* __restrict__ G0RF,
+                                   typename Cx<T>::type* __restrict__ W, int nfields) {
+  using C = typename Cx<T>::type;
+  constexpr int HV = H * H * H;
+  const int y0 = blockIdx.x * kZB, c = blockIdx.y, slot = blockIdx.z;
+  const int ny = min(kZB, H - y0);
+  const int tid = threadIdx.x;
+  const int yy = tid / H, x = tid % H;
+  if (yy >= ny) return;
+  const int y = y0 + yy;
+  const int2* et = ET + static_cast<size_t>(c) * HV + y * H + x;
+  const bool has_b = 2 * slot + 1 < nfields;
+  const C* rp = G0RF + static_cast<size_t>(slot) * g->n_orbits * 2;
+  const C* ph = tables + g->ph_off;
+  C v[H];
+#pragma unroll
+  for (int z = 0; z < H; ++z) {
+    const int2 t = et[z * H * H];
+    const C a = rp[2 * t.x];
+    const C b = has_b ? rp[2 * t.x + 1] : mk<C>(static_cast<T>(0), static_cast<T>(0));
+    v[z] = cmulc(mk<C>(a.x - b.y, a.y + b.x), ph[t.y]);
+  }
+  reg_fft<C, true, H>(v);
+  C* dst = W + (static_cast<size_t>(slot) * g->n_ch + c) * HV + y * H + x;
+#pragma unroll
+  for (int z = 0; z < H; ++z) dst[z * H * H] = v[z];
+}
+
+
+constexpr int kMaxDynSmemFast = 227 * 1024;
+
+#define CFFT_FOR_H(H, ...)                                                        \
+  switch (H) {                                                                    \
+    case 4: { constexpr int HH = 4; __VA_ARGS__; } break;                         \
+    case 6: { constexpr int HH = 6; __VA_ARGS__; } break;                         \
+    case 8: { constexpr int HH = 8; __VA_ARGS__; } break;                         \
+    case 12: { constexpr int HH = 12; __VA_ARGS__; } break;                       \
+    case 16: { constexpr int HH = 16; __VA_ARGS__; } break;                       \
+    case 24: { constexpr int HH = 24; __VA_ARGS__; } break;                       \
+    case 32: { constexpr int HH = 32; __VA_ARGS__; } break;                       \
+    default: { constexpr int HH = sizeof(T) == 4 ? 48 : 32; __VA_ARGS__; } break; \
+  }
+
+#define CFFT_FOR_M(M, ...)                                        \
+  switch (M) {                                                     \
+    case 4: { constexpr int MM = 4; __VA_ARGS__; } break;         \
+    case 6: { constexpr int MM = 6; __VA_ARGS__; } break;         \
+    case 8: { constexpr int MM = 8; __VA_ARGS__; } break;         \
+    case 12: { constexpr int MM = 12; __VA_ARGS__; } break;       \
+    case 16: { constexpr int MM = 16; __VA_ARGS__; } break;       \
+    case 24: { constexpr int MM = 24; __VA_ARGS__; } break;       \
+    case 32: { constexpr int MM = 32; __VA_ARGS__; } break;       \
+    case 48: { constexpr int MM = 48; __VA_ARGS__; } break;       \
+    case 64: { constexpr int MM = 64; __VA_ARGS__; } break;       \
+    default: { constexpr int MM = 96; __VA_ARGS__; } break;       \
+  }
+
+#define CFFT_FOR_CT(CTV, ...)                                      \
+  switch (CTV) {                                                   \
+    case 1: { constexpr int CTT = 1; __VA_ARGS__; } break;         \
+    case 2: { constexpr int CTT = 2; __VA_ARGS__; } break;         \
+    case 3: { constexpr int CTT = 3; __VA_ARGS__; } break;         \
+    case 4: { constexpr int CTT = 4; __VA_ARGS__; } break;         \
+    default: { constexpr int CTT = 0; __VA_ARGS__; } break;        \
+  }
+
+inline Status fast_cuda(cudaError_t e, const char* what, std::string* err) {
+  if (e == cudaSuccess) return Status::kOk;
+  *err = std::string(what) + ": " + cudaGetErrorString(e);
+  return Status::kCuda;
+}
+
+// Per-device set-up of this unit: its own copy of the constant-memory twiddles
+// e^{-2 pi i j / N} (FP64 values rounded) and the shared-memory limits of its kernels.
+template <typename T, int GROUP>
+Status fast_unit_init(std::string* err) {
+  static std::mutex mu;
+  static bool done[64] = {false};
+  int dev = 0;
+  Status s = fast_cuda(cudaGetDevice(&dev), "cudaGetDevice", err);
+  if (s != Status::kOk) return s;
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= 0 && dev < 64 && done[dev]) return Status::kOk;
+  std::vector<float2> tf(kTwTotal);
+  std::vector<double2> td(kTwTotal);
+  const int sizes[8] = {4, 6, 8, 12, 16, 24, 32, 48};
+  const int offs[8] = {kTwOff4, kTwOff6, kTwOff8, kTwOff12, kTwOff16, kTwOff24, kTwOff32, kTwOff48};
+  for (int k = 0; k < 8; ++k)
+    for (int j = 0; j < sizes[k]; ++j) {
+      const double c = std::cos(2.0 * M_PI * j / sizes[k]), sn = -std::sin(2.0 * M_PI * j / sizes[k]);
+      td[offs[k] + j] = make_double2(c, sn);
+      tf[offs[k] + j] = make_float2(static_cast<float>(c), static_cast<float>(sn));
+    }
+  if ((s = fast_cuda(cudaMemcpyToSymbol(c_tw_f, tf.data(), sizeof(float2) * kTwTotal), "upload twiddles", err)) != Status::kOk) return s;
+  if ((s = fast_cuda(cudaMemcpyToSymbol(c_tw_d, td.data(), sizeof(double2) * kTwTotal), "upload twiddles", err)) != Status::kOk) return s;
+  for (int H : {4, 6, 8, 12, 16, 24, 32, 48}) {
+    if (!fast_size_ok(H, sizeof(T))) continue;
+    CFFT_FOR_H(H, {
+      if constexpr (GROUP == 0) {
+        for (int ct = 0; ct < 5; ++ct) {
+          CFFT_FOR_CT(ct, {
+            cudaFuncSetAttribute(k_plane_fwd_h<T, HH, CTT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
+            cudaFuncSetAttribute(k_plane_bwd_h<T, HH, CTT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
+          });
+        }
+      } else {
+        cudaFuncSetAttribute(k_fft_z_fwd_h<T, HH>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
+        cudaFuncSetAttribute(k_expand_ifft_z_h<T, HH>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
+      }
+    });
+  }
+  if constexpr (GROUP == 1) {
+    cudaFuncSetAttribute(k_inv_recon_reps_smem<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
+    cudaFuncSetAttribute(k_inv_recon_reps_smem<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
+    cudaFuncSetAttribute(k_inv_recon_reps_smem<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
+    cudaFuncSetAttribute(k_inv_recon_reps_smem<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
+  }
+  if ((s = fast_cuda(cudaGetLastError(), "set shared-memory attributes", err)) != Status::kOk) return s;
+  if (dev >= 0 && dev < 64) done[dev] = true;
+  return Status::kOk;
+}
+
+// One fast-path stage for `a.nb` fields (two per workspace slot).
+template <typename T, int GROUP>
+Status fast_unit_launch(const FastArgs& a, std::string* err) {
+  using C = typename Cx<T>::type;
+  const DevGeom* g = static_cast<const DevGeom*>(a.geom);
+  const C* tab = static_cast<const C*>(a.tables);
+  C* W = static_cast<C*>(a.W);
+  C* G0R = static_cast<C*>(a.G0R);
+  const T* f0 = static_cast<const T*>(a.f0);
+  const T* E = static_cast<const T*>(a.E);
+  C* F = static_cast<C*>(a.F);
+  const C* Fin = static_cast<const C*>(a.Fin);
+  T* f0_out = static_cast<T*>(a.f0_out);
+  cudaStream_t st = static_cast<cudaStream_t>(a.stream);
+  const int H = a.H, nb = a.nb, nch = a.n_ch;
+  const int nslots = (nb + 1) / 2;
+  const size_t cs = sizeof(C);
+  if constexpr (GROUP == 0) {
+    const int thr_plane = std::max(128, ((nch * H + 31) / 32) * 32);
+    const size_t smem_plane = static_cast<size_t>(nch) * H * (H + 1) * cs;
+    if (a.stage == 0) {
+      CFFT_FOR_H(H, {
+        CFFT_FOR_CT(a.cent_type, {
+          k_plane_fwd_h<T, HH, CTT><<<dim3(H, nslots), thr_plane, smem_plane, st>>>(g, tab, f0, E, W, nb);
+        });
+      });
+    } else {
+      CFFT_FOR_H(H, {
+        CFFT_FOR_CT(a.cent_type, {
+          k_plane_bwd_h<T, HH, CTT><<<dim3(H, nslots), thr_plane, smem_plane, st>>>(g, tab, W, E, f0_out, nb);
+        });
+      });
+    }
+  } else {
+    const int thr_z = std::max(64, ((kZB * H + 31) / 32) * 32);
+    const size_t smem_z = static_cast<size_t>(kZB) * H * (H + 1) * cs;
+    const dim3 gz((H + kZB - 1) / kZB, nch, nslots);
+    switch (a.stage) {
+      case 1:
+        CFFT_FOR_H(H, { k_fft_z_fwd_h<T, HH><<<gz, thr_z, smem_z, st>>>(g, W, W); });
+        break;
+      case 2: {
+        const dim3 gr((a.n_spec + 255) / 256, nslots);
+        const int M = a.centered ? 2 * H : H;
+        const T* K = static_cast<const T*>(a.K);
+        const uint32_t* sh = static_cast<const uint32_t*>(a.spec_h);
+        const bool use_K = a.use_K, perm = a.rep_perm;
+        if (a.rep_diag8) {
+          CFFT_FOR_M(M, {
+            if (use_K) k_recon_diag8<T, MM, true><<<gr, 256, 0, st>>>(g, tab, sh, K, W, F, nb);
+            else k_recon_diag8<T, MM, false><<<gr, 256, 0, st>>>(g, tab, sh, nullptr, W, F, nb);
+          });
+          break;
+        }
+#define CFFT_RECON_D(DD)                                                                                  \
+  CFFT_FOR_M(M, {                                                                                         \
+    if (use_K) {                                                                                          \
+      if (perm) k_recon_h<T, MM, DD, true, true><<<gr, 256, 0, st>>>(g, tab, sh, K, W, F, nb);            \
+      else k_recon_h<T, MM, DD, true, false><<<gr, 256, 0, st>>>(g, tab, sh, K, W, F, nb);                \
+    } else {                                                                                              \
+      if (perm) k_recon_h<T, MM, DD, false, true><<<gr, 256, 0, st>>>(g, tab, sh, nullptr, W, F, nb);     \
+      else k_recon_h<T, MM, DD, false, false><<<gr, 256, 0, st>>>(g, tab, sh, nullptr, W, F, nb);         \
+    }                                                                                                     \
+  })
+        switch (a.d) {
+          case 1: CFFT_RECON_D(1); break;
+          case 2: CFFT_RECON_D(2); break;
+          case 4: CFFT_RECON_D(4); break;
+          default: CFFT_RECON_D(8); break;
+        }
+#undef CFFT_RECON_D
+        break;
+      }
+      case 3: {
+        const int no = a.n_orbits;
+        if (a.reps_smem) {
+          const int parts = nb >= 100 ? 1 : std::max(1, std::min((148 + nb - 1) / nb, (no + 1023) / 1024));
+          const int per = (no + parts - 1) / parts;
+          const size_t smem = static_cast<size_t>(a.n_spec) * cs;
+          const uint32_t* pk = static_cast<const uint32_t*>(a.inv_pk);
+          switch (a.d) {
+            case 1: k_inv_recon_reps_smem<T, 1><<<dim3(parts, nb), 1024, smem, st>>>(g, tab, pk, Fin, G0R, per); break;
+            case 2: k_inv_recon_reps_smem<T, 2><<<dim3(parts, nb), 1024, smem, st>>>(g, tab, pk, Fin, G0R, per); break;
+            case 4: k_inv_recon_reps_smem<T, 4><<<dim3(parts, nb), 1024, smem, st>>>(g, tab, pk, Fin, G0R, per); break;
+            default: k_inv_recon_reps_smem<T, 8><<<dim3(parts, nb), 1024, smem, st>>>(g, tab, pk, Fin, G0R, per); break;
+          }
+          break;
+        }
+        k_inv_recon_reps<T><<<dim3((no + 127) / 128, (nslots + kRepSlots - 1) / kRepSlots), 128, 0, st>>>(
+            g, tab, static_cast<const int32_t*>(a.inv_spec), static_cast<const int32_t*>(a.inv_phase), Fin, G0R, nb);
+        break;
+      }
+      default:
+        CFFT_FOR_H(H, {
+          if (a.reps_smem)
+            k_expand2_ifft_z_h<T, HH><<<gz, thr_z, 0, st>>>(g, tab, static_cast<const int2*>(a.expand), G0R, W, nb);
+          else
+            k_expand_ifft_z_h<T, HH><<<gz, thr_z, smem_z, st>>>(g, tab, static_cast<const int2*>(a.expand), G0R, W);
+        });
+        break;
+    }
+  }
+  return fast_cuda(cudaGetLastError(), "fast-path launch", err);
+}
+
+}  // namespace
+}  // namespace cfft

@@ -1,0 +1,9 @@
+// Fast-path plane stages (0, 5), double precision.
+#include "fast_kernels.cuh"
+
+namespace cfft {
+
+Status fast_planes_f64(const FastArgs& a, std::string* err) { return fast_unit_launch<double, 0>(a, err); }
+Status fast_init_planes_f64(std::string* err) { return fast_unit_init<double, 0>(err); }
+
+}  // namespace cfft

@@ -178,9 +178,6 @@ std::vector<SpecPoint> calc_spectral_asu(const std::vector<SymOp>& ops, const in
   std::vector<long> work;
   for (long lin = 0; lin < total; ++lin) {
     if (visited[lin]) continue;
-    int k[3];
-    long rem = lin;
-    k[0] = rem % n[0]; rem /= n[0]; k[1] = rem % n[1]; k[2] = rem / n[1];
     visited[lin] = 1;
     int orbit = 1;
     long min_lin = lin;
@@ -207,7 +204,7 @@ std::vector<SpecPoint> calc_spectral_asu(const std::vector<SymOp>& ops, const in
       }
     }
     int kr[3];
-    rem = min_lin;
+    long rem = min_lin;
     kr[0] = rem % n[0]; rem /= n[0]; kr[1] = rem % n[1]; kr[2] = rem / n[1];
     // Extinction filter: |sum_{g in Stab(k)} exp(-2 pi i k.t_g / N)| > 1e-5.
     double sr = 0.0, si = 0.0;
