@@ -249,11 +249,11 @@ def run_ours(args):
     us_field = ms_step * 1000.0 / fields_total  # whole-job time per field
     # e2e through the host-buffer C entry points with pinned host memory
     e2e = None
-    if rank == 0 or world > 1:
+    if not args.no_e2e:
         f0_h = torch.empty(f0.shape, dtype=torch.float32, pin_memory=True)
         f0_h.copy_(f0.cpu())
         F_h = torch.empty((B, plan.n_spec), dtype=torch.complex64, pin_memory=True)
-        out_h = torch.empty_like(f0_h)
+        out_h = torch.empty(f0.shape, dtype=torch.float32, pin_memory=True)  # empty_like would be pageable
 
         def e2e_step():
             lib.cfft_forward_host(h, ctypes.c_void_p(f0_h.data_ptr()), ctypes.c_void_p(F_h.data_ptr()), B)
@@ -273,8 +273,24 @@ def run_ours(args):
         e2e_us = te.item() * 1e6 / fields_total
         fb = 4 * int(np.prod(M)) * B
         sb = 8 * plan.n_spec * B
+        # Host-link bound of this step: each call is limited by its larger direction
+        # (forward: f0 in; backward: f0 out), timed as plain pinned copies of f0.
+        dbuf = torch.empty_like(f0)
+        bw = {}
+        for name, src, dst in (("h2d", f0_h, dbuf), ("d2h", dbuf, out_h)):
+            dst.copy_(src, non_blocking=True)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            for _ in range(3):
+                dst.copy_(src, non_blocking=True)
+            torch.cuda.synchronize()
+            bw[name] = 3 * fb / (time.perf_counter() - t1) / 1e9
+        del dbuf
+        bound_us = (fb / bw["h2d"] + fb / bw["d2h"]) / 1e3 / B
         e2e = {"value": e2e_us, "unit": UNIT, "h2d_bytes_per_step": fb + sb, "d2h_bytes_per_step": sb + fb,
-               "note": "cfft_forward_host + cfft_backward_host, pinned host buffers, copies inside the timed region"}
+               "pcie_gbs": {k: round(v, 2) for k, v in bw.items()}, "copy_bound": round(bound_us, 3),
+               "note": "cfft_forward_host + cfft_backward_host, pinned host buffers, copies inside the timed region; "
+                       "copy_bound = f0 bytes in and out at the measured pinned copy rates, per field"}
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -332,6 +348,7 @@ def main():
     ap.add_argument("--batch", type=int, default=128)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing (profiling runs)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

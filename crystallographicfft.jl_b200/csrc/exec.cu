@@ -412,16 +412,17 @@ Status launch_stage(Plan* p, int stage, const T* f0, typename Cx<T>::type* F, co
     a.inv_spec = p->d_inv_spec; a.inv_phase = p->d_inv_phase; a.inv_pk = p->d_inv_pk; a.expand = p->d_expand;
     a.W = W;
     a.G0R = p->d_g0r ? static_cast<char*>(p->d_g0r) + lane * p->g0r_lane_bytes : nullptr;
+    a.FT = p->d_ft ? static_cast<char*>(p->d_ft) + lane * p->ft_lane_bytes : nullptr;
     a.f0 = f0; a.F = F; a.Fin = Fin; a.f0_out = f0_out; a.E = E;
     a.stage = stage; a.nb = nb; a.H = p->fast_h; a.n_ch = T_.n_ch; a.centered = T_.centered ? 1 : 0;
     a.cent_type = p->cent_type; a.d = T_.d;
     a.n_spec = static_cast<int>(T_.spec.size()); a.n_orbits = static_cast<int>(T_.orbit_rep.size());
-    a.use_K = use_K; a.rep_diag8 = p->rep_diag8; a.rep_perm = p->rep_perm; a.reps_smem = p->reps_smem;
+    a.use_K = use_K; a.rep_diag8 = p->rep_diag8; a.rep_perm = p->rep_perm; a.reps_quad = p->reps_quad;
     a.stream = st;
     const bool planes = stage == 0 || stage == 5;
     Status s = sizeof(T) == 4 ? (planes ? fast_planes_f32(a, err) : fast_other_f32(a, err))
                               : (planes ? fast_planes_f64(a, err) : fast_other_f64(a, err));
-    ++g_launches;
+    g_launches += (stage == 3 && p->reps_quad) ? 2 : 1;  // regroup + gather
     return s;
   }
   switch (stage) {
@@ -714,10 +715,10 @@ Status plan_device_init(Plan* p, std::string* err) {
   if ((st = alloc(&p->d_work_T, p->lanes * p->w_lane_bytes, "channel workspace")) != Status::kOk) return st;
   if ((st = alloc(&p->d_work_F, B * T.spec.size() * cs, "spectrum workspace")) != Status::kOk) return st;
   if ((st = alloc(&p->d_work_E, B * mvol * rs, "interaction workspace")) != Status::kOk) return st;
-  // Per-field representative gather from a shared-memory copy of the spectrum.
+  // Packed alias rows (spec+1 in 20 bits, conj, phase in 11 bits) for the quad gather.
   std::vector<uint32_t> inv_pk;
-  p->reps_smem = p->fast_h && T.spec.size() * cs <= 200 * 1024 && T.spec.size() < (1u << 20) - 1 && T.P <= 2048;
-  if (p->reps_smem) {
+  p->reps_quad = p->fast_h && T.spec.size() < (1u << 20) - 1 && T.P <= 2048 && T.orbit_rep.size() < (1u << 21);
+  if (p->reps_quad) {
     inv_pk.resize(T.inv_spec.size());
     for (size_t k = 0; k < inv_pk.size(); ++k) {
       const int sp = T.inv_spec[k];
@@ -727,9 +728,16 @@ Status plan_device_init(Plan* p, std::string* err) {
     if ((st = alloc(&p->d_inv_pk, inv_pk.size() * 4, "packed inverse table")) != Status::kOk) return st;
   }
   if (p->fast_h) {
-    if ((st = alloc(&p->d_expand, expand.size() * sizeof(int2), "expansion table")) != Status::kOk) return st;
-    p->g0r_lane_bytes = (((chunk + 1) * T.orbit_rep.size() * cs + 255) / 256) * 256;
+    // The quad path reads the expansion entries packed in 32 bits (orbit | phase << 21).
+    if ((st = alloc(&p->d_expand, expand.size() * (p->reps_quad ? 4 : sizeof(int2)), "expansion table")) != Status::kOk)
+      return st;
+    const size_t chunk4 = (chunk + 3) / 4 * 4;  // quads of fields
+    p->g0r_lane_bytes = (((p->reps_quad ? chunk4 : chunk + 1) * T.orbit_rep.size() * cs + 255) / 256) * 256;
     if ((st = alloc(&p->d_g0r, p->lanes * p->g0r_lane_bytes, "representative workspace")) != Status::kOk) return st;
+    if (p->reps_quad) {
+      p->ft_lane_bytes = ((chunk4 * T.spec.size() * cs + 255) / 256) * 256;
+      if ((st = alloc(&p->d_ft, p->lanes * p->ft_lane_bytes, "grouped spectra")) != Status::kOk) return st;
+    }
   }
   CFFT_CUDA(cudaMemcpy(p->d_geom, &g, sizeof(g), cudaMemcpyHostToDevice), "upload geometry");
   CFFT_CUDA(cudaMemcpy(p->d_tables, tab.data(), tab.size(), cudaMemcpyHostToDevice), "upload tables");
@@ -740,9 +748,15 @@ Status plan_device_init(Plan* p, std::string* err) {
     CFFT_CUDA(cudaMemcpy(p->d_inv_phase, T.inv_phase.data(), T.inv_phase.size() * 4, cudaMemcpyHostToDevice), "upload inv phase");
     CFFT_CUDA(cudaMemcpy(p->d_img_mask, masks.data(), masks.size() * 4, cudaMemcpyHostToDevice), "upload masks");
   }
-  if (p->fast_h)
+  if (p->fast_h && p->reps_quad) {
+    std::vector<uint32_t> epk(expand.size());
+    for (size_t i = 0; i < expand.size(); ++i)
+      epk[i] = static_cast<uint32_t>(expand[i].x) | (static_cast<uint32_t>(expand[i].y) << 21);
+    CFFT_CUDA(cudaMemcpy(p->d_expand, epk.data(), epk.size() * 4, cudaMemcpyHostToDevice), "upload expansion");
+  } else if (p->fast_h) {
     CFFT_CUDA(cudaMemcpy(p->d_expand, expand.data(), expand.size() * sizeof(int2), cudaMemcpyHostToDevice), "upload expansion");
-  if (p->reps_smem)
+  }
+  if (p->reps_quad)
     CFFT_CUDA(cudaMemcpy(p->d_inv_pk, inv_pk.data(), inv_pk.size() * 4, cudaMemcpyHostToDevice), "upload packed table");
   // Orbit expansion writes only alive positions; channel positions never written stay zero.
   CFFT_CUDA(cudaMemset(p->d_work_T, 0, p->lanes * p->w_lane_bytes), "clear workspace");
@@ -790,7 +804,7 @@ Status plan_upload_kernel(Plan* p, std::string* err) {
 void plan_device_free(Plan* p) {
   void** bufs[] = {&p->d_geom, &p->d_tables, &p->d_spec_h, &p->d_K, &p->d_orbit_rep, &p->d_inv_spec,
                    &p->d_inv_phase, &p->d_img_mask, &p->d_fill_map, &p->d_work_T, &p->d_work_F,
-                   &p->d_work_E, &p->d_stage_in, &p->d_stage_out, &p->d_expand, &p->d_g0r, &p->d_inv_pk};
+                   &p->d_work_E, &p->d_stage_in, &p->d_stage_out, &p->d_expand, &p->d_g0r, &p->d_inv_pk, &p->d_ft};
   for (void** b : bufs)
     if (*b) { cudaFree(*b); *b = nullptr; }
   if (p->own_stream) { cudaStreamDestroy(static_cast<cudaStream_t>(p->own_stream)); p->own_stream = nullptr; }
@@ -799,6 +813,11 @@ void plan_device_free(Plan* p) {
     if (p->ev_join[l]) { cudaEventDestroy(static_cast<cudaEvent_t>(p->ev_join[l])); p->ev_join[l] = nullptr; }
   }
   if (p->ev_fork) { cudaEventDestroy(static_cast<cudaEvent_t>(p->ev_fork)); p->ev_fork = nullptr; }
+  for (void** sp : {&p->h2d_stream, &p->d2h_stream})
+    if (*sp) { cudaStreamDestroy(static_cast<cudaStream_t>(*sp)); *sp = nullptr; }
+  for (int i = 0; i < Plan::kHostPieces; ++i)
+    for (void** ep : {&p->ev_in[i], &p->ev_done[i]})
+      if (*ep) { cudaEventDestroy(static_cast<cudaEvent_t>(*ep)); *ep = nullptr; }
 }
 
 Status exec_forward(Plan* p, const void* f0, void* F, int B, void* stream, std::string* err) {
@@ -945,36 +964,85 @@ Status exec_sub_to_full(Plan* p, const void* f0, void* u, int B, void* stream, s
   return Status::kOk;
 }
 
-// which: 0 forward, 1 backward, 2 scft step (in place on the host buffer `out`)
+// which: 0 forward, 1 backward, 2 scft step (in place on the host buffer `out`).
+// The batch is cut into up to kHostPieces pieces of whole fields; piece i is copied in
+// on h2d_stream, transformed on own_stream once its copy has landed, and copied out on
+// d2h_stream, so the host<->device copies of different pieces (and the transforms)
+// overlap.  The call returns when every output byte is in the host buffer.
 Status exec_host(Plan* p, int which, const void* in, void* out, int B, std::string* err) {
   Status st = check_batch(p, B, err);
   if (st != Status::kOk) return st;
   const PlanTables& T = p->T;
   const size_t rs = p->precision, cs = 2 * rs;
-  const size_t fbytes = static_cast<size_t>(B) * T.M[0] * T.M[1] * T.M[2] * rs;
-  const size_t sbytes = static_cast<size_t>(B) * T.spec.size() * cs;
-  const size_t fmax = static_cast<size_t>(p->max_batch) * T.M[0] * T.M[1] * T.M[2] * rs;
-  const size_t smax = static_cast<size_t>(p->max_batch) * T.spec.size() * cs;
+  const size_t fvol = static_cast<size_t>(T.M[0]) * T.M[1] * T.M[2] * rs;   // bytes per field
+  const size_t svol = T.spec.size() * cs;                                    // bytes per spectrum
+  const size_t fmax = static_cast<size_t>(p->max_batch) * fvol;
+  const size_t smax = static_cast<size_t>(p->max_batch) * svol;
   if (!p->d_stage_in) {
     CFFT_CUDA(cudaMalloc(&p->d_stage_in, std::max(fmax, smax)), "alloc staging");
     CFFT_CUDA(cudaMalloc(&p->d_stage_out, std::max(fmax, smax)), "alloc staging");
     p->workspace_bytes += 2 * std::max(fmax, smax);
   }
-  cudaStream_t s = static_cast<cudaStream_t>(p->own_stream);
-  if (which == 0) {
-    CFFT_CUDA(cudaMemcpyAsync(p->d_stage_in, in, fbytes, cudaMemcpyHostToDevice, s), "H2D");
-    if ((st = exec_forward(p, p->d_stage_in, p->d_stage_out, B, s, err)) != Status::kOk) return st;
-    CFFT_CUDA(cudaMemcpyAsync(out, p->d_stage_out, sbytes, cudaMemcpyDeviceToHost, s), "D2H");
-  } else if (which == 1) {
-    CFFT_CUDA(cudaMemcpyAsync(p->d_stage_in, in, sbytes, cudaMemcpyHostToDevice, s), "H2D");
-    if ((st = exec_backward(p, p->d_stage_in, p->d_stage_out, B, s, err)) != Status::kOk) return st;
-    CFFT_CUDA(cudaMemcpyAsync(out, p->d_stage_out, fbytes, cudaMemcpyDeviceToHost, s), "D2H");
-  } else {
-    CFFT_CUDA(cudaMemcpyAsync(p->d_stage_in, out, fbytes, cudaMemcpyHostToDevice, s), "H2D");
-    if ((st = exec_scft_step(p, p->d_stage_in, B, s, err)) != Status::kOk) return st;
-    CFFT_CUDA(cudaMemcpyAsync(out, p->d_stage_in, fbytes, cudaMemcpyDeviceToHost, s), "D2H");
+  if (!p->h2d_stream) {
+    for (void** sp : {&p->h2d_stream, &p->d2h_stream}) {
+      cudaStream_t cs_;
+      CFFT_CUDA(cudaStreamCreateWithFlags(&cs_, cudaStreamNonBlocking), "create copy stream");
+      *sp = cs_;
+    }
+    for (int i = 0; i < Plan::kHostPieces; ++i)
+      for (void** ep : {&p->ev_in[i], &p->ev_done[i]}) {
+        cudaEvent_t e;
+        CFFT_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "create copy event");
+        *ep = e;
+      }
   }
-  CFFT_CUDA(cudaStreamSynchronize(s), "synchronize");
+  cudaStream_t s = static_cast<cudaStream_t>(p->own_stream);
+  cudaStream_t sin = static_cast<cudaStream_t>(p->h2d_stream);
+  cudaStream_t sout = static_cast<cudaStream_t>(p->d2h_stream);
+  const size_t in_per = which == 1 ? svol : fvol, out_per = which == 0 ? svol : fvol;
+  // Pieces of at least 2 MiB of input, at most kHostPieces of them.
+  const int by_bytes = static_cast<int>(std::max<size_t>(1, in_per * B / (2u << 20)));
+  const int want = std::max(1, std::min({Plan::kHostPieces, B, by_bytes}));
+  const int pb = (B + want - 1) / want;
+  const int pieces = (B + pb - 1) / pb;
+  const char* hin = static_cast<const char*>(which == 2 ? out : in);
+  char* hout = static_cast<char*>(out);
+  char* din = static_cast<char*>(p->d_stage_in);
+  char* dout = static_cast<char*>(which == 2 ? p->d_stage_in : p->d_stage_out);
+  Status res = Status::kOk;
+  for (int i = 0; i < pieces && res == Status::kOk; ++i) {
+    const int b0 = i * pb, nb = std::min(pb, B - b0);
+    cudaEvent_t ein = static_cast<cudaEvent_t>(p->ev_in[i]), edone = static_cast<cudaEvent_t>(p->ev_done[i]);
+    cudaError_t ce = cudaMemcpyAsync(din + b0 * in_per, hin + b0 * in_per, nb * in_per, cudaMemcpyHostToDevice, sin);
+    if (ce == cudaSuccess) ce = cudaEventRecord(ein, sin);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(s, ein, 0);
+    if (ce != cudaSuccess) {
+      *err = std::string("host pipeline H2D: ") + cudaGetErrorString(ce);
+      res = Status::kCuda;
+      break;
+    }
+    if (which == 0) res = exec_forward(p, din + b0 * in_per, dout + b0 * out_per, nb, s, err);
+    else if (which == 1) res = exec_backward(p, din + b0 * in_per, dout + b0 * out_per, nb, s, err);
+    else res = exec_scft_step(p, din + b0 * in_per, nb, s, err);
+    if (res != Status::kOk) break;
+    ce = cudaEventRecord(edone, s);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(sout, edone, 0);
+    if (ce == cudaSuccess)
+      ce = cudaMemcpyAsync(hout + b0 * out_per, dout + b0 * out_per, nb * out_per, cudaMemcpyDeviceToHost, sout);
+    if (ce != cudaSuccess) {
+      *err = std::string("host pipeline D2H: ") + cudaGetErrorString(ce);
+      res = Status::kCuda;
+    }
+  }
+  // Drain all three streams before returning (also on error: no copy may still touch
+  // the caller's buffers after the call).
+  cudaError_t e1 = cudaStreamSynchronize(sin), e2 = cudaStreamSynchronize(s), e3 = cudaStreamSynchronize(sout);
+  if (res != Status::kOk) return res;
+  for (cudaError_t e : {e1, e2, e3})
+    if (e != cudaSuccess) {
+      *err = std::string("host pipeline synchronize: ") + cudaGetErrorString(e);
+      return Status::kCuda;
+    }
   return Status::kOk;
 }
 

@@ -31,13 +31,21 @@ struct Plan {
   void* d_stage_in = nullptr;   // host-API staging
   void* d_stage_out = nullptr;
   void* d_expand = nullptr;     // fast path: per channel position (orbit index, phase numerator)
-  void* d_g0r = nullptr;        // fast path: chunk x n_orbits complex (G0 at representatives)
+  void* d_g0r = nullptr;        // fast path: G0 at orbit representatives (per lane)
+  void* d_ft = nullptr;         // packed backward path: spectra regrouped in quads of fields (per lane)
   void* d_inv_pk = nullptr;     // fast path: packed alias table for the shared-memory gather
   void* own_stream = nullptr;
   void* lane_stream[2] = {nullptr, nullptr};  // concurrent chunk lanes (fork/join on the caller's stream)
   void* ev_fork = nullptr;
   void* ev_join[2] = {nullptr, nullptr};
-  size_t w_lane_bytes = 0, g0r_lane_bytes = 0;
+  // host-buffer entry points: pieces of the batch flow H2D (h2d_stream) -> compute
+  // (own_stream) -> D2H (d2h_stream), so the copies of neighbouring pieces overlap.
+  static constexpr int kHostPieces = 8;
+  void* h2d_stream = nullptr;
+  void* d2h_stream = nullptr;
+  void* ev_in[kHostPieces] = {};
+  void* ev_done[kHostPieces] = {};
+  size_t w_lane_bytes = 0, g0r_lane_bytes = 0, ft_lane_bytes = 0;
   size_t workspace_bytes = 0;
   // launch geometry
   int threads_xy = 0, threads_z = 0;
@@ -47,7 +55,7 @@ struct Plan {
   int cent_type = 0;            // plane-kernel centring (0 plain, 1 I, 2 F, 3 C, 4 A)
   bool rep_perm = false;        // representative ops are signed permutations
   bool rep_diag8 = false;       // representative ops are the 8 diagonal sign matrices
-  bool reps_smem = false;       // representative gather stages the spectrum in shared memory
+  bool reps_quad = false;       // packed alias rows; fields gathered and expanded in quads
   size_t smem_xy = 0, smem_z = 0;
 };
 

@@ -21,6 +21,7 @@ struct FastArgs {
   const void* expand = nullptr;
   void* W = nullptr;      // channel workspace of this lane
   void* G0R = nullptr;    // representative workspace of this lane
+  void* FT = nullptr;     // quad-grouped spectra of this lane (packed backward path)
   // call operands
   const void* f0 = nullptr;
   void* F = nullptr;
@@ -30,7 +31,7 @@ struct FastArgs {
   // geometry / dispatch
   int stage = 0, nb = 0, H = 0, n_ch = 1, centered = 0, cent_type = 0, d = 1;
   int n_spec = 0, n_orbits = 0;
-  bool use_K = false, rep_diag8 = false, rep_perm = false, reps_smem = false;
+  bool use_K = false, rep_diag8 = false, rep_perm = false, reps_quad = false;
   void* stream = nullptr;
 };
 

@@ -8,6 +8,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -601,84 +602,145 @@ __global__ void k_inv_recon_reps(const DevGeom* __restrict__ g, const typename C
   }
 }
 
-// G0 at orbit representatives for one field, with the field's whole spectrum staged
-// in shared memory (one CTA per field and representative range): every alias gather
-// is a shared-memory read.  Aliases are packed as spec+1 (bits 0-19), conjugation
-// (bit 20) and phase numerator (bits 21-31); with d = 8 a thread reads its
-// representative's 8 entries as two 16-byte loads.  Output layout: G0RP[slot][o][f&1].
-template <typename T, int D>
-__global__ void k_inv_recon_reps_smem(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
-                                      const uint32_t* __restrict__ inv_pk, const typename Cx<T>::type* __restrict__ F,
-                                      typename Cx<T>::type* __restrict__ G0RP, int reps_per_part) {
-  using C = typename Cx<T>::type;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* sF = reinterpret_cast<C*>(smem_raw);
-  const int ns = g->n_spec;
-  const int f = blockIdx.y;
-  const C* Ff = F + static_cast<size_t>(f) * ns;
-  for (int i = threadIdx.x; i < ns; i += blockDim.x) sF[i] = Ff[i];
-  __syncthreads();
-  const C* ph = tables + g->ph_off;
-  const T inv_d = static_cast<T>(1.0 / static_cast<double>(D));
-  const int o0 = blockIdx.x * reps_per_part;
-  const int o1 = min(g->n_orbits, o0 + reps_per_part);
-  C* out = G0RP + static_cast<size_t>(f >> 1) * g->n_orbits * 2 + (f & 1);
-  for (int o = o0 + threadIdx.x; o < o1; o += blockDim.x) {
-    uint32_t e[D];
-    if constexpr (D == 8) {
-      const uint4* p4 = reinterpret_cast<const uint4*>(inv_pk + static_cast<size_t>(o) * 8);
-      const uint4 u0 = p4[0], u1 = p4[1];
-      e[0] = u0.x; e[1] = u0.y; e[2] = u0.z; e[3] = u0.w; e[4] = u1.x; e[5] = u1.y; e[6] = u1.z; e[7] = u1.w;
-    } else {
+template <int D>
+__device__ __forceinline__ void load_alias_row(const uint32_t* __restrict__ inv_pk, int o, uint32_t (&e)[D]) {
+  if constexpr (D == 8) {
+    const uint4* p4 = reinterpret_cast<const uint4*>(inv_pk + static_cast<size_t>(o) * 8);
+    const uint4 u0 = __ldg(p4), u1 = __ldg(p4 + 1);
+    e[0] = u0.x; e[1] = u0.y; e[2] = u0.z; e[3] = u0.w; e[4] = u1.x; e[5] = u1.y; e[6] = u1.z; e[7] = u1.w;
+  } else if constexpr (D == 4) {
+    const uint4 u0 = __ldg(reinterpret_cast<const uint4*>(inv_pk + static_cast<size_t>(o) * 4));
+    e[0] = u0.x; e[1] = u0.y; e[2] = u0.z; e[3] = u0.w;
+  } else {
 #pragma unroll
-      for (int a = 0; a < D; ++a) e[a] = inv_pk[static_cast<size_t>(o) * D + a];
-    }
-    C acc = mk<C>(static_cast<T>(0), static_cast<T>(0));
-#pragma unroll
-    for (int a = 0; a < D; ++a) {
-      const uint32_t sp = e[a] & 0xFFFFFu;
-      if (sp == 0) continue;
-      C v = sF[sp - 1];
-      if (e[a] & (1u << 20)) v = cconj(v);
-      acc = cadd(acc, cmulc(v, ph[e[a] >> 21]));
-    }
-    out[static_cast<size_t>(o) * 2] = cscale(acc, inv_d);
+    for (int a = 0; a < D; ++a) e[a] = __ldg(inv_pk + static_cast<size_t>(o) * D + a);
   }
 }
 
-// Backward expansion from per-field representatives (G0RP[slot][o][a|b]) + inverse z
-// FFT: thread (yy, x) assembles its z line X = (G_a + i G_b) e^{+2 pi i j/P} in
-// registers, transforms it and stores it coalesced across x.  No shared memory.
+// Four complex values (fields 4g .. 4g+3 of one spectral point or orbit) as 16-byte
+// vector loads / stores: 32 bytes for float, 64 for double.
+template <typename C>
+__device__ __forceinline__ void load_quad(const C* __restrict__ p, C (&v)[4]) {
+  if constexpr (sizeof(C) == 8) {
+    const float4 u0 = __ldg(reinterpret_cast<const float4*>(p)), u1 = __ldg(reinterpret_cast<const float4*>(p) + 1);
+    v[0] = mk<C>(u0.x, u0.y); v[1] = mk<C>(u0.z, u0.w); v[2] = mk<C>(u1.x, u1.y); v[3] = mk<C>(u1.z, u1.w);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) v[k] = __ldg(p + k);
+  }
+}
+template <typename C>
+__device__ __forceinline__ void store_quad(C* __restrict__ p, const C (&v)[4]) {
+  if constexpr (sizeof(C) == 8) {
+    reinterpret_cast<float4*>(p)[0] = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
+    reinterpret_cast<float4*>(p)[1] = make_float4(v[2].x, v[2].y, v[3].x, v[3].y);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) p[k] = v[k];
+  }
+}
+
+// Regroup the spectra of nb fields into quads: FT[q][s][k] = F[4q + k][s] (zero past
+// the last field), so one gather of a spectral point serves four fields with one
+// fully used 32-byte sector (float).  Coalesced on both sides.
+template <typename T>
+__global__ void k_group_spectra(const typename Cx<T>::type* __restrict__ F, typename Cx<T>::type* __restrict__ FT,
+                                int ns, int nb) {
+  using C = typename Cx<T>::type;
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  const int q = blockIdx.y;
+  C v[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int f = 4 * q + k;
+    v[k] = f < nb ? F[static_cast<size_t>(f) * ns + s] : mk<C>(static_cast<T>(0), static_cast<T>(0));
+  }
+  store_quad(FT + (static_cast<size_t>(q) * ns + s) * 4, v);
+}
+
+// Backward inverse reconstruction for a quad of fields:
+//   G0(q_o) = (1/d) sum_a ph_a F(spec_a)   (F conjugated where flagged)
+// from the packed alias rows (spec+1 in bits 0-19, conj in bit 20, phase numerator in
+// bits 21-31; 0 = no alias).  Four consecutive lanes take the four fields of one
+// orbit, so every alias gather of a warp reads whole 32-byte quads; the d loads of a
+// lane are independent and in flight together.  The field pairs of each workspace
+// slot are combined as the slot's transform input X = G_a + i G_b and stored as
+// G0P[q][o][pair] (pair 0: fields 4q, 4q+1; pair 1: fields 4q+2, 4q+3).
+template <typename T, int D>
+__global__ void __launch_bounds__(256)
+k_inv_recon_quad(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                 const uint32_t* __restrict__ inv_pk, const typename Cx<T>::type* __restrict__ FT,
+                 typename Cx<T>::type* __restrict__ G0P) {
+  using C = typename Cx<T>::type;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int no = g->n_orbits;
+  const int o = t >> 2, k = t & 3;
+  const bool valid = o < no;  // no early return: lanes exchange values below
+  const int oc = valid ? o : no - 1;
+  const int q = blockIdx.y;
+  const C* ft = FT + static_cast<size_t>(q) * g->n_spec * 4 + k;
+  const C* ph = tables + g->ph_off;
+  uint32_t e[D];
+  load_alias_row<D>(inv_pk, oc, e);
+  C v[D];
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    const uint32_t sp = e[a] & 0xFFFFFu;
+    v[a] = __ldg(ft + static_cast<size_t>(sp ? sp - 1 : 0) * 4);
+  }
+  C acc = mk<C>(static_cast<T>(0), static_cast<T>(0));
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    C w = ph[e[a] >> 21];
+    if ((e[a] & 0xFFFFFu) == 0) w = mk<C>(static_cast<T>(0), static_cast<T>(0));
+    acc = cadd(acc, cmulc(((e[a] >> 20) & 1u) ? cconj(v[a]) : v[a], w));
+  }
+  const T inv_d = static_cast<T>(1.0 / static_cast<double>(D));
+  acc = cscale(acc, inv_d);
+  // lane k (even) takes G_b from lane k + 1; fields past the batch were zero-filled.
+  const T bx = __shfl_down_sync(0xffffffffu, acc.x, 1);
+  const T by = __shfl_down_sync(0xffffffffu, acc.y, 1);
+  if (valid && !(k & 1))
+    G0P[(static_cast<size_t>(q) * no + o) * 2 + (k >> 1)] = mk<C>(acc.x - by, acc.y + bx);
+}
+
+// Backward orbit expansion + inverse z FFT for a quad of fields (two workspace
+// slots): the two halves of the CTA build the z lines of slots 2q and 2q+1 at the same
+// (y, x) positions, X_slot(R^T q) = X_slot(q_o) e^{+2 pi i j / P}, from the packed
+// expansion entries (orbit in bits 0-20, phase numerator in bits 21-31) and the
+// combined representatives G0P[q][o][pair]; both halves read the same entries and
+// 16-byte pairs (the second read hits L1).  The line is transformed in registers and
+// stored coalesced across x.  No shared memory.
 template <typename T, int H>
-__global__ void k_expand2_ifft_z_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
-                                   const int2* __restrict__ ET, const typename Cx<T>::type* __restrict__ G0RF,
+__global__ void k_expand4_ifft_z_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                                   const uint32_t* __restrict__ ETP, const typename Cx<T>::type* __restrict__ G0P,
                                    typename Cx<T>::type* __restrict__ W, int nfields) {
   using C = typename Cx<T>::type;
   constexpr int HV = H * H * H;
-  const int y0 = blockIdx.x * kZB, c = blockIdx.y, slot = blockIdx.z;
+  constexpr int kHalf = ((kZB * H + 31) / 32) * 32;
+  const int y0 = blockIdx.x * kZB, c = blockIdx.y, q = blockIdx.z;
+  const int half = threadIdx.x / kHalf, r = threadIdx.x % kHalf;
+  const int slot = 2 * q + half;
+  if (2 * slot >= nfields) return;
   const int ny = min(kZB, H - y0);
-  const int tid = threadIdx.x;
-  const int yy = tid / H, x = tid % H;
+  const int yy = r / H, x = r % H;
   if (yy >= ny) return;
   const int y = y0 + yy;
-  const int2* et = ET + static_cast<size_t>(c) * HV + y * H + x;
-  const bool has_b = 2 * slot + 1 < nfields;
-  const C* rp = G0RF + static_cast<size_t>(slot) * g->n_orbits * 2;
+  const uint32_t* et = ETP + static_cast<size_t>(c) * HV + y * H + x;
+  const C* rp = G0P + static_cast<size_t>(q) * g->n_orbits * 2 + half;
   const C* ph = tables + g->ph_off;
   C v[H];
 #pragma unroll
   for (int z = 0; z < H; ++z) {
-    const int2 t = et[z * H * H];
-    const C a = rp[2 * t.x];
-    const C b = has_b ? rp[2 * t.x + 1] : mk<C>(static_cast<T>(0), static_cast<T>(0));
-    v[z] = cmulc(mk<C>(a.x - b.y, a.y + b.x), ph[t.y]);
+    const uint32_t t = __ldg(et + z * H * H);
+    v[z] = cmulc(__ldg(rp + 2 * static_cast<size_t>(t & 0x1FFFFFu)), ph[t >> 21]);
   }
   reg_fft<C, true, H>(v);
   C* dst = W + (static_cast<size_t>(slot) * g->n_ch + c) * HV + y * H + x;
 #pragma unroll
   for (int z = 0; z < H; ++z) dst[z * H * H] = v[z];
 }
-
 
 constexpr int kMaxDynSmemFast = 227 * 1024;
 
@@ -762,12 +824,6 @@ Status fast_unit_init(std::string* err) {
       }
     });
   }
-  if constexpr (GROUP == 1) {
-    cudaFuncSetAttribute(k_inv_recon_reps_smem<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
-    cudaFuncSetAttribute(k_inv_recon_reps_smem<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
-    cudaFuncSetAttribute(k_inv_recon_reps_smem<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
-    cudaFuncSetAttribute(k_inv_recon_reps_smem<T, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
-  }
   if ((s = fast_cuda(cudaGetLastError(), "set shared-memory attributes", err)) != Status::kOk) return s;
   if (dev >= 0 && dev < 64) done[dev] = true;
   return Status::kOk;
@@ -848,16 +904,17 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
       }
       case 3: {
         const int no = a.n_orbits;
-        if (a.reps_smem) {
-          const int parts = nb >= 100 ? 1 : std::max(1, std::min((148 + nb - 1) / nb, (no + 1023) / 1024));
-          const int per = (no + parts - 1) / parts;
-          const size_t smem = static_cast<size_t>(a.n_spec) * cs;
+        if (a.reps_quad) {
+          const int nq = (nb + 3) / 4;
+          C* FT = static_cast<C*>(a.FT);
+          k_group_spectra<T><<<dim3((a.n_spec + 255) / 256, nq), 256, 0, st>>>(Fin, FT, a.n_spec, nb);
+          const dim3 gq((4 * no + 255) / 256, nq);
           const uint32_t* pk = static_cast<const uint32_t*>(a.inv_pk);
           switch (a.d) {
-            case 1: k_inv_recon_reps_smem<T, 1><<<dim3(parts, nb), 1024, smem, st>>>(g, tab, pk, Fin, G0R, per); break;
-            case 2: k_inv_recon_reps_smem<T, 2><<<dim3(parts, nb), 1024, smem, st>>>(g, tab, pk, Fin, G0R, per); break;
-            case 4: k_inv_recon_reps_smem<T, 4><<<dim3(parts, nb), 1024, smem, st>>>(g, tab, pk, Fin, G0R, per); break;
-            default: k_inv_recon_reps_smem<T, 8><<<dim3(parts, nb), 1024, smem, st>>>(g, tab, pk, Fin, G0R, per); break;
+            case 1: k_inv_recon_quad<T, 1><<<gq, 256, 0, st>>>(g, tab, pk, FT, G0R); break;
+            case 2: k_inv_recon_quad<T, 2><<<gq, 256, 0, st>>>(g, tab, pk, FT, G0R); break;
+            case 4: k_inv_recon_quad<T, 4><<<gq, 256, 0, st>>>(g, tab, pk, FT, G0R); break;
+            default: k_inv_recon_quad<T, 8><<<gq, 256, 0, st>>>(g, tab, pk, FT, G0R); break;
           }
           break;
         }
@@ -867,9 +924,11 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
       }
       default:
         CFFT_FOR_H(H, {
-          if (a.reps_smem)
-            k_expand2_ifft_z_h<T, HH><<<gz, thr_z, 0, st>>>(g, tab, static_cast<const int2*>(a.expand), G0R, W, nb);
-          else
+          if (a.reps_quad) {
+            constexpr int half = ((kZB * HH + 31) / 32) * 32;
+            k_expand4_ifft_z_h<T, HH><<<dim3((HH + kZB - 1) / kZB, nch, (nb + 3) / 4), 2 * half, 0, st>>>(
+                g, tab, static_cast<const uint32_t*>(a.expand), G0R, W, nb);
+          } else
             k_expand_ifft_z_h<T, HH><<<gz, thr_z, smem_z, st>>>(g, tab, static_cast<const int2*>(a.expand), G0R, W);
         });
         break;
