@@ -39,6 +39,7 @@ class CFFTInfo(ctypes.Structure):
         ("n_spec", c_int), ("n_ops", c_int), ("n_rep", c_int), ("centering", c_int),
         ("centered", c_int), ("n_channels", c_int), ("n_orbits", c_int), ("n_rem_ops", c_int),
         ("precision", c_int), ("max_batch", c_int), ("P", c_int), ("workspace_bytes", ctypes.c_int64),
+        ("exec_path", c_int), ("chunk", c_int), ("lanes", c_int),
     ]
 
 

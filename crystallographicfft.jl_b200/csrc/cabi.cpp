@@ -186,6 +186,9 @@ cfft_status cfft_plan_info(cfft_plan plan, cfft_info* info) {
   info->max_batch = p->max_batch;
   info->P = T.P;
   info->workspace_bytes = static_cast<int64_t>(p->workspace_bytes);
+  info->exec_path = (p->fast_h > 0 ? 1 : 0) | (p->reps_quad ? 2 : 0) | (p->cluster ? 4 : 0);
+  info->chunk = p->chunk;
+  info->lanes = p->lanes;
   return CFFT_OK;
 }
 

@@ -407,6 +407,7 @@ Status launch_stage(Plan* p, int stage, const T* f0, typename Cx<T>::type* F, co
   C* W = reinterpret_cast<C*>(static_cast<char*>(p->d_work_T) + lane * p->w_lane_bytes);
   const PlanTables& T_ = p->T;
   if (p->fast_h > 0) {
+    if (p->cluster && (stage == 1 || stage == 4)) return Status::kOk;  // fused into stages 0 and 5
     FastArgs a;
     a.geom = p->d_geom; a.tables = p->d_tables; a.spec_h = p->d_spec_h; a.K = p->d_K;
     a.inv_spec = p->d_inv_spec; a.inv_phase = p->d_inv_phase; a.inv_pk = p->d_inv_pk; a.expand = p->d_expand;
@@ -418,6 +419,8 @@ Status launch_stage(Plan* p, int stage, const T* f0, typename Cx<T>::type* F, co
     a.cent_type = p->cent_type; a.d = T_.d;
     a.n_spec = static_cast<int>(T_.spec.size()); a.n_orbits = static_cast<int>(T_.orbit_rep.size());
     a.use_K = use_K; a.rep_diag8 = p->rep_diag8; a.rep_perm = p->rep_perm; a.reps_quad = p->reps_quad;
+    a.cluster = p->cluster;
+    a.cluster_ctas = p->cluster_ctas;
     a.stream = st;
     const bool planes = stage == 0 || stage == 5;
     Status s = sizeof(T) == 4 ? (planes ? fast_planes_f32(a, err) : fast_other_f32(a, err))
@@ -681,7 +684,7 @@ Status plan_device_init(Plan* p, std::string* err) {
   size_t ch = std::max<size_t>(1, std::min<size_t>(B, budget / std::max<size_t>(per_field, 1)));
   // Batches of at least 8 fields on the fast path run as two concurrent lanes.
   p->lanes = 1;
-  if (const char* ln = std::getenv("CFFT_LANES")) p->lanes = std::max(1, std::min(2, std::atoi(ln)));
+  if (const char* ln = std::getenv("CFFT_LANES")) p->lanes = std::max(1, std::min(Plan::kMaxLanes, std::atoi(ln)));
   else if (p->fast_h && B >= 8) p->lanes = 2;
   if (p->lanes > 1) ch = std::min(ch, (B + p->lanes - 1) / p->lanes);
   if (p->fast_h && ch < B && ch > 1) ch &= ~static_cast<size_t>(1);
@@ -771,6 +774,28 @@ Status plan_device_init(Plan* p, std::string* err) {
       if ((st = fast_init_planes_f32(err)) != Status::kOk) return st;
       if ((st = fast_init_other_f32(err)) != Status::kOk) return st;
     }
+    // Fused cluster kernels (CFFT_CLUSTER = 8 or 16 CTAs per cluster) when the slot's
+    // channel volume fits the CTAs of one cluster and at least one cluster can be
+    // resident.  Off by default: on B200 at H = 32 the separate plane and z kernels are
+    // faster (1.66 vs 1.90 / 2.07 us per Im-3m 128^3 field), because one slot per SM
+    // group serialises the load, transform and exchange phases.
+    const char* ce = std::getenv("CFFT_CLUSTER");
+    const int want = ce ? std::atoi(ce) : 0;
+    p->cluster_ctas = want == 16 ? 16 : 8;
+    p->cluster = want != 0 && p->reps_quad && fast_cluster_fits(p->fast_h, T.n_ch, p->precision);
+    if (p->cluster) {
+      int mc = 0;
+      st = p->precision == 8 ? fast_cluster_probe_f64(p->fast_h, p->cent_type, p->cluster_ctas, &mc, err)
+                             : fast_cluster_probe_f32(p->fast_h, p->cent_type, p->cluster_ctas, &mc, err);
+      if (st != Status::kOk) return st;
+      if (mc < 1 && p->cluster_ctas == 16) {  // the device does not take 16-CTA clusters here
+        p->cluster_ctas = 8;
+        st = p->precision == 8 ? fast_cluster_probe_f64(p->fast_h, p->cent_type, 8, &mc, err)
+                               : fast_cluster_probe_f32(p->fast_h, p->cent_type, 8, &mc, err);
+        if (st != Status::kOk) return st;
+      }
+      p->cluster = mc >= 1;
+    }
   }
   cudaStream_t s;
   CFFT_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "create stream");
@@ -808,7 +833,7 @@ void plan_device_free(Plan* p) {
   for (void** b : bufs)
     if (*b) { cudaFree(*b); *b = nullptr; }
   if (p->own_stream) { cudaStreamDestroy(static_cast<cudaStream_t>(p->own_stream)); p->own_stream = nullptr; }
-  for (int l = 0; l < 2; ++l) {
+  for (int l = 0; l < Plan::kMaxLanes; ++l) {
     if (p->lane_stream[l]) { cudaStreamDestroy(static_cast<cudaStream_t>(p->lane_stream[l])); p->lane_stream[l] = nullptr; }
     if (p->ev_join[l]) { cudaEventDestroy(static_cast<cudaEvent_t>(p->ev_join[l])); p->ev_join[l] = nullptr; }
   }

@@ -35,9 +35,10 @@ struct Plan {
   void* d_ft = nullptr;         // packed backward path: spectra regrouped in quads of fields (per lane)
   void* d_inv_pk = nullptr;     // fast path: packed alias table for the shared-memory gather
   void* own_stream = nullptr;
-  void* lane_stream[2] = {nullptr, nullptr};  // concurrent chunk lanes (fork/join on the caller's stream)
+  static constexpr int kMaxLanes = 4;
+  void* lane_stream[kMaxLanes] = {};  // concurrent chunk lanes (fork/join on the caller's stream)
   void* ev_fork = nullptr;
-  void* ev_join[2] = {nullptr, nullptr};
+  void* ev_join[kMaxLanes] = {};
   // host-buffer entry points: pieces of the batch flow H2D (h2d_stream) -> compute
   // (own_stream) -> D2H (d2h_stream), so the copies of neighbouring pieces overlap.
   static constexpr int kHostPieces = 8;
@@ -56,6 +57,8 @@ struct Plan {
   bool rep_perm = false;        // representative ops are signed permutations
   bool rep_diag8 = false;       // representative ops are the 8 diagonal sign matrices
   bool reps_quad = false;       // packed alias rows; fields gathered and expanded in quads
+  bool cluster = false;         // fused cluster kernels: fold+xyz FFT and expand+xyz IFFT+unfold
+  int cluster_ctas = 8;         // CTAs per cluster
   size_t smem_xy = 0, smem_z = 0;
 };
 

@@ -32,6 +32,8 @@ struct FastArgs {
   int stage = 0, nb = 0, H = 0, n_ch = 1, centered = 0, cent_type = 0, d = 1;
   int n_spec = 0, n_orbits = 0;
   bool use_K = false, rep_diag8 = false, rep_perm = false, reps_quad = false;
+  bool cluster = false;   // fused cluster kernels for stages 0 (with 1) and 5 (with 4)
+  int cluster_ctas = 8;   // CTAs per cluster (8, or 16 where the device allows it)
   void* stream = nullptr;
 };
 
@@ -40,6 +42,10 @@ Status fast_planes_f32(const FastArgs& a, std::string* err);
 Status fast_planes_f64(const FastArgs& a, std::string* err);
 Status fast_other_f32(const FastArgs& a, std::string* err);
 Status fast_other_f64(const FastArgs& a, std::string* err);
+// Largest number of concurrently resident kc-CTA clusters of the fused forward and
+// backward kernels for channel edge H and centring type ct (0 if they cannot run).
+Status fast_cluster_probe_f32(int H, int ct, int kc, int* max_clusters, std::string* err);
+Status fast_cluster_probe_f64(int H, int ct, int kc, int* max_clusters, std::string* err);
 // Per-device set-up of each unit: constant-memory twiddles and shared-memory limits.
 Status fast_init_planes_f32(std::string* err);
 Status fast_init_planes_f64(std::string* err);
@@ -51,5 +57,14 @@ inline bool fast_size_ok(int H, int real_bytes) {
   return H == 4 || H == 6 || H == 8 || H == 12 || H == 16 || H == 24 || H == 32 || (H == 48 && real_bytes == 4);
 }
 constexpr int kFastZB = 4;  // xz-planes (y values) per CTA in the z kernels
+
+// The fused cluster kernels hold one slot's channel volume in the shared memory of 8
+// CTAs (H / 8 z-planes of nch padded H x (H + 1) planes each, one z line per thread).
+inline bool fast_cluster_fits(int H, int nch, int real_bytes) {
+  if (H % 8 != 0 || H < 16 || H > 32) return false;
+  const long threads = static_cast<long>(nch) * (H / 8) * H;
+  const long smem = static_cast<long>(H / 8) * nch * H * (H + 1) * 2 * real_bytes;
+  return threads >= 32 && threads <= 1024 && smem <= 227 * 1024;
+}
 
 }  // namespace cfft

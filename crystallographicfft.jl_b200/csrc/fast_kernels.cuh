@@ -13,6 +13,8 @@
 #include <string>
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "device_common.cuh"
 #include "fast_api.h"
 
@@ -112,12 +114,11 @@ template <int CT> struct Cent {
 // builds X = G_a + i G_b and the unfold reads field a from the real part and field b
 // from the imaginary part.  This halves the FFT work and the workspace traffic.
 
-// Row / column FFTs of nch padded H x H planes (row stride S = H + 1, plane stride
-// H * S), one thread per line, compile-time strides.
+// Row / column FFTs of nch padded planes for a group of threads (gtid of gnth).
 template <typename C, bool INV, int H>
-__device__ __forceinline__ void smem_rows(C* buf, int nlines) {
+__device__ __forceinline__ void group_rows(C* buf, int nlines, int tid, int nth) {
   constexpr int S = H + 1;
-  for (int l = threadIdx.x; l < nlines; l += blockDim.x) {
+  for (int l = tid; l < nlines; l += nth) {
     C* p = buf + l * S;
     C v[H];
 #pragma unroll
@@ -128,9 +129,9 @@ __device__ __forceinline__ void smem_rows(C* buf, int nlines) {
   }
 }
 template <typename C, bool INV, int H>
-__device__ __forceinline__ void smem_cols(C* buf, int nlines) {
+__device__ __forceinline__ void group_cols(C* buf, int nlines, int tid, int nth) {
   constexpr int S = H + 1;
-  for (int l = threadIdx.x; l < nlines; l += blockDim.x) {
+  for (int l = tid; l < nlines; l += nth) {
     C* p = buf + (l / H) * (H * S) + (l % H);
     C v[H];
 #pragma unroll
@@ -141,28 +142,19 @@ __device__ __forceinline__ void smem_cols(C* buf, int nlines) {
   }
 }
 
-// Forward plane kernel, cubic H: fold (or plain load) of two fields + x FFT + y FFT
-// -> W[slot][c][z][y][x].
+// Fold (or plain load, CT = 0) of the two fields of one slot at channel z-plane iz into
+// the nch padded planes at buf (channel c at buf + c * H * (H + 1)), with the fold
+// twiddles e^{-2 pi i off.n / M} and the interaction factors E when given.  Work is
+// spread over threads tid of nth.
 template <typename T, int H, int CT>
-__global__ void k_plane_fwd_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
-                              const T* __restrict__ f0, const T* __restrict__ E, typename Cx<T>::type* __restrict__ W,
-                              int nfields) {
+__device__ __forceinline__ void fold_plane(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                                           const T* __restrict__ srca, const T* __restrict__ srcb,
+                                           const T* __restrict__ Ea, const T* __restrict__ Eb, bool has_b, bool USE_E,
+                                           int iz, typename Cx<T>::type* buf, int tid, int nth) {
   using C = typename Cx<T>::type;
   constexpr int S = H + 1;
-  constexpr int PL = H * S;  // padded plane
-  const bool USE_E = E != nullptr;  // warp-uniform
+  constexpr int PL = H * S;
   constexpr int nch = Cent<CT>::n;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* buf = reinterpret_cast<C*>(smem_raw);
-  const int iz = blockIdx.x, slot = blockIdx.y;
-  const int fa = 2 * slot;
-  const bool has_b = fa + 1 < nfields;
-  const int tid = threadIdx.x, nth = blockDim.x;
-  const size_t mvol = static_cast<size_t>(g->M[0]) * g->M[1] * g->M[2];
-  const T* srca = f0 + static_cast<size_t>(fa) * mvol;
-  const T* srcb = srca + mvol;
-  const T* Ea = USE_E ? E + static_cast<size_t>(fa) * mvol : nullptr;
-  const T* Eb = USE_E ? Ea + mvol : nullptr;
   const T zero = static_cast<T>(0);
   if constexpr (CT == 0) {
     const size_t zoff = static_cast<size_t>(iz) * H * H;
@@ -252,49 +244,22 @@ __global__ void k_plane_fwd_h(const DevGeom* __restrict__ g, const typename Cx<T
       }
     }
   }
-  __syncthreads();
-  smem_rows<C, false, H>(buf, nch * H);   // x lines
-  __syncthreads();
-  smem_cols<C, false, H>(buf, nch * H);   // y lines
-  __syncthreads();
-  constexpr int HV = H * H * H;
-  C* dst0 = W + static_cast<size_t>(slot) * nch * HV + iz * H * H;
-  for (int c = 0; c < nch; ++c)
-    for (int e = tid; e < H * H; e += nth) dst0[c * HV + e] = buf[c * PL + (e / H) * S + (e % H)];
 }
 
-// Backward plane kernel, cubic H: inverse x/y FFT of W[slot][c][iz] + unfold of the two
-// fields (real part -> field a, imaginary part -> field b).
+// Unfold of the nch inverse-transformed planes at buf (channel z-plane iz) into the two
+// fields of the slot: conjugate fold twiddle, inverse WHT8 / 8, real part -> field a,
+// imaginary part -> field b, times E when given.
 template <typename T, int H, int CT>
-__global__ void k_plane_bwd_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
-                              const typename Cx<T>::type* __restrict__ W, const T* __restrict__ E, T* __restrict__ f0,
-                              int nfields) {
+__device__ __forceinline__ void unfold_plane(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                                             const typename Cx<T>::type* buf, T* __restrict__ dsta, T* __restrict__ dstb,
+                                             const T* __restrict__ Ea, const T* __restrict__ Eb, bool has_b, bool USE_E,
+                                             int iz, int tid, int nth) {
   using C = typename Cx<T>::type;
   constexpr int S = H + 1;
   constexpr int PL = H * S;
-  const bool USE_E = E != nullptr;  // warp-uniform
   constexpr int nch = Cent<CT>::n;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* buf = reinterpret_cast<C*>(smem_raw);
-  const int iz = blockIdx.x, slot = blockIdx.y;
-  const int fa = 2 * slot;
-  const bool has_b = fa + 1 < nfields;
-  const int tid = threadIdx.x, nth = blockDim.x;
   const size_t hvol = static_cast<size_t>(H) * H * H;
-  constexpr int HV = H * H * H;
-  const C* src0 = W + static_cast<size_t>(slot) * nch * HV + iz * H * H;
-  for (int c = 0; c < nch; ++c)
-    for (int e = tid; e < H * H; e += nth) buf[c * PL + (e / H) * S + (e % H)] = src0[c * HV + e];
-  __syncthreads();
-  smem_rows<C, true, H>(buf, nch * H);
-  __syncthreads();
-  smem_cols<C, true, H>(buf, nch * H);
-  __syncthreads();
   const size_t mvol = static_cast<size_t>(g->M[0]) * g->M[1] * g->M[2];
-  T* dsta = f0 + static_cast<size_t>(fa) * mvol;
-  T* dstb = dsta + mvol;
-  const T* Ea = USE_E ? E + static_cast<size_t>(fa) * mvol : nullptr;
-  const T* Eb = USE_E ? Ea + mvol : nullptr;
   if constexpr (CT == 0) {
     const T scale = static_cast<T>(1.0 / static_cast<double>(mvol));
     const size_t zoff = static_cast<size_t>(iz) * H * H;
@@ -341,6 +306,206 @@ __global__ void k_plane_bwd_h(const DevGeom* __restrict__ g, const typename Cx<T
       }
     }
   }
+}
+
+// Forward plane kernel, cubic H: fold (or plain load) of two fields + x FFT + y FFT
+// -> W[slot][c][z][y][x].
+template <typename T, int H, int CT>
+__global__ void k_plane_fwd_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                              const T* __restrict__ f0, const T* __restrict__ E, typename Cx<T>::type* __restrict__ W,
+                              int nfields) {
+  using C = typename Cx<T>::type;
+  constexpr int S = H + 1;
+  constexpr int PL = H * S;  // padded plane
+  constexpr int nch = Cent<CT>::n;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int iz = blockIdx.x, slot = blockIdx.y;
+  const int fa = 2 * slot;
+  const bool has_b = fa + 1 < nfields;
+  const bool USE_E = E != nullptr;  // warp-uniform
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const size_t mvol = static_cast<size_t>(g->M[0]) * g->M[1] * g->M[2];
+  const T* srca = f0 + static_cast<size_t>(fa) * mvol;
+  const T* Ea = USE_E ? E + static_cast<size_t>(fa) * mvol : nullptr;
+  fold_plane<T, H, CT>(g, tables, srca, srca + mvol, Ea, USE_E ? Ea + mvol : nullptr, has_b, USE_E, iz, buf, tid, nth);
+  __syncthreads();
+  group_rows<C, false, H>(buf, nch * H, tid, nth);   // x lines
+  __syncthreads();
+  group_cols<C, false, H>(buf, nch * H, tid, nth);   // y lines
+  __syncthreads();
+  constexpr int HV = H * H * H;
+  C* dst0 = W + static_cast<size_t>(slot) * nch * HV + iz * H * H;
+  for (int c = 0; c < nch; ++c)
+    for (int e = tid; e < H * H; e += nth) dst0[c * HV + e] = buf[c * PL + (e / H) * S + (e % H)];
+}
+
+// Backward plane kernel, cubic H: inverse x/y FFT of W[slot][c][iz] + unfold of the two
+// fields (real part -> field a, imaginary part -> field b).
+template <typename T, int H, int CT>
+__global__ void k_plane_bwd_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                              const typename Cx<T>::type* __restrict__ W, const T* __restrict__ E, T* __restrict__ f0,
+                              int nfields) {
+  using C = typename Cx<T>::type;
+  constexpr int S = H + 1;
+  constexpr int PL = H * S;
+  constexpr int nch = Cent<CT>::n;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int iz = blockIdx.x, slot = blockIdx.y;
+  const int fa = 2 * slot;
+  const bool has_b = fa + 1 < nfields;
+  const bool USE_E = E != nullptr;  // warp-uniform
+  const int tid = threadIdx.x, nth = blockDim.x;
+  constexpr int HV = H * H * H;
+  const C* src0 = W + static_cast<size_t>(slot) * nch * HV + iz * H * H;
+  for (int c = 0; c < nch; ++c)
+    for (int e = tid; e < H * H; e += nth) buf[c * PL + (e / H) * S + (e % H)] = src0[c * HV + e];
+  __syncthreads();
+  group_rows<C, true, H>(buf, nch * H, tid, nth);
+  __syncthreads();
+  group_cols<C, true, H>(buf, nch * H, tid, nth);
+  __syncthreads();
+  const size_t mvol = static_cast<size_t>(g->M[0]) * g->M[1] * g->M[2];
+  T* dsta = f0 + static_cast<size_t>(fa) * mvol;
+  const T* Ea = USE_E ? E + static_cast<size_t>(fa) * mvol : nullptr;
+  unfold_plane<T, H, CT>(g, tables, buf, dsta, dsta + mvol, Ea, USE_E ? Ea + mvol : nullptr, has_b, USE_E, iz, tid, nth);
+}
+
+// ---------------------------------------------------------------- cluster kernels
+// One thread-block cluster of KC CTAs holds the whole channel volume of one workspace
+// slot (two fields) in distributed shared memory: CTA r owns the channel z-planes
+// [ZPC r, ZPC r + ZPC), ZPC = H / KC, as padded nch x H x (H+1)
+// planes.  The z transforms then read (forward) or write (backward) the peers' planes
+// directly, so the channel workspace never makes the plane <-> z round trip through L2.
+template <int H, int CT, int KC> struct ClusterShape {
+  static constexpr int nch = Cent<CT>::n;
+  static constexpr int zpc = H / KC;                    // channel z-planes per CTA
+  static constexpr int threads = nch * zpc * H;         // one z line (c, y, x) per thread
+  static constexpr int group = nch * H;                 // threads per plane in the x/y phase
+};
+// KC = 8 (portable) for H = 16, 24, 32; KC = 16 (non-portable, two CTAs per SM) for H = 32.
+template <typename T, int H, int CT, int KC>
+constexpr bool cluster_fits() {
+  return H % KC == 0 && H >= 16 && H <= 32 && (KC == 8 || (KC == 16 && H == 32)) &&
+         ClusterShape<H, CT, KC>::threads >= 32 && ClusterShape<H, CT, KC>::threads <= 1024 &&
+         static_cast<long>(ClusterShape<H, CT, KC>::zpc) * Cent<CT>::n * H * (H + 1) * 2 * sizeof(T) <= 227 * 1024;
+}
+template <typename T, int H, int CT, int KC>
+constexpr size_t cluster_smem() {
+  return static_cast<size_t>(ClusterShape<H, CT, KC>::zpc) * Cent<CT>::n * H * (H + 1) * 2 * sizeof(T);
+}
+
+// Forward: fold + x/y FFT of the CTA's ZPC planes, cluster barrier, z FFT of the lines
+// (c, y in the CTA's rows, x) gathered from the peers' planes, cluster barrier (every
+// peer has finished reading), then the lines are transposed through the CTA's own
+// shared memory and stored z-fastest: WT[slot][c][x][y][z].
+template <typename T, int H, int CT, int KC>
+__global__ void __launch_bounds__(ClusterShape<H, CT, KC>::threads)
+k_fwd_cluster_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                const T* __restrict__ f0, const T* __restrict__ E, typename Cx<T>::type* __restrict__ WT, int nfields) {
+  using C = typename Cx<T>::type;
+  using CS = ClusterShape<H, CT, KC>;
+  constexpr int S = H + 1, PL = H * S, NCH = CS::nch, ZPC = CS::zpc, HV = H * H * H;
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int r = static_cast<int>(cluster.block_rank());
+  const int slot = blockIdx.y;
+  const int fa = 2 * slot;
+  const bool has_b = fa + 1 < nfields;
+  const bool USE_E = E != nullptr;
+  const int tid = threadIdx.x;
+  const size_t mvol = static_cast<size_t>(g->M[0]) * g->M[1] * g->M[2];
+  {
+    const int grp = tid / CS::group, gtid = tid % CS::group;
+    C* pbuf = buf + grp * NCH * PL;
+    const T* srca = f0 + static_cast<size_t>(fa) * mvol;
+    const T* Ea = USE_E ? E + static_cast<size_t>(fa) * mvol : nullptr;
+    fold_plane<T, H, CT>(g, tables, srca, srca + mvol, Ea, USE_E ? Ea + mvol : nullptr, has_b, USE_E, ZPC * r + grp,
+                         pbuf, gtid, CS::group);
+    __syncthreads();
+    group_rows<C, false, H>(pbuf, NCH * H, gtid, CS::group);
+    __syncthreads();
+    group_cols<C, false, H>(pbuf, NCH * H, gtid, CS::group);
+  }
+  cluster.sync();
+  const int c = tid / (ZPC * H), yy = (tid / H) % ZPC, x = tid % H;
+  const int y = ZPC * r + yy;
+  C v[H];
+#pragma unroll
+  for (int z = 0; z < H; ++z) {
+    const C* rb = cluster.map_shared_rank(buf, z / ZPC);
+    v[z] = rb[((z % ZPC) * NCH + c) * PL + y * S + x];
+  }
+  reg_fft<C, false, H>(v);
+  cluster.sync();
+  constexpr int RUN = ZPC * H, PCX = RUN + 1;  // staging [c][x][yy][z], padded per (c, x)
+#pragma unroll
+  for (int z = 0; z < H; ++z) buf[(c * H + x) * PCX + yy * H + z] = v[z];
+  __syncthreads();
+  C* dst = WT + static_cast<size_t>(slot) * NCH * HV;
+  for (int e = tid; e < NCH * H * RUN; e += CS::threads) {
+    const int cx = e / RUN, rr = e % RUN;
+    dst[static_cast<size_t>(cx / H) * HV + ((cx % H) * H + ZPC * r) * H + rr] = buf[cx * PCX + rr];
+  }
+}
+
+// Backward: cluster barrier (every peer is running), orbit expansion + inverse z FFT of
+// the CTA's lines (c, y, x) from the combined representatives G0P[slot / 2][o][slot & 1]
+// and the packed expansion entries (orbit | phase << 21), written into the owning
+// peers' planes; cluster barrier; inverse x/y FFT + unfold of the CTA's own planes.
+template <typename T, int H, int CT, int KC>
+__global__ void __launch_bounds__(ClusterShape<H, CT, KC>::threads)
+k_bwd_cluster_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                const uint32_t* __restrict__ ETP, const typename Cx<T>::type* __restrict__ G0P,
+                const T* __restrict__ E, T* __restrict__ f0, int nfields) {
+  using C = typename Cx<T>::type;
+  using CS = ClusterShape<H, CT, KC>;
+  constexpr int S = H + 1, PL = H * S, NCH = CS::nch, ZPC = CS::zpc, HV = H * H * H;
+  namespace cg = cooperative_groups;
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);
+  const int r = static_cast<int>(cluster.block_rank());
+  const int slot = blockIdx.y;
+  const int tid = threadIdx.x;
+  cluster.sync();
+  {
+    const int c = tid / (ZPC * H), yy = (tid / H) % ZPC, x = tid % H;
+    const int y = ZPC * r + yy;
+    const uint32_t* et = ETP + static_cast<size_t>(c) * HV + y * H + x;
+    const C* rp = G0P + static_cast<size_t>(slot >> 1) * g->n_orbits * 2 + (slot & 1);
+    const C* ph = tables + g->ph_off;
+    C v[H];
+#pragma unroll
+    for (int z = 0; z < H; ++z) {
+      const uint32_t t = __ldg(et + z * H * H);
+      v[z] = cmulc(__ldg(rp + 2 * static_cast<size_t>(t & 0x1FFFFFu)), ph[t >> 21]);
+    }
+    reg_fft<C, true, H>(v);
+#pragma unroll
+    for (int z = 0; z < H; ++z) {
+      C* rb = cluster.map_shared_rank(buf, z / ZPC);
+      rb[((z % ZPC) * NCH + c) * PL + y * S + x] = v[z];
+    }
+  }
+  cluster.sync();
+  const int grp = tid / CS::group, gtid = tid % CS::group;
+  C* pbuf = buf + grp * NCH * PL;
+  group_rows<C, true, H>(pbuf, NCH * H, gtid, CS::group);
+  __syncthreads();
+  group_cols<C, true, H>(pbuf, NCH * H, gtid, CS::group);
+  __syncthreads();
+  const int fa = 2 * slot;
+  const bool has_b = fa + 1 < nfields;
+  const bool USE_E = E != nullptr;
+  const size_t mvol = static_cast<size_t>(g->M[0]) * g->M[1] * g->M[2];
+  T* dsta = f0 + static_cast<size_t>(fa) * mvol;
+  const T* Ea = USE_E ? E + static_cast<size_t>(fa) * mvol : nullptr;
+  unfold_plane<T, H, CT>(g, tables, pbuf, dsta, dsta + mvol, Ea, USE_E ? Ea + mvol : nullptr, has_b, USE_E,
+                         ZPC * r + grp, gtid, CS::group);
 }
 
 constexpr int kZB = kFastZB;
@@ -785,6 +950,66 @@ inline Status fast_cuda(cudaError_t e, const char* what, std::string* err) {
   return Status::kCuda;
 }
 
+// Cluster kernels: attributes, launch (cluster size at run time, through
+// cudaLaunchKernelEx) and occupancy, for the instantiations that fit.
+template <typename T, int H, int CT, int KC>
+void cluster_attrs() {
+  if constexpr (cluster_fits<T, H, CT, KC>()) {
+    const int smem = static_cast<int>(cluster_smem<T, H, CT, KC>());
+    cudaFuncSetAttribute(k_fwd_cluster_h<T, H, CT, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_bwd_cluster_h<T, H, CT, KC>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (KC > 8) {
+      cudaFuncSetAttribute(k_fwd_cluster_h<T, H, CT, KC>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      cudaFuncSetAttribute(k_bwd_cluster_h<T, H, CT, KC>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    }
+  }
+}
+
+template <typename T, int H, int CT, int KC>
+cudaLaunchConfig_t cluster_config(int nslots, cudaStream_t st, cudaLaunchAttribute* attr) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(KC, static_cast<unsigned>(nslots), 1);
+  cfg.blockDim = dim3(ClusterShape<H, CT, KC>::threads, 1, 1);
+  cfg.dynamicSmemBytes = cluster_smem<T, H, CT, KC>();
+  cfg.stream = st;
+  attr->id = cudaLaunchAttributeClusterDimension;
+  attr->val.clusterDim.x = KC;
+  attr->val.clusterDim.y = 1;
+  attr->val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+template <typename T, int H, int CT, int KC>
+bool cluster_launch(int stage, int nslots, cudaStream_t st, const DevGeom* g, const typename Cx<T>::type* tab,
+                    const T* f0, const T* E, typename Cx<T>::type* W, const uint32_t* ETP,
+                    const typename Cx<T>::type* G0P, T* f0_out, int nb, cudaError_t* ce) {
+  if constexpr (cluster_fits<T, H, CT, KC>()) {
+    cudaLaunchAttribute attr;
+    const cudaLaunchConfig_t cfg = cluster_config<T, H, CT, KC>(nslots, st, &attr);
+    if (stage == 0) *ce = cudaLaunchKernelEx(&cfg, k_fwd_cluster_h<T, H, CT, KC>, g, tab, f0, E, W, nb);
+    else *ce = cudaLaunchKernelEx(&cfg, k_bwd_cluster_h<T, H, CT, KC>, g, tab, ETP, G0P, E, f0_out, nb);
+    return true;
+  }
+  return false;
+}
+
+template <typename T, int H, int CT, int KC>
+cudaError_t cluster_occupancy(int* max_clusters) {
+  if constexpr (cluster_fits<T, H, CT, KC>()) {
+    cudaLaunchAttribute attr;
+    const cudaLaunchConfig_t cfg = cluster_config<T, H, CT, KC>(1, nullptr, &attr);
+    int nf = 0, nbk = 0;
+    cudaError_t e = cudaOccupancyMaxActiveClusters(&nf, k_fwd_cluster_h<T, H, CT, KC>, &cfg);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveClusters(&nbk, k_bwd_cluster_h<T, H, CT, KC>, &cfg);
+    if (e == cudaSuccess) *max_clusters = std::min(nf, nbk);
+    return e;
+  }
+  *max_clusters = 0;
+  return cudaSuccess;
+}
+
 // Per-device set-up of this unit: its own copy of the constant-memory twiddles
 // e^{-2 pi i j / N} (FP64 values rounded) and the shared-memory limits of its kernels.
 template <typename T, int GROUP>
@@ -816,6 +1041,8 @@ Status fast_unit_init(std::string* err) {
           CFFT_FOR_CT(ct, {
             cudaFuncSetAttribute(k_plane_fwd_h<T, HH, CTT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
             cudaFuncSetAttribute(k_plane_bwd_h<T, HH, CTT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
+            cluster_attrs<T, HH, CTT, 8>();
+            cluster_attrs<T, HH, CTT, 16>();
           });
         }
       } else {
@@ -826,6 +1053,27 @@ Status fast_unit_init(std::string* err) {
   }
   if ((s = fast_cuda(cudaGetLastError(), "set shared-memory attributes", err)) != Status::kOk) return s;
   if (dev >= 0 && dev < 64) done[dev] = true;
+  return Status::kOk;
+}
+
+// Occupancy of the fused cluster kernels with KC CTAs per cluster: resident clusters
+// (the smaller of the forward and backward kernels), 0 when they do not fit.
+template <typename T>
+Status fast_unit_cluster_probe(int H, int ct, int kc, int* max_clusters, std::string* err) {
+  *max_clusters = 0;
+  Status s = fast_unit_init<T, 0>(err);
+  if (s != Status::kOk) return s;
+  cudaError_t e = cudaSuccess;
+  CFFT_FOR_H(H, {
+    CFFT_FOR_CT(ct, {
+      if (kc == 16) e = cluster_occupancy<T, HH, CTT, 16>(max_clusters);
+      else e = cluster_occupancy<T, HH, CTT, 8>(max_clusters);
+    });
+  });
+  if (e != cudaSuccess) {  // e.g. a cluster size this device does not allow: not used
+    cudaGetLastError();
+    *max_clusters = 0;
+  }
   return Status::kOk;
 }
 
@@ -847,6 +1095,27 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
   const int nslots = (nb + 1) / 2;
   const size_t cs = sizeof(C);
   if constexpr (GROUP == 0) {
+    if (a.cluster) {
+      bool launched = false;
+      cudaError_t ce = cudaSuccess;
+      CFFT_FOR_H(H, {
+        CFFT_FOR_CT(a.cent_type, {
+          if (a.cluster_ctas == 16) {
+            launched = cluster_launch<T, HH, CTT, 16>(a.stage, nslots, st, g, tab, f0, E, W,
+                                                      static_cast<const uint32_t*>(a.expand), G0R, f0_out, nb, &ce);
+          } else {
+            launched = cluster_launch<T, HH, CTT, 8>(a.stage, nslots, st, g, tab, f0, E, W,
+                                                     static_cast<const uint32_t*>(a.expand), G0R, f0_out, nb, &ce);
+          }
+        });
+      });
+      if (!launched) {
+        *err = "no fused cluster kernel for this channel grid";
+        return Status::kUnsupported;
+      }
+      if (ce != cudaSuccess) return fast_cuda(ce, "fused cluster launch", err);
+      return fast_cuda(cudaGetLastError(), "fused cluster launch", err);
+    }
     const int thr_plane = std::max(128, ((nch * H + 31) / 32) * 32);
     const size_t smem_plane = static_cast<size_t>(nch) * H * (H + 1) * cs;
     if (a.stage == 0) {

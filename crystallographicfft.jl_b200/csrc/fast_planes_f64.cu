@@ -5,5 +5,8 @@ namespace cfft {
 
 Status fast_planes_f64(const FastArgs& a, std::string* err) { return fast_unit_launch<double, 0>(a, err); }
 Status fast_init_planes_f64(std::string* err) { return fast_unit_init<double, 0>(err); }
+Status fast_cluster_probe_f64(int H, int ct, int kc, int* max_clusters, std::string* err) {
+  return fast_unit_cluster_probe<double>(H, ct, kc, max_clusters, err);
+}
 
 }  // namespace cfft

@@ -82,6 +82,10 @@ typedef struct cfft_info {
   int max_batch;
   int P;                 /* lcm(N): phase denominator */
   int64_t workspace_bytes;
+  int exec_path;         /* bit 0: compile-time sized kernels; bit 1: packed quad backward gather;
+                            bit 2: fused 8-CTA cluster kernels (0 for host-only plans) */
+  int chunk;             /* fields per workspace chunk */
+  int lanes;             /* concurrent chunk lanes */
 } cfft_info;
 
 /* ---------------- plan-time functions (host only, no GPU needed) ---------------- */
