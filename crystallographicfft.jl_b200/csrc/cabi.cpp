@@ -139,14 +139,26 @@ static cfft_status plan_create_impl(const cfft_desc* desc, cfft_plan* plan, bool
     return ret(Status::kInvalid, err);
   if (desc->precision != 4 && desc->precision != 8) return ret(Status::kInvalid, "precision must be 4 or 8");
   if (desc->max_batch < 1) return ret(Status::kInvalid, "max_batch must be positive");
-  if (desc->path < 0 || desc->path > 2) return ret(Status::kInvalid, "unknown path");
+  if (desc->path < 0 || desc->path > 4) return ret(Status::kInvalid, "unknown path");
   auto* p = new (std::nothrow) cfft::Plan();
   if (!p) return ret(Status::kAlloc, "host allocation failed");
   p->precision = desc->precision;
   p->max_batch = desc->max_batch;
   p->ds = desc->ds;
   std::memcpy(p->lattice, desc->lattice, sizeof(p->lattice));
-  Status s = cfft::build_tables(ops, n, desc->dim, desc->path != CFFT_PATH_M2, &p->T, &err);
+  const bool plain = desc->path == CFFT_PATH_M2 || desc->path == CFFT_PATH_M2Q;
+  Status s = cfft::build_tables(ops, n, desc->dim, !plain, &p->T, &err);
+  if (s == Status::kOk && (desc->path == CFFT_PATH_M2Q || desc->path == CFFT_PATH_M7)) {
+    // plan_m7_scft (src/q_fused_krfft.jl:822-850) refuses P lattices and odd subgrids;
+    // the centred plan exists exactly when neither holds.
+    if (desc->path == CFFT_PATH_M7 && !p->T.centered) {
+      s = Status::kInvalid;
+      err = "M7 SCFT requires a centred lattice (I/F/C/A) with L = 2 and even M; use M2Q";
+    } else {
+      p->qmode = desc->path;
+      s = cfft::build_q_tables(p->T, p->lattice, p->ds, &p->q_host, &p->q_gather, &err);
+    }
+  }
   if (s == Status::kOk && device) s = cfft::plan_device_init(p, &err);
   if (s == Status::kOk && !device) cfft::compute_kernel(p->T, p->lattice, p->ds, &p->T.K);
   if (s != Status::kOk) {
@@ -189,6 +201,15 @@ cfft_status cfft_plan_info(cfft_plan plan, cfft_info* info) {
   info->exec_path = (p->fast_h > 0 ? 1 : 0) | (p->reps_quad ? 2 : 0) | (p->cluster ? 4 : 0);
   info->chunk = p->chunk;
   info->lanes = p->lanes;
+  return CFFT_OK;
+}
+
+cfft_status cfft_plan_q_tables(cfft_plan plan, double* Q, int32_t* gather) {
+  if (!plan) return ret(Status::kInvalid, "null plan");
+  const auto* p = reinterpret_cast<cfft::Plan*>(plan);
+  if (!p->qmode) return ret(Status::kUnsupported, "not an M2Q / M7 plan");
+  if (Q) std::memcpy(Q, p->q_host.data(), p->q_host.size() * sizeof(double));
+  if (gather) std::memcpy(gather, p->q_gather.data(), p->q_gather.size() * sizeof(int32_t));
   return CFFT_OK;
 }
 
@@ -236,6 +257,10 @@ cfft_status cfft_update_kernel(cfft_plan plan, double ds, const double* lattice)
   p->ds = ds;
   if (lattice) std::memcpy(p->lattice, lattice, sizeof(p->lattice));
   std::string err;
+  if (p->qmode) {  // update_m2_kernel! rebuilds the Q matrices (src/q_fused_krfft.jl:1036-1052)
+    Status s = cfft::build_q_tables(p->T, p->lattice, p->ds, &p->q_host, &p->q_gather, &err);
+    if (s != Status::kOk) return ret(s, err);
+  }
   if (!p->d_geom) {
     cfft::compute_kernel(p->T, p->lattice, p->ds, &p->T.K);
     return CFFT_OK;

@@ -400,7 +400,8 @@ std::vector<unsigned char> make_table_bytes(const Plan& p, DevGeom* g) {
 // `nb` fields starting at the caller's pointers; the workspace holds one chunk.
 template <typename T>
 Status launch_stage(Plan* p, int stage, const T* f0, typename Cx<T>::type* F, const typename Cx<T>::type* Fin,
-                    T* f0_out, const T* E, bool use_K, int nb, cudaStream_t st, std::string* err, int lane = 0) {
+                    T* f0_out, const T* E, bool use_K, int nb, cudaStream_t st, std::string* err, int lane = 0,
+                    bool q_step = false) {
   using C = typename Cx<T>::type;
   const DevGeom* g = static_cast<const DevGeom*>(p->d_geom);
   const C* tab = static_cast<const C*>(p->d_tables);
@@ -421,11 +422,19 @@ Status launch_stage(Plan* p, int stage, const T* f0, typename Cx<T>::type* F, co
     a.use_K = use_K; a.rep_diag8 = p->rep_diag8; a.rep_perm = p->rep_perm; a.reps_quad = p->reps_quad;
     a.cluster = p->cluster;
     a.cluster_ctas = p->cluster_ctas;
+    if (q_step) {  // stage 4: Q-multiply + inverse z FFT into the Q workspace; stage 5 reads it
+      a.q_step = true;
+      a.QT = p->d_qt;
+      a.GT = p->d_gt;
+      C* WQ = reinterpret_cast<C*>(static_cast<char*>(p->d_work_Q) + lane * p->w_lane_bytes);
+      if (stage == 4) a.W2 = WQ;
+      else if (stage == 5) a.W = WQ;
+    }
     a.stream = st;
     const bool planes = stage == 0 || stage == 5;
     Status s = sizeof(T) == 4 ? (planes ? fast_planes_f32(a, err) : fast_other_f32(a, err))
                               : (planes ? fast_planes_f64(a, err) : fast_other_f64(a, err));
-    g_launches += (stage == 3 && p->reps_quad) ? 2 : 1;  // regroup + gather
+    g_launches += (stage == 3 && p->reps_quad && !q_step) ? 2 : 1;  // regroup + gather
     return s;
   }
   switch (stage) {
@@ -491,6 +500,15 @@ Status run_chunks(Plan* p, bool fwd, bool bwd, const T* f0, typename Cx<T>::type
     T* fout = f0_out ? f0_out + b0 * mvol : nullptr;
     const T* Ec = E ? E + b0 * mvol : nullptr;
     auto* Fc = F + b0 * ns;
+    if (fwd && bwd && use_K && p->qmode) {
+      // Q-matrix diffusion step: forward transform to G0, Q-multiply + inverse z FFT,
+      // inverse x/y FFT + unfold (no spectral-ASU round trip).
+      for (int s : {0, 1, 4, 5}) {
+        Status r = launch_stage<T>(p, s, fin, Fc, Fc, fout, Ec, false, nb, ls, err, lane, true);
+        if (r != Status::kOk) return r;
+      }
+      continue;
+    }
     if (fwd)
       for (int s = 0; s < 3; ++s) {
         Status r = launch_stage<T>(p, s, fin, Fc, nullptr, nullptr, Ec, use_K, nb, ls, err, lane);
@@ -552,6 +570,13 @@ int64_t launch_count(bool reset) {
   const int64_t v = g_launches;
   if (reset) g_launches = 0;
   return v;
+}
+
+// M-grid column-major index of channel point (c, x, y, z) of the channel grid.
+static long q_of_channel_point(const PlanTables& T, int c, int x, int y, int z) {
+  if (!T.centered) return x + static_cast<long>(T.M[0]) * (y + static_cast<long>(T.M[1]) * z);
+  const auto& o = T.offsets[c];
+  return (2 * x + o[0]) + static_cast<long>(T.M[0]) * ((2 * y + o[1]) + static_cast<long>(T.M[1]) * (2 * z + o[2]));
 }
 
 Status plan_device_init(Plan* p, std::string* err) {
@@ -742,6 +767,38 @@ Status plan_device_init(Plan* p, std::string* err) {
       if ((st = alloc(&p->d_ft, p->lanes * p->ft_lane_bytes, "grouped spectra")) != Status::kOk) return st;
     }
   }
+  // Q-matrix step (M2Q / M7): runs on the compile-time sized kernels only.
+  if (p->qmode) {
+    if (!p->fast_h) {
+      *err = "the Q-matrix step needs a cubic channel grid of edge 4, 6, 8, 12, 16, 24, 32 (or 48 in FP32)";
+      return Status::kUnsupported;
+    }
+    const size_t np = static_cast<size_t>(T.n_ch) * hvol;
+    if ((st = alloc(&p->d_qt, T.d * np * cs, "Q coefficients")) != Status::kOk) return st;
+    if ((st = alloc(&p->d_gt, T.d * np * 4, "Q gather")) != Status::kOk) return st;
+    if ((st = alloc(&p->d_work_Q, p->lanes * p->w_lane_bytes, "Q workspace")) != Status::kOk) return st;
+    // Gather targets as indices into the z-fastest forward workspace WT[c][x][y][z].
+    const int H = T.H[0];
+    const long Mvol = static_cast<long>(T.M[0]) * T.M[1] * T.M[2];
+    std::vector<int32_t> gt(static_cast<size_t>(T.d) * np);
+    for (int b = 0; b < T.d; ++b)
+      for (int c = 0; c < T.n_ch; ++c)
+        for (int z = 0; z < H; ++z)
+          for (int y = 0; y < H; ++y)
+            for (int x = 0; x < H; ++x) {
+              const size_t pos = ((static_cast<size_t>(c) * H + z) * H + y) * H + x;
+              const long gq = p->q_gather[b * Mvol + q_of_channel_point(T, c, x, y, z)];
+              const int gv[3] = {static_cast<int>(gq % T.M[0]), static_cast<int>((gq / T.M[0]) % T.M[1]),
+                                 static_cast<int>(gq / (static_cast<long>(T.M[0]) * T.M[1]))};
+              int cc = 0, k[3] = {gv[0], gv[1], gv[2]};
+              if (T.centered) {
+                cc = T.chan_of_parity[(gv[0] & 1) + 2 * (gv[1] & 1) + 4 * (gv[2] & 1)];
+                for (int dd = 0; dd < 3; ++dd) k[dd] = gv[dd] >> 1;
+              }
+              gt[b * np + pos] = cc < 0 ? -1 : static_cast<int32_t>(cc * hvol + (static_cast<size_t>(k[0]) * H + k[1]) * H + k[2]);
+            }
+    CFFT_CUDA(cudaMemcpy(p->d_gt, gt.data(), gt.size() * 4, cudaMemcpyHostToDevice), "upload Q gather");
+  }
   CFFT_CUDA(cudaMemcpy(p->d_geom, &g, sizeof(g), cudaMemcpyHostToDevice), "upload geometry");
   CFFT_CUDA(cudaMemcpy(p->d_tables, tab.data(), tab.size(), cudaMemcpyHostToDevice), "upload tables");
   CFFT_CUDA(cudaMemcpy(p->d_spec_h, hp.data(), hp.size() * 4, cudaMemcpyHostToDevice), "upload spectral points");
@@ -782,7 +839,7 @@ Status plan_device_init(Plan* p, std::string* err) {
     const char* ce = std::getenv("CFFT_CLUSTER");
     const int want = ce ? std::atoi(ce) : 0;
     p->cluster_ctas = want == 16 ? 16 : 8;
-    p->cluster = want != 0 && p->reps_quad && fast_cluster_fits(p->fast_h, T.n_ch, p->precision);
+    p->cluster = want != 0 && !p->qmode && p->reps_quad && fast_cluster_fits(p->fast_h, T.n_ch, p->precision);
     if (p->cluster) {
       int mc = 0;
       st = p->precision == 8 ? fast_cluster_probe_f64(p->fast_h, p->cent_type, p->cluster_ctas, &mc, err)
@@ -823,13 +880,38 @@ Status plan_upload_kernel(Plan* p, std::string* err) {
     std::vector<float> k(p->T.K.begin(), p->T.K.end());
     CFFT_CUDA(cudaMemcpy(p->d_K, k.data(), k.size() * 4, cudaMemcpyHostToDevice), "upload K");
   }
+  if (p->qmode && p->d_qt) {
+    // Q first row in the order the Q-multiply kernel walks the channel points: [b][c][z][y][x].
+    const PlanTables& T = p->T;
+    const int H = T.H[0], d = T.d;
+    const long Mvol = static_cast<long>(T.M[0]) * T.M[1] * T.M[2];
+    const size_t np = static_cast<size_t>(T.n_ch) * H * H * H;
+    std::vector<double> qt(static_cast<size_t>(d) * np * 2);
+    for (int b = 0; b < d; ++b)
+      for (int c = 0; c < T.n_ch; ++c)
+        for (int z = 0; z < H; ++z)
+          for (int y = 0; y < H; ++y)
+            for (int x = 0; x < H; ++x) {
+              const size_t pos = ((static_cast<size_t>(c) * H + z) * H + y) * H + x;
+              const long q = q_of_channel_point(T, c, x, y, z);
+              qt[(b * np + pos) * 2] = p->q_host[(b * Mvol + q) * 2];
+              qt[(b * np + pos) * 2 + 1] = p->q_host[(b * Mvol + q) * 2 + 1];
+            }
+    if (p->precision == 8) {
+      CFFT_CUDA(cudaMemcpy(p->d_qt, qt.data(), qt.size() * 8, cudaMemcpyHostToDevice), "upload Q");
+    } else {
+      std::vector<float> qf(qt.begin(), qt.end());
+      CFFT_CUDA(cudaMemcpy(p->d_qt, qf.data(), qf.size() * 4, cudaMemcpyHostToDevice), "upload Q");
+    }
+  }
   return Status::kOk;
 }
 
 void plan_device_free(Plan* p) {
   void** bufs[] = {&p->d_geom, &p->d_tables, &p->d_spec_h, &p->d_K, &p->d_orbit_rep, &p->d_inv_spec,
                    &p->d_inv_phase, &p->d_img_mask, &p->d_fill_map, &p->d_work_T, &p->d_work_F,
-                   &p->d_work_E, &p->d_stage_in, &p->d_stage_out, &p->d_expand, &p->d_g0r, &p->d_inv_pk, &p->d_ft};
+                   &p->d_work_E, &p->d_stage_in, &p->d_stage_out, &p->d_expand, &p->d_g0r, &p->d_inv_pk, &p->d_ft,
+                   &p->d_qt, &p->d_gt, &p->d_work_Q};
   for (void** b : bufs)
     if (*b) { cudaFree(*b); *b = nullptr; }
   if (p->own_stream) { cudaStreamDestroy(static_cast<cudaStream_t>(p->own_stream)); p->own_stream = nullptr; }

@@ -58,6 +58,14 @@ struct Plan {
   bool rep_diag8 = false;       // representative ops are the 8 diagonal sign matrices
   bool reps_quad = false;       // packed alias rows; fields gathered and expanded in quads
   bool cluster = false;         // fused cluster kernels: fold+xyz FFT and expand+xyz IFFT+unfold
+  // Q-matrix diffusion step (M2Q: plain path, M7: centred path): host tables and their
+  // channel-point ordered device copies, plus a second channel workspace per lane.
+  int qmode = 0;                // 0 none, 3 M2Q, 4 M7 (the cfft_path value)
+  std::vector<double> q_host;   // d x Mvol complex (re, im)
+  std::vector<int32_t> q_gather;  // d x Mvol
+  void* d_qt = nullptr;         // d x n_ch x H^3 complex coefficients
+  void* d_gt = nullptr;         // d x n_ch x H^3 int32 workspace index (-1: extinct class)
+  void* d_work_Q = nullptr;     // lanes x channel workspace (Q-multiply output)
   int cluster_ctas = 8;         // CTAs per cluster
   size_t smem_xy = 0, smem_z = 0;
 };

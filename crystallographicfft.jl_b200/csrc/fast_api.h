@@ -34,6 +34,11 @@ struct FastArgs {
   bool use_K = false, rep_diag8 = false, rep_perm = false, reps_quad = false;
   bool cluster = false;   // fused cluster kernels for stages 0 (with 1) and 5 (with 4)
   int cluster_ctas = 8;   // CTAs per cluster (8, or 16 where the device allows it)
+  // Q-matrix step: stage 4 reads W (forward G0, z-fastest) and writes W2
+  bool q_step = false;
+  const void* QT = nullptr;   // d x n_ch x H^3 coefficients
+  const void* GT = nullptr;   // d x n_ch x H^3 int32 workspace indices (-1: extinct)
+  void* W2 = nullptr;
   void* stream = nullptr;
 };
 

@@ -907,6 +907,47 @@ __global__ void k_expand4_ifft_z_h(const DevGeom* __restrict__ g, const typename
   for (int z = 0; z < H; ++z) dst[z * H * H] = v[z];
 }
 
+// Q-matrix diffusion step (execute_m2_q! / execute_m7_scft!, src/q_fused_krfft.jl:553-667,
+// 870-895): for every channel point (c, x, y, z) of a slot, q its subgrid position,
+//   Y'(q) = sum_b Q_b(q) G0(R_b^T q mod M)
+// with G0 gathered from the forward workspace WT (z-fastest; index -1 marks a parity
+// class without a channel, where G0 = 0), assembled as the z line of (c, y, x), inverse z
+// FFT in registers, stored W2[slot][c][z][y][x] for the inverse plane kernel.  Both
+// fields of the slot (G0_a + i G0_b) go through the same complex-linear map.
+template <typename T, int H>
+__global__ void k_qmul_ifft_z_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ QT,
+                                const int32_t* __restrict__ GT, const typename Cx<T>::type* __restrict__ WT,
+                                typename Cx<T>::type* __restrict__ W2) {
+  using C = typename Cx<T>::type;
+  constexpr int HV = H * H * H;
+  const int y0 = blockIdx.x * kZB, c = blockIdx.y, slot = blockIdx.z;
+  const int ny = min(kZB, H - y0);
+  const int yy = threadIdx.x / H, x = threadIdx.x % H;
+  if (yy >= ny) return;
+  const int y = y0 + yy;
+  const int d = g->d;
+  const size_t np = static_cast<size_t>(g->n_ch) * HV;
+  const C* wt = WT + static_cast<size_t>(slot) * g->n_ch * HV;
+  C v[H];
+#pragma unroll
+  for (int z = 0; z < H; ++z) {
+    const size_t pos = static_cast<size_t>(c) * HV + (z * H + y) * H + x;
+    C acc = mk<C>(static_cast<T>(0), static_cast<T>(0));
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      if (b < d) {
+        const int32_t gi = __ldg(GT + b * np + pos);
+        if (gi >= 0) acc = cadd(acc, cmul(__ldg(QT + b * np + pos), __ldg(wt + gi)));
+      }
+    }
+    v[z] = acc;
+  }
+  reg_fft<C, true, H>(v);
+  C* dst = W2 + (static_cast<size_t>(slot) * g->n_ch + c) * HV + y * H + x;
+#pragma unroll
+  for (int z = 0; z < H; ++z) dst[z * H * H] = v[z];
+}
+
 constexpr int kMaxDynSmemFast = 227 * 1024;
 
 #define CFFT_FOR_H(H, ...)                                                        \
@@ -1192,6 +1233,14 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
         break;
       }
       default:
+        if (a.q_step) {
+          CFFT_FOR_H(H, {
+            k_qmul_ifft_z_h<T, HH><<<gz, thr_z, 0, st>>>(g, static_cast<const C*>(a.QT),
+                                                         static_cast<const int32_t*>(a.GT), W,
+                                                         static_cast<C*>(a.W2));
+          });
+          break;
+        }
         CFFT_FOR_H(H, {
           if (a.reps_quad) {
             constexpr int half = ((kZB * HH + 31) / 32) * 32;

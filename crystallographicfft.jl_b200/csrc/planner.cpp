@@ -5,6 +5,7 @@
 // identical to the reference's.
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <numeric>
 #include <set>
 
@@ -547,6 +548,111 @@ void compute_kernel(const PlanTables& T, const double* lattice, double ds, std::
     }
     (*K)[s] = std::exp(-k2 * ds);
   }
+}
+
+// Q-matrix tables of the M2+Q / M7 diffusion step (plan_m2_q, _build_q_matrices!,
+// src/q_fused_krfft.jl:83-169,182-413).  For each subgrid point q (column-major) and
+// parity class a, h_a = q + M.alpha_a (classes in Iterators.product order, first axis
+// fastest), B[a][b] = e^{-2 pi i h_a.t_b / N} over the representative operations b and
+// K_a = exp(-ds |2 pi A^-T h_a,c|^2).  Q(q) = B^-1 diag(K) B; only its first row is
+// used: Q[b] = sum_a y_a K_a B[a][b] with B^T y = e_0.  gather[b][q] = lin(R_b^T q mod M).
+// Q is returned interleaved (re, im) as Q[(b * Mvol + q) * 2 + {0, 1}].
+Status build_q_tables(const PlanTables& T, const double* lattice, double ds, std::vector<double>* Q,
+                      std::vector<int32_t>* gather, std::string* err) {
+  using cd = std::complex<double>;
+  const int d = static_cast<int>(T.rep_ops.size());
+  const long Mvol = static_cast<long>(T.M[0]) * T.M[1] * T.M[2];
+  if (d < 1 || d > 8) { *err = "Q tables need 1..8 representative operations"; return Status::kInvalid; }
+  double A[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) A[i][j] = lattice[i + 3 * j];
+  if (T.dim == 2)
+    for (int i = 0; i < 3; ++i) { A[i][2] = (i == 2); A[2][i] = (i == 2); }
+  const double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
+                     A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+                     A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+  if (det == 0.0) { *err = "singular lattice"; return Status::kInvalid; }
+  double inv[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      const int i1 = (j + 1) % 3, i2 = (j + 2) % 3, j1 = (i + 1) % 3, j2 = (i + 2) % 3;
+      inv[i][j] = (A[i1][j1] * A[i2][j2] - A[i1][j2] * A[i2][j1]) / det;  // adjugate / det
+    }
+  // parity classes alpha_a, first axis fastest
+  std::vector<std::array<int, 3>> alpha(d);
+  for (int a = 0; a < d; ++a) {
+    int r = a;
+    for (int k = 0; k < 3; ++k) { alpha[a][k] = r % T.L[k]; r /= T.L[k]; }
+  }
+  if (T.L[0] * T.L[1] * T.L[2] != d) { *err = "parity classes do not match the representatives"; return Status::kInvalid; }
+  Q->assign(static_cast<size_t>(d) * Mvol * 2, 0.0);
+  gather->assign(static_cast<size_t>(d) * Mvol, 0);
+  for (long q = 0; q < Mvol; ++q) {
+    const long qv[3] = {q % T.M[0], (q / T.M[0]) % T.M[1], q / (static_cast<long>(T.M[0]) * T.M[1])};
+    cd Bm[8][8];
+    double Kv[8];
+    for (int a = 0; a < d; ++a) {
+      long h[3];
+      double hc[3];
+      for (int k = 0; k < 3; ++k) {
+        h[k] = qv[k] + static_cast<long>(T.M[k]) * alpha[a][k];
+        hc[k] = (h[k] >= T.N[k] / 2) ? static_cast<double>(h[k] - T.N[k]) : static_cast<double>(h[k]);
+        if (k >= T.dim) hc[k] = 0.0;
+      }
+      double k2 = 0.0;
+      for (int i = 0; i < 3; ++i) {
+        double kk = 0.0;
+        for (int j = 0; j < 3; ++j) kk += inv[j][i] * hc[j];
+        kk *= 2.0 * M_PI;
+        k2 += kk * kk;
+      }
+      Kv[a] = std::exp(-k2 * ds);
+      for (int b = 0; b < d; ++b) {
+        double ph = 0.0;
+        for (int k = 0; k < T.dim; ++k) ph += static_cast<double>(h[k]) * T.rep_ops[b].t[k] / T.N[k];
+        Bm[a][b] = std::polar(1.0, -2.0 * M_PI * ph);
+      }
+    }
+    // Solve B^T y = e_0 by Gaussian elimination with partial pivoting.
+    cd Mx[8][9];
+    for (int i = 0; i < d; ++i) {
+      for (int j = 0; j < d; ++j) Mx[i][j] = Bm[j][i];
+      Mx[i][d] = (i == 0) ? cd(1.0, 0.0) : cd(0.0, 0.0);
+    }
+    for (int c = 0; c < d; ++c) {
+      int piv = c;
+      for (int i = c + 1; i < d; ++i)
+        if (std::abs(Mx[i][c]) > std::abs(Mx[piv][c])) piv = i;
+      if (std::abs(Mx[piv][c]) < 1e-12) { *err = "singular alias matrix B"; return Status::kInvalid; }
+      if (piv != c)
+        for (int j = 0; j <= d; ++j) std::swap(Mx[c][j], Mx[piv][j]);
+      for (int i = c + 1; i < d; ++i) {
+        const cd f = Mx[i][c] / Mx[c][c];
+        for (int j = c; j <= d; ++j) Mx[i][j] -= f * Mx[c][j];
+      }
+    }
+    cd y[8];
+    for (int i = d - 1; i >= 0; --i) {
+      cd acc = Mx[i][d];
+      for (int j = i + 1; j < d; ++j) acc -= Mx[i][j] * y[j];
+      y[i] = acc / Mx[i][i];
+    }
+    for (int b = 0; b < d; ++b) {
+      cd acc(0.0, 0.0);
+      for (int a = 0; a < d; ++a) acc += y[a] * Kv[a] * Bm[a][b];
+      (*Q)[(static_cast<size_t>(b) * Mvol + q) * 2] = acc.real();
+      (*Q)[(static_cast<size_t>(b) * Mvol + q) * 2 + 1] = acc.imag();
+      long g = 0, stride = 1;
+      for (int k = 0; k < 3; ++k) {
+        long v = 0;
+        for (int j = 0; j < 3; ++j) v += static_cast<long>(T.rep_ops[b].R[j][k]) * qv[j];  // (R^T q)_k
+        g += floor_mod(v, T.M[k]) * stride;
+        stride *= T.M[k];
+      }
+      (*gather)[static_cast<size_t>(b) * Mvol + q] = static_cast<int32_t>(g);
+    }
+  }
+  return Status::kOk;
 }
 
 }  // namespace cfft

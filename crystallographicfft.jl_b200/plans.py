@@ -24,7 +24,7 @@ import numpy as np
 from . import symmetry as sym
 from ._lib import LIB, CFFTDesc, CFFTError, CFFTInfo, check
 
-PATH_AUTO, PATH_M2, PATH_CENTERED = 0, 1, 2
+PATH_AUTO, PATH_M2, PATH_CENTERED, PATH_M2Q, PATH_M7 = 0, 1, 2, 3, 4
 _REAL = {4: np.float32, 8: np.float64}
 _CPLX = {4: np.complex64, 8: np.complex128}
 
@@ -114,6 +114,16 @@ class KRFFTPlan:
         return int(np.prod(self.M))
 
     # -- tables ---------------------------------------------------------------
+    def q_tables(self):
+        """Q-matrix first row (n_rep, Mvol) complex and gather indices (n_rep, Mvol), 0-based
+        column-major subgrid positions, of an M2Q / M7 plan (_build_q_matrices!,
+        src/q_fused_krfft.jl:182-413)."""
+        d, mvol = self.info.n_rep, self.mvol
+        q = np.zeros(2 * d * mvol, dtype=np.float64)
+        gidx = np.zeros(d * mvol, dtype=np.int32)
+        check(LIB.cfft_plan_q_tables(self._h, q.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), sym._ptr(gidx)))
+        return (q[0::2] + 1j * q[1::2]).reshape(d, mvol), gidx.reshape(d, mvol)
+
     def spectral_asu(self):
         idx = np.zeros((self.n_spec, 3), dtype=np.int32)
         mult = np.zeros(self.n_spec, dtype=np.int32)
@@ -321,6 +331,36 @@ def plan_m2_scft(N, sg_num, dim, ds, lattice, *, precision=8, max_batch=1):
     spec = sym.calc_spectral_asu(ops_s, dim, N)
     return KRFFTPlan(spec, ops_s, N=N, ds=ds, lattice=lattice, precision=precision, max_batch=max_batch,
                      path=PATH_M2)
+
+
+def plan_m2_q(N, sg_num, dim, ds, lattice, *, precision=8, max_batch=1, device=True):
+    """plan_m2_q (src/q_fused_krfft.jl:83-169): the plain stride-L path whose SCFT step
+    multiplies the subgrid spectrum by the first row of Q(q) = B^-1 diag(K) B."""
+    ops = sym.get_ops(sg_num, dim, N)
+    _, ops_s = sym.find_optimal_shift(ops, N)
+    spec = sym.calc_spectral_asu(ops_s, dim, N)
+    return KRFFTPlan(spec, ops_s, N=N, ds=ds, lattice=lattice, precision=precision, max_batch=max_batch,
+                     path=PATH_M2Q, device=device)
+
+
+def execute_m2_q(plan, f0):
+    """execute_m2_q! (src/q_fused_krfft.jl:553-576): f0 <- real(IFFT(Q . FFT(f0)))."""
+    return plan.scft_step(f0)
+
+
+def plan_m7_scft(N, sg_num, dim, ds, lattice, *, precision=8, max_batch=1, device=True):
+    """plan_m7_scft (src/q_fused_krfft.jl:822-850): centring fold + channel FFTs + Q-multiply
+    + unfold.  Raises CFFTError for P lattices and odd subgrids, like the reference."""
+    ops = sym.get_ops(sg_num, dim, N)
+    _, ops_s = sym.find_optimal_shift(ops, N)
+    spec = sym.calc_spectral_asu(ops_s, dim, N)
+    return KRFFTPlan(spec, ops_s, N=N, ds=ds, lattice=lattice, precision=precision, max_batch=max_batch,
+                     path=PATH_M7, device=device)
+
+
+def execute_m7_scft(plan, f0):
+    """execute_m7_scft! (src/q_fused_krfft.jl:870-895)."""
+    return plan.scft_step(f0)
 
 
 def execute_krfft(plan, u):

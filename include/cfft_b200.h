@@ -46,7 +46,12 @@ typedef enum cfft_status {
 typedef enum cfft_path {
   CFFT_PATH_AUTO = 0,     /* centred fold when applicable, else M2 (plan_krfft_centered) */
   CFFT_PATH_M2 = 1,       /* plain stride-L path: plan_krfft + plan_m2_backward */
-  CFFT_PATH_CENTERED = 2  /* same as AUTO: plan_krfft_centered falls back to M2 itself */
+  CFFT_PATH_CENTERED = 2, /* same as AUTO: plan_krfft_centered falls back to M2 itself */
+  CFFT_PATH_M2Q = 3,      /* plan_m2_q (src/q_fused_krfft.jl:83): plain stride-L FFT; the SCFT
+                             step applies the Q-matrix first row (d-tap gather) to the subgrid
+                             spectrum instead of going through the spectral ASU */
+  CFFT_PATH_M7 = 4        /* plan_m7_scft (src/q_fused_krfft.jl:822): centring fold + channel FFTs
+                             + Q-multiply + unfold; centred lattices only, like the reference */
 } cfft_path;
 
 typedef enum cfft_centering {
@@ -89,6 +94,12 @@ typedef struct cfft_info {
 } cfft_info;
 
 /* ---------------- plan-time functions (host only, no GPU needed) ---------------- */
+
+/* _build_q_matrices! (src/q_fused_krfft.jl:182-413) tables of an M2Q / M7 plan (also
+ * host plans): Q first row Q[(b * Mvol + q) * 2 + {re, im}] and gather[b * Mvol + q]
+ * (0-based column-major subgrid index of R_b^T q mod M), b < n_rep, q < M1 M2 M3.
+ * Either pointer may be NULL.  CFFT_UNSUPPORTED for plans of the other paths. */
+cfft_status cfft_plan_q_tables(cfft_plan plan, double* Q, int32_t* gather);
 
 /* get_ops(sg, dim, N) (src/symmetry_ops.jl:51-53): operations of space group `sg`
  * (plane group for dim = 2) in ITA order, converted to grid units like convert_op
