@@ -12,7 +12,8 @@ from .symmetry import (  # noqa: F401
 )
 from .plans import (  # noqa: F401
     DiffusionSolver, KRFFTPlan, PATH_AUTO, PATH_CENTERED, PATH_M2, PATH_M2Q, PATH_M7, execute_centered_ikrfft,
-    execute_centered_krfft, execute_m2_q, execute_m7_scft, plan_m2_q, plan_m7_scft,
+    execute_centered_krfft, execute_m2_q, execute_m7_scft, plan_m2_q, plan_m7_scft, PATH_FULLGRID,
+    CenteringPreFoldPlan, plan_centering_prefold, plan_krfft_prefold, execute_prefold_krfft,
     execute_centered_scft, execute_krfft, execute_m2_backward, execute_m2_scft, fft_reconstruct,
     fft_reconstruct_centered, fullgrid_to_subgrid, ifft_unrecon_centered, plan_centered_ikrfft, plan_centered_scft,
     plan_diffusion, plan_krfft, plan_krfft_centered, plan_m2_backward, plan_m2_scft, step_diffusion,

@@ -139,7 +139,7 @@ static cfft_status plan_create_impl(const cfft_desc* desc, cfft_plan* plan, bool
     return ret(Status::kInvalid, err);
   if (desc->precision != 4 && desc->precision != 8) return ret(Status::kInvalid, "precision must be 4 or 8");
   if (desc->max_batch < 1) return ret(Status::kInvalid, "max_batch must be positive");
-  if (desc->path < 0 || desc->path > 4) return ret(Status::kInvalid, "unknown path");
+  if (desc->path < 0 || desc->path > 5) return ret(Status::kInvalid, "unknown path");
   auto* p = new (std::nothrow) cfft::Plan();
   if (!p) return ret(Status::kAlloc, "host allocation failed");
   p->precision = desc->precision;
@@ -147,7 +147,7 @@ static cfft_status plan_create_impl(const cfft_desc* desc, cfft_plan* plan, bool
   p->ds = desc->ds;
   std::memcpy(p->lattice, desc->lattice, sizeof(p->lattice));
   const bool plain = desc->path == CFFT_PATH_M2 || desc->path == CFFT_PATH_M2Q;
-  Status s = cfft::build_tables(ops, n, desc->dim, !plain, &p->T, &err);
+  Status s = cfft::build_tables(ops, n, desc->dim, !plain, &p->T, &err, desc->path == CFFT_PATH_FULLGRID);
   if (s == Status::kOk && (desc->path == CFFT_PATH_M2Q || desc->path == CFFT_PATH_M7)) {
     // plan_m7_scft (src/q_fused_krfft.jl:822-850) refuses P lattices and odd subgrids;
     // the centred plan exists exactly when neither holds.

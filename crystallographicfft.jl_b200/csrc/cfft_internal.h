@@ -93,7 +93,7 @@ struct PlanTables {
 };
 
 Status build_tables(const std::vector<SymOp>& shifted_ops, const int* N, int dim, bool want_centered,
-                    PlanTables* T, std::string* err);
+                    PlanTables* T, std::string* err, bool full_grid = false);
 void compute_kernel(const PlanTables& T, const double* lattice, double ds, std::vector<double>* K);
 Status build_q_tables(const PlanTables& T, const double* lattice, double ds, std::vector<double>* Q,
                       std::vector<int32_t>* gather, std::string* err);

@@ -342,7 +342,7 @@ int alive_offsets(Centering c, std::array<int, 3>* o) {
 static long lcm_l(long a, long b) { return a / std::gcd(a, b) * b; }
 
 Status build_tables(const std::vector<SymOp>& shifted_ops, const int* N_in, int dim, bool want_centered,
-                    PlanTables* T, std::string* err) {
+                    PlanTables* T, std::string* err, bool full_grid) {
   if (shifted_ops.empty()) { *err = "empty operation list"; return Status::kInvalid; }
   T->dim = dim;
   for (int d = 0; d < 3; ++d) T->N[d] = d < dim ? N_in[d] : 1;
@@ -355,7 +355,9 @@ Status build_tables(const std::vector<SymOp>& shifted_ops, const int* N_in, int 
       op.t[d] = 0;
       for (int j = 0; j < 3; ++j) op.R[d][j] = op.R[j][d] = (d == j);
     }
-  const std::array<int, 3> L = auto_L(T->ops, dim);
+  // Full-grid plans (the centring prefold, src/centering_prefold.jl) keep L = 1: the
+  // "subgrid" is the whole grid and the identity is the only representative.
+  const std::array<int, 3> L = full_grid ? std::array<int, 3>{1, 1, 1} : auto_L(T->ops, dim);
   for (int d = 0; d < 3; ++d) {
     T->L[d] = L[d];
     if (N[d] % L[d] != 0) { *err = "Grid size N not divisible by auto L"; return Status::kNotCommensurate; }
@@ -376,7 +378,10 @@ Status build_tables(const std::vector<SymOp>& shifted_ops, const int* N_in, int 
   T->centering = detect_centering_type(T->ops, N, dim);
   // plan_krfft_centered falls back to the plain path for P, L != 2, or odd M
   // (src/centering_fold.jl:339-352).
-  T->centered = want_centered && T->centering != kCentP && dim == 3 && L[0] == 2 && L[1] == 2 && L[2] == 2 &&
+  // Full-grid plans fold the whole grid into the parity channels of (N/2)^3, which is
+  // exact for any field; the centring only decides which channels exist.
+  T->centered = want_centered && T->centering != kCentP && dim == 3 &&
+                (full_grid || (L[0] == 2 && L[1] == 2 && L[2] == 2)) &&
                 T->M[0] % 2 == 0 && T->M[1] % 2 == 0 && T->M[2] % 2 == 0;
   for (int p = 0; p < 8; ++p) T->chan_of_parity[p] = -1;
   if (T->centered) {

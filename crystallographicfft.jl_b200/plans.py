@@ -24,7 +24,7 @@ import numpy as np
 from . import symmetry as sym
 from ._lib import LIB, CFFTDesc, CFFTError, CFFTInfo, check
 
-PATH_AUTO, PATH_M2, PATH_CENTERED, PATH_M2Q, PATH_M7 = 0, 1, 2, 3, 4
+PATH_AUTO, PATH_M2, PATH_CENTERED, PATH_M2Q, PATH_M7, PATH_FULLGRID = 0, 1, 2, 3, 4, 5
 _REAL = {4: np.float32, 8: np.float64}
 _CPLX = {4: np.complex64, 8: np.complex128}
 
@@ -361,6 +361,51 @@ def plan_m7_scft(N, sg_num, dim, ds, lattice, *, precision=8, max_batch=1, devic
 def execute_m7_scft(plan, f0):
     """execute_m7_scft! (src/q_fused_krfft.jl:870-895)."""
     return plan.scft_step(f0)
+
+
+class CenteringPreFoldPlan:
+    """CenteringPreFoldPlan / plan_centering_prefold (src/centering_prefold.jl:27-58): the
+    channel definition of the prefold (parity classes kept, halved grid, shift offsets of
+    the folded copies).  Host metadata only; the device prefold is plan_krfft_prefold."""
+
+    def __init__(self, centering, N):
+        N = tuple(int(n) for n in N)
+        h = tuple(n // 2 for n in N)
+        if centering == "I":
+            self.N_sub, self.parities = h, [(0, 0, 0), (1, 1, 0), (1, 0, 1), (0, 1, 1)]
+            self.shift_offsets = [(h[0], 0, 0), (0, h[1], 0), (0, 0, h[2])]
+        elif centering == "F":
+            self.N_sub, self.parities, self.shift_offsets = h, [(0, 0, 0), (1, 1, 1)], [(h[0], 0, 0)]
+        elif centering == "C":
+            self.N_sub, self.parities, self.shift_offsets = (h[0], h[1], N[2]), [(0, 0, 0), (1, 1, 0)], [(h[0], 0, 0)]
+        elif centering == "A":
+            self.N_sub, self.parities, self.shift_offsets = (N[0], h[1], h[2]), [(0, 0, 0), (0, 1, 1)], [(0, h[1], 0)]
+        else:
+            raise CFFTError(1, "CentP has no pre-fold")
+        self.centering, self.N_full, self.n_channels = centering, N, len(self.parities)
+
+
+def plan_centering_prefold(centering, N):
+    """plan_centering_prefold (src/centering_prefold.jl:36-58)."""
+    return CenteringPreFoldPlan(centering, N)
+
+
+def plan_krfft_prefold(ops_shifted, N, *, precision=8, max_batch=1, ds=0.0, lattice=None, device=True):
+    """The prefold CenteredKRFFTPlan (plan_krfft_centered(ops, N), src/centering_prefold.jl:
+    175-205; that constructor shares its name and struct name with the fold plan in the
+    reference): a full-grid plan whose forward folds the whole grid into the parity
+    channels of (N/2)^3 and merges the channel spectra onto the spectral ASU.  Its
+    backward returns the whole grid with the symmetry fill."""
+    dim = len(N)
+    spec = sym.calc_spectral_asu(ops_shifted, dim, N)
+    return KRFFTPlan(spec, ops_shifted, N=N, ds=ds, lattice=np.eye(3) if lattice is None else lattice,
+                     precision=precision, max_batch=max_batch, path=PATH_FULLGRID, device=device)
+
+
+def execute_prefold_krfft(plan, u):
+    """execute_centered_krfft!(::CenteredKRFFTPlan (prefold), u) (src/centering_prefold.jl:
+    236-244): prefold + channel FFTs + _merge_channels! -> spectrum on the ASU."""
+    return plan.forward(u)
 
 
 def execute_krfft(plan, u):

@@ -50,8 +50,14 @@ typedef enum cfft_path {
   CFFT_PATH_M2Q = 3,      /* plan_m2_q (src/q_fused_krfft.jl:83): plain stride-L FFT; the SCFT
                              step applies the Q-matrix first row (d-tap gather) to the subgrid
                              spectrum instead of going through the spectral ASU */
-  CFFT_PATH_M7 = 4        /* plan_m7_scft (src/q_fused_krfft.jl:822): centring fold + channel FFTs
+  CFFT_PATH_M7 = 4,       /* plan_m7_scft (src/q_fused_krfft.jl:822): centring fold + channel FFTs
                              + Q-multiply + unfold; centred lattices only, like the reference */
+  CFFT_PATH_FULLGRID = 5  /* full-grid plan, L = 1: the forward is the centring prefold of the whole
+                             grid u into parity channels of (N/2)^3 + channel FFTs + merge onto the
+                             spectral ASU (CenteringPreFoldPlan, _merge_channels!,
+                             src/centering_prefold.jl:27-257); the backward returns the whole grid
+                             with the symmetry fill (src/recursive_blocks_backward.jl:531-545).
+                             Fields are N1 x N2 x N3 (M = N in cfft_info). */
 } cfft_path;
 
 typedef enum cfft_centering {
