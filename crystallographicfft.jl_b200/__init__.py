@@ -20,4 +20,13 @@ from .plans import (  # noqa: F401
     subgrid_to_fullgrid, update_kernel, update_m2_kernel,
 )
 
+from .variants import (  # noqa: F401
+    G0ASUBackwardPlan, StagedPm3mPlan, VariantKRFFTPlan, execute_fractal_krfft, execute_fractal_krfft_v2,
+    execute_fractal_krfft_v3, execute_g0asu_ikrfft, execute_g0asu_krfft, execute_general_g0asu_krfft,
+    execute_recursive_krfft, execute_selective_krfft, execute_sparse_krfft, execute_staged, execute_staged_full,
+    lookup_full_spectrum, plan_fractal_krfft, plan_fractal_krfft_v2, plan_fractal_krfft_v3, plan_krfft_g0asu,
+    plan_krfft_g0asu_backward, plan_krfft_g0asu_general, plan_krfft_recursive, plan_krfft_selective,
+    plan_krfft_sparse, plan_staged_pm3m, plan_staged_pm3m_full,
+)
+
 __version__ = "0.1.0"

@@ -297,6 +297,9 @@ cfft_status cfft_fullgrid_to_subgrid(cfft_plan plan, const void* u, void* f0, in
 cfft_status cfft_subgrid_to_fullgrid(cfft_plan plan, const void* f0, void* u, int batch, void* stream) {
   CFFT_EXEC(cfft::exec_sub_to_full(p, f0, u, batch, stream, &err));
 }
+cfft_status cfft_subgrid_spectrum(cfft_plan plan, const void* f0, void* G0, int batch, void* stream) {
+  CFFT_EXEC(cfft::exec_subgrid_spectrum(p, f0, G0, batch, stream, &err));
+}
 cfft_status cfft_forward_host(cfft_plan plan, const void* f0_host, void* F_host, int batch) {
   CFFT_EXEC(cfft::exec_host(p, 0, f0_host, F_host, batch, &err));
 }

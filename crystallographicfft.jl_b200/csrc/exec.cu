@@ -306,6 +306,52 @@ __global__ void k_interaction(const T* __restrict__ w, T* __restrict__ E, T half
     E[i] = exp(-w[i] * half_dt);
 }
 
+// Subgrid spectrum G0 = FFT_M(f0) of each field from the forward workspace of the
+// compile-time sized path (slot s holds X = G0_a + i G0_b, z-fastest per channel):
+// G0_a(q) = (X(q) + conj X(-q)) / 2, G0_b(q) = (X(q) - conj X(-q)) / 2i.  On the
+// centred path q = 2k + off reads channel chan_of_parity(off) at k, and -q at
+// k' = off ? H - 1 - k : (H - k) mod H; parity classes without a channel are 0.
+// Output [field][q3][q2][q1] complex (x fastest), one thread per subgrid point.
+template <typename T>
+__global__ void k_unpack_g0(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ WT,
+                            typename Cx<T>::type* __restrict__ G0, int nfields) {
+  using C = typename Cx<T>::type;
+  const long mvol = static_cast<long>(g->M[0]) * g->M[1] * g->M[2];
+  const long q = static_cast<long>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (q >= mvol) return;
+  const int slot = blockIdx.y;
+  const int qv[3] = {static_cast<int>(q % g->M[0]), static_cast<int>((q / g->M[0]) % g->M[1]),
+                     static_cast<int>(q / (static_cast<long>(g->M[0]) * g->M[1]))};
+  const int H0 = g->H[0], H1 = g->H[1], H2 = g->H[2];
+  const long hv = static_cast<long>(H0) * H1 * H2;
+  int c = 0, k[3], km[3];
+  if (g->centered) {
+    c = g->chan_of_parity[(qv[0] & 1) + 2 * (qv[1] & 1) + 4 * (qv[2] & 1)];
+    const int Hd[3] = {H0, H1, H2};
+    for (int d = 0; d < 3; ++d) {
+      k[d] = qv[d] >> 1;
+      km[d] = (qv[d] & 1) ? Hd[d] - 1 - k[d] : (Hd[d] - k[d]) % Hd[d];
+    }
+  } else {
+    const int Md[3] = {g->M[0], g->M[1], g->M[2]};
+    for (int d = 0; d < 3; ++d) {
+      k[d] = qv[d];
+      km[d] = (Md[d] - qv[d]) % Md[d];
+    }
+  }
+  C ga = mk<C>(static_cast<T>(0), static_cast<T>(0)), gb = ga;
+  if (c >= 0) {
+    const C* w = WT + (static_cast<long>(slot) * g->n_ch + c) * hv;
+    const C x = w[(static_cast<long>(k[0]) * H1 + k[1]) * H2 + k[2]];
+    const C xm = w[(static_cast<long>(km[0]) * H1 + km[1]) * H2 + km[2]];
+    const T h = static_cast<T>(0.5);
+    ga = mk<C>(h * (x.x + xm.x), h * (x.y - xm.y));
+    gb = mk<C>(h * (x.y + xm.y), h * (xm.x - x.x));
+  }
+  G0[(2L * slot) * mvol + q] = ga;
+  if (2 * slot + 1 < nfields) G0[(2L * slot + 1) * mvol + q] = gb;
+}
+
 template <typename T>
 __global__ void k_full_to_sub(const T* __restrict__ u, T* __restrict__ f0, int N1, int N2, int L1, int L2, int L3,
                               int M1, int M2, size_t mvol, size_t nvol, int B) {
@@ -1048,6 +1094,44 @@ Status exec_full_to_sub(Plan* p, const void* u, void* f0, int B, void* stream, s
                                               T.L[0], T.L[1], T.L[2], T.M[0], T.M[1], mvol, nvol, B);
   ++g_launches;
   CFFT_CUDA(cudaGetLastError(), "fullgrid_to_subgrid launch");
+  return Status::kOk;
+}
+
+// Subgrid spectrum G0 = FFT_M(f0) per field (the F000 of execute_staged!, the Y buffer
+// of the M2Q path): forward fold + transforms of each chunk, then k_unpack_g0.
+Status exec_subgrid_spectrum(Plan* p, const void* f0, void* G0, int B, void* stream, std::string* err) {
+  Status st = check_batch(p, B, err);
+  if (st != Status::kOk) return st;
+  if (!f0 || !G0) { *err = "null pointer"; return Status::kInvalid; }
+  if (!p->fast_h) {
+    *err = "the subgrid spectrum needs a cubic channel grid of edge 4, 6, 8, 12, 16, 24, 32 (or 48 in FP32)";
+    return Status::kUnsupported;
+  }
+  const PlanTables& T = p->T;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t mvol = static_cast<size_t>(T.M[0]) * T.M[1] * T.M[2];
+  const dim3 blk(256);
+  for (int b0 = 0; b0 < B; b0 += p->chunk) {
+    const int nb = std::min(p->chunk, B - b0);
+    const dim3 grid(static_cast<unsigned>((mvol + 255) / 256), static_cast<unsigned>((nb + 1) / 2));
+    if (p->precision == 8) {
+      const double* fin = static_cast<const double*>(f0) + b0 * mvol;
+      for (int stage = 0; stage < 2; ++stage)
+        if ((st = launch_stage<double>(p, stage, fin, nullptr, nullptr, nullptr, nullptr, false, nb, s, err)) != Status::kOk)
+          return st;
+      k_unpack_g0<double><<<grid, blk, 0, s>>>(static_cast<const DevGeom*>(p->d_geom), static_cast<const double2*>(p->d_work_T),
+                                               static_cast<double2*>(G0) + b0 * mvol, nb);
+    } else {
+      const float* fin = static_cast<const float*>(f0) + b0 * mvol;
+      for (int stage = 0; stage < 2; ++stage)
+        if ((st = launch_stage<float>(p, stage, fin, nullptr, nullptr, nullptr, nullptr, false, nb, s, err)) != Status::kOk)
+          return st;
+      k_unpack_g0<float><<<grid, blk, 0, s>>>(static_cast<const DevGeom*>(p->d_geom), static_cast<const float2*>(p->d_work_T),
+                                              static_cast<float2*>(G0) + b0 * mvol, nb);
+    }
+    ++g_launches;
+  }
+  CFFT_CUDA(cudaGetLastError(), "subgrid spectrum launch");
   return Status::kOk;
 }
 

@@ -81,6 +81,7 @@ Status exec_step_diffusion(Plan* p, void* q, const void* w, double dt, int n_ste
                            std::string* err);
 Status exec_full_to_sub(Plan* p, const void* u, void* f0, int B, void* stream, std::string* err);
 Status exec_sub_to_full(Plan* p, const void* f0, void* u, int B, void* stream, std::string* err);
+Status exec_subgrid_spectrum(Plan* p, const void* f0, void* G0, int B, void* stream, std::string* err);
 Status exec_host(Plan* p, int which, const void* in, void* out, int B, std::string* err);
 Status exec_profile_roundtrip(Plan* p, const void* f0, void* F, void* f0_out, int B, void* stream, float* ms,
                               int* n, std::string* err);

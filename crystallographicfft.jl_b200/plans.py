@@ -276,6 +276,20 @@ class KRFFTPlan:
         check(LIB.cfft_fullgrid_to_subgrid(self._h, ctypes.c_void_p(u.data_ptr()), ctypes.c_void_p(f0.data_ptr()), B, self._stream()))
         return f0
 
+    def subgrid_spectrum(self, f0, out=None):
+        """G0 = FFT_M(f0) of each field on the whole subgrid, (B, M3, M2, M1) complex
+        (cfft_subgrid_spectrum; the F000 of execute_staged!, the Y buffer of execute_m2_q!)."""
+        torch = _torch()
+        self._check_tensor(f0, "r")
+        B = self._batch_of(f0, self.mvol)
+        cdt = torch.complex64 if self.precision == 4 else torch.complex128
+        shape = tuple(reversed(self.M))
+        G0 = torch.empty(((B,) + shape) if B > 1 else shape, dtype=cdt, device=f0.device) if out is None else out
+        self._check_tensor(G0, "c")
+        check(LIB.cfft_subgrid_spectrum(self._h, ctypes.c_void_p(f0.data_ptr()), ctypes.c_void_p(G0.data_ptr()), B,
+                                        self._stream()))
+        return G0
+
     def subgrid_to_fullgrid(self, f0, out=None):
         """subgrid_to_fullgrid! (src/q_fused_krfft.jl:681-688) on device tensors."""
         torch = _torch()

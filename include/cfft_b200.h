@@ -186,6 +186,13 @@ cfft_status cfft_step_diffusion(cfft_plan plan, void* q, const void* w, double d
 cfft_status cfft_fullgrid_to_subgrid(cfft_plan plan, const void* u, void* f0, int batch, void* stream);
 cfft_status cfft_subgrid_to_fullgrid(cfft_plan plan, const void* f0, void* u, int batch, void* stream);
 
+/* Subgrid spectrum G0 = FFT_M(f0) of each field, [batch][M3][M2][M1] complex: the
+ * F000 array returned by execute_staged! / execute_staged_full! (src/staged_krfft.jl:
+ * 562-567,883-889) and the Y buffer of execute_m2_q! (src/q_fused_krfft.jl:553-576); on
+ * the centred path the assembled G0 of fft_channels! + assemble_G0! (src/centering_fold.jl:
+ * 264-296).  Compile-time sized channel grids only (CFFT_UNSUPPORTED otherwise). */
+cfft_status cfft_subgrid_spectrum(cfft_plan plan, const void* f0, void* G0, int batch, void* stream);
+
 /* Allocation-free forward.  No counterpart in the reference: it exists for callers
  * that cannot allocate device memory themselves or through this library -- for
  * example a process whose device memory is owned entirely by another allocator, or
