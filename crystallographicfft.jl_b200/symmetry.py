@@ -205,3 +205,133 @@ def get_k_vector(spec: SpectralIndexing, i: int):
         v = int(spec.idx[i, d])
         out.append(v - n if v >= n - n // 2 else v)
     return out
+
+
+# ---------------------------------------------------------------------------
+# Mirror / glide adaptation data (src/mirror_table.jl:14-285)
+# ---------------------------------------------------------------------------
+
+
+@dataclass
+class MirrorAdaptationEntry:
+    """MirrorAdaptationEntry (src/mirror_table.jl:14-26), computed from the operation table:
+    up to three mutually orthogonal mirror/glide planes, the centring and the reduction
+    factors of a DCT-style mirror adaptation."""
+
+    n_mirrors: int
+    normals: list          # integer plane normals (null vector of R + I)
+    translations: list     # fractional (Fraction) translation of the first op per normal
+    centering: str         # P, I, F, C, A, B, R
+    centering_vecs: list   # fractional centring translations
+    all_axial: bool
+    det_T: int
+    mirror_reduction: int
+    centering_multiplier: int
+    effective_reduction: int
+    has_glide: bool
+
+
+def _mirror_normal(R):
+    """Null vector of R + I (the -1 eigenvector) from cross products of its rows, as a
+    primitive integer vector with the sign the cross product gives."""
+    A = R + np.eye(3, dtype=np.int64)
+    for a, b in ((0, 1), (0, 2), (1, 2)):
+        n = np.cross(A[a], A[b])
+        if n.any():
+            g = int(np.gcd.reduce(np.abs(n)))
+            return n // g
+    return None
+
+
+def _centering_class(vecs):
+    from fractions import Fraction
+
+    half, zero = Fraction(1, 2), Fraction(0)
+    if not vecs:
+        return "P"
+    fset = {(zero, half, half), (half, zero, half), (half, half, zero)}
+    if len(vecs) >= 3 and fset <= set(vecs):
+        return "F"
+    if (half, half, half) in vecs:
+        return "I"
+    for v in vecs:
+        if sorted(v) == [zero, half, half]:
+            return "C" if v[2] == 0 else ("B" if v[1] == 0 else "A")
+    if (Fraction(2, 3), Fraction(1, 3), Fraction(1, 3)) in vecs or (Fraction(1, 3), Fraction(2, 3), Fraction(2, 3)) in vecs:
+        return "R"
+    return "other"
+
+
+def get_mirror_adaptation(sg: int) -> MirrorAdaptationEntry:
+    """get_mirror_adaptation (src/mirror_table.jl:265) from this library's operation table:
+    mirror/glide operations are those with R^2 = I and det R = -1; planes with parallel
+    normals keep the first operation in listing order; the kept set is the orthogonal
+    triple (else pair, else single) preferring axial normals, as the table's generator
+    chooses it."""
+    from fractions import Fraction
+
+    N = (12, 12, 12)  # every ITA translation is a multiple of 1/12
+    ops = get_ops(sg, 3, N)
+    eye = np.eye(3, dtype=np.int64)
+    frac = lambda t: tuple(Fraction(int(v) % 12, 12) for v in t)
+    cvecs = [frac(op.t) for op in ops if np.array_equal(op.Rm, eye) and any(v % 12 for v in op.t)]
+    cent = _centering_class(cvecs)
+    mirrors = []
+    for op in ops:
+        R = op.Rm
+        if not np.array_equal(R @ R, eye) or round(np.linalg.det(R)) != -1:
+            continue
+        n = _mirror_normal(R)
+        if n is None or any(not np.cross(n, m[0]).any() for m in mirrors):
+            continue
+        mirrors.append((n, frac(op.t)))
+    score = lambda m: int(np.sum(m[0] == 0))
+    best, best_score = [], -1
+    for i in range(len(mirrors)):
+        for j in range(i + 1, len(mirrors)):
+            if np.dot(mirrors[i][0], mirrors[j][0]) != 0:
+                continue
+            for k in range(j + 1, len(mirrors)):
+                if np.dot(mirrors[i][0], mirrors[k][0]) == 0 and np.dot(mirrors[j][0], mirrors[k][0]) == 0:
+                    s = score(mirrors[i]) + score(mirrors[j]) + score(mirrors[k])
+                    if s > best_score or len(best) < 3:
+                        best, best_score = [mirrors[i], mirrors[j], mirrors[k]], s
+            if len(best) < 2:
+                best, best_score = [mirrors[i], mirrors[j]], score(mirrors[i]) + score(mirrors[j])
+        if not best:
+            best, best_score = [mirrors[i]], score(mirrors[i])
+    normals = [m[0] for m in best]
+    all_axial = all(int(np.count_nonzero(n)) == 1 for n in normals)
+    # The reference's table carries det_T = 1 in every entry, non-axial normals included,
+    # so the effective reduction is mirror_reduction x centring multiplier throughout.
+    det_T = 1
+    nm = len(best)
+    mult = {"F": 4, "I": 2, "C": 2, "A": 2, "B": 2}.get(cent, 1)  # R keeps 1, as the table has it
+    return MirrorAdaptationEntry(
+        n_mirrors=nm, normals=[[int(v) for v in n] for n in normals], translations=[list(m[1]) for m in best],
+        centering=cent, centering_vecs=[list(v) for v in cvecs], all_axial=all_axial, det_T=int(det_T),
+        mirror_reduction=2 ** nm, centering_multiplier=mult, effective_reduction=(2 ** nm) * mult // int(det_T),
+        has_glide=any(any(x != 0 for x in m[1]) for m in best))
+
+
+class _MirrorTable(dict):
+    """MIRROR_ADAPTATION_TABLE (src/mirror_table.jl:28-259): entries computed on first use."""
+
+    def __missing__(self, sg):
+        e = get_mirror_adaptation(int(sg))
+        self[sg] = e
+        return e
+
+
+MIRROR_ADAPTATION_TABLE = _MirrorTable()
+
+
+def needs_dct_path(sg: int) -> bool:
+    """needs_dct_path (src/mirror_table.jl:267-278): glide planes auto_L cannot use."""
+    e = MIRROR_ADAPTATION_TABLE[sg]
+    return e.has_glide and e.n_mirrors >= 1
+
+
+def needs_basis_change(sg: int) -> bool:
+    """needs_basis_change (src/mirror_table.jl:280-285)."""
+    return not MIRROR_ADAPTATION_TABLE[sg].all_axial

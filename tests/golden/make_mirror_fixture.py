@@ -60,8 +60,13 @@ def main(path):
         trans = parse_vecs(parts[2])
         centering = parts[3].lstrip(":")
         cvecs = parse_vecs(parts[4])
+        # remaining fields: all_axial, det_T, mirror_reduction, centering_multiplier,
+        # effective_reduction, has_glide
         table[sg] = {"n_mirrors": n_mirrors, "normals": normals, "translations": trans,
-                     "centering": centering, "centering_vecs": cvecs}
+                     "centering": centering, "centering_vecs": cvecs,
+                     "all_axial": parts[5] == "true", "det_T": int(parts[6]),
+                     "mirror_reduction": int(parts[7]), "centering_multiplier": int(parts[8]),
+                     "effective_reduction": int(parts[9]), "has_glide": parts[10] == "true"}
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "mirror_table.json")
     with open(out, "w") as f:
         json.dump({str(k): table[k] for k in sorted(table)}, f, indent=0, sort_keys=True)

@@ -153,3 +153,21 @@ def test_plan_errors(cf):
         plan.forward(np.zeros(plan.M))  # host-only plan has no device state
     assert e.value.status == 1
     plan.close()
+
+
+def test_mirror_adaptation_table_matches_reference(cf):
+    # MIRROR_ADAPTATION_TABLE (src/mirror_table.jl) recomputed from the operation table,
+    # field by field against the reference's table (tests/golden/mirror_table.json)
+    table = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "mirror_table.json")))
+    for sg in cf.available_groups(3):
+        want, got = table[str(sg)], cf.get_mirror_adaptation(sg)
+        assert got.n_mirrors == want["n_mirrors"], sg
+        assert got.normals == want["normals"], sg
+        assert [[x % 1 for x in t] for t in got.translations] == \
+            [[Fraction(x) % 1 for x in t] for t in want["translations"]], sg
+        assert got.centering == want["centering"], sg
+        assert sorted(map(tuple, got.centering_vecs)) == sorted(tuple(Fraction(x) for x in v) for v in want["centering_vecs"]), sg
+        for k in ("all_axial", "det_T", "mirror_reduction", "centering_multiplier", "effective_reduction", "has_glide"):
+            assert getattr(got, k) == want[k], (sg, k)
+        assert cf.needs_dct_path(sg) == (want["has_glide"] and want["n_mirrors"] >= 1)
+        assert cf.needs_basis_change(sg) == (not want["all_axial"])
