@@ -129,34 +129,127 @@ const GroupEntry kGroups[] = {
     {72, 3, 'I', 16, "-x,-y,z;-x+1/2,y+1/2,-z;-x,-y,-z"},
     {73, 3, 'I', 16, "-x+1/2,-y,z+1/2;-x,y+1/2,-z+1/2;-x,-y,-z"},
     {74, 3, 'I', 16, "-x,-y+1/2,z;-x,y+1/2,-z;-x,-y,-z"},
-    // ---------------- tetragonal (selection) ----------------
+    // ---------------- tetragonal (all 68; origin choice 2 where there are two) ----------------
     {75, 3, 'P', 4, "-x,-y,z;-y,x,z"},
+    {76, 3, 'P', 4, "-x,-y,z+1/2;-y,x,z+1/4"},
+    {77, 3, 'P', 4, "-x,-y,z;-y,x,z+1/2"},
+    {78, 3, 'P', 4, "-x,-y,z+1/2;-y,x,z+3/4"},
     {79, 3, 'I', 8, "-x,-y,z;-y,x,z"},
+    {80, 3, 'I', 8, "-x+1/2,-y+1/2,z+1/2;-y,x+1/2,z+1/4"},
     {81, 3, 'P', 4, "-x,-y,z;y,-x,-z"},
+    {82, 3, 'I', 8, "-x,-y,z;y,-x,-z"},
     {83, 3, 'P', 8, "-x,-y,z;-y,x,z;-x,-y,-z"},
+    {84, 3, 'P', 8, "-x,-y,z;-y,x,z+1/2;-x,-y,-z"},
+    {85, 3, 'P', 8, "-x+1/2,-y+1/2,z;-y+1/2,x,z;-x,-y,-z"},
+    {86, 3, 'P', 8, "-x+1/2,-y+1/2,z;-y,x+1/2,z+1/2;-x,-y,-z"},
     {87, 3, 'I', 16, "-x,-y,z;-y,x,z;-x,-y,-z"},
+    {88, 3, 'I', 16, "-x+1/2,-y,z+1/2;-y+3/4,x+1/4,z+1/4;-x,-y,-z"},
     {89, 3, 'P', 8, "-x,-y,z;-y,x,z;-x,y,-z"},
+    {90, 3, 'P', 8, "-x,-y,z;-y+1/2,x+1/2,z;-x+1/2,y+1/2,-z"},
+    {91, 3, 'P', 8, "-x,-y,z+1/2;-y,x,z+1/4;-x,y,-z"},
+    {92, 3, 'P', 8, "-x,-y,z+1/2;-y+1/2,x+1/2,z+1/4;-x+1/2,y+1/2,-z+1/4"},
+    {93, 3, 'P', 8, "-x,-y,z;-y,x,z+1/2;-x,y,-z"},
+    {94, 3, 'P', 8, "-x,-y,z;-y+1/2,x+1/2,z+1/2;-x+1/2,y+1/2,-z+1/2"},
+    {95, 3, 'P', 8, "-x,-y,z+1/2;-y,x,z+3/4;-x,y,-z"},
+    {96, 3, 'P', 8, "-x,-y,z+1/2;-y+1/2,x+1/2,z+3/4;-x+1/2,y+1/2,-z+3/4"},
+    {97, 3, 'I', 16, "-x,-y,z;-y,x,z;-x,y,-z"},
+    {98, 3, 'I', 16, "-x+1/2,-y+1/2,z+1/2;-y,x+1/2,z+1/4;-x+1/2,y,-z+3/4"},
     {99, 3, 'P', 8, "-x,-y,z;-y,x,z;x,-y,z"},
+    {100, 3, 'P', 8, "-x,-y,z;-y,x,z;x+1/2,-y+1/2,z"},
+    {101, 3, 'P', 8, "-x,-y,z;-y,x,z+1/2;x,-y,z+1/2"},
+    {102, 3, 'P', 8, "-x,-y,z;-y+1/2,x+1/2,z+1/2;x+1/2,-y+1/2,z+1/2"},
+    {103, 3, 'P', 8, "-x,-y,z;-y,x,z;x,-y,z+1/2"},
+    {104, 3, 'P', 8, "-x,-y,z;-y,x,z;x+1/2,-y+1/2,z+1/2"},
+    {105, 3, 'P', 8, "-x,-y,z;-y,x,z+1/2;x,-y,z"},
+    {106, 3, 'P', 8, "-x,-y,z;-y,x,z+1/2;x+1/2,-y+1/2,z"},
     {107, 3, 'I', 16, "-x,-y,z;-y,x,z;x,-y,z"},
+    {108, 3, 'I', 16, "-x,-y,z;-y,x,z;x,-y,z+1/2"},
+    {109, 3, 'I', 16, "-x+1/2,-y+1/2,z+1/2;-y,x+1/2,z+1/4;x,-y,z"},
+    {110, 3, 'I', 16, "-x+1/2,-y+1/2,z+1/2;-y,x+1/2,z+1/4;x,-y,z+1/2"},
     {111, 3, 'P', 8, "-x,-y,z;y,-x,-z;-x,y,-z"},
+    {112, 3, 'P', 8, "-x,-y,z;y,-x,-z;-x,y,-z+1/2"},
+    {113, 3, 'P', 8, "-x,-y,z;y,-x,-z;-x+1/2,y+1/2,-z"},
+    {114, 3, 'P', 8, "-x,-y,z;y,-x,-z;-x+1/2,y+1/2,-z+1/2"},
     {115, 3, 'P', 8, "-x,-y,z;y,-x,-z;x,-y,z"},
+    {116, 3, 'P', 8, "-x,-y,z;y,-x,-z;x,-y,z+1/2"},
+    {117, 3, 'P', 8, "-x,-y,z;y,-x,-z;x+1/2,-y+1/2,z"},
+    {118, 3, 'P', 8, "-x,-y,z;y,-x,-z;x+1/2,-y+1/2,z+1/2"},
+    {119, 3, 'I', 16, "-x,-y,z;y,-x,-z;x,-y,z"},
+    {120, 3, 'I', 16, "-x,-y,z;y,-x,-z;x,-y,z+1/2"},
+    {121, 3, 'I', 16, "-x,-y,z;y,-x,-z;-x,y,-z"},
+    {122, 3, 'I', 16, "-x,-y,z;y,-x,-z;-x+1/2,y,-z+3/4"},
     {123, 3, 'P', 16, "-x,-y,z;-y,x,z;-x,y,-z;-x,-y,-z"},
+    {124, 3, 'P', 16, "-x,-y,z;-y,x,z;-x,y,-z+1/2;-x,-y,-z"},
+    {125, 3, 'P', 16, "-x+1/2,-y+1/2,z;-y+1/2,x,z;-x+1/2,y,-z;-x,-y,-z"},
+    {126, 3, 'P', 16, "-x+1/2,-y+1/2,z;-y+1/2,x,z;-x+1/2,y,-z+1/2;-x,-y,-z"},
+    {127, 3, 'P', 16, "-x,-y,z;-y,x,z;-x+1/2,y+1/2,-z;-x,-y,-z"},
+    {128, 3, 'P', 16, "-x,-y,z;-y,x,z;-x+1/2,y+1/2,-z+1/2;-x,-y,-z"},
     {129, 3, 'P', 16, "-x+1/2,-y+1/2,z;-y+1/2,x,z;-x,y+1/2,-z;-x,-y,-z"},
+    {130, 3, 'P', 16, "-x+1/2,-y+1/2,z;-y+1/2,x,z;-x,y+1/2,-z+1/2;-x,-y,-z"},
     {131, 3, 'P', 16, "-x,-y,z;-y,x,z+1/2;-x,y,-z;-x,-y,-z"},
+    {132, 3, 'P', 16, "-x,-y,z;-y,x,z+1/2;-x,y,-z+1/2;-x,-y,-z"},
+    {133, 3, 'P', 16, "-x+1/2,-y+1/2,z;-y+1/2,x,z+1/2;-x+1/2,y,-z;-x,-y,-z"},
+    {134, 3, 'P', 16, "-x+1/2,-y+1/2,z;-y+1/2,x,z+1/2;-x+1/2,y,-z+1/2;-x,-y,-z"},
+    {135, 3, 'P', 16, "-x,-y,z;-y,x,z+1/2;-x+1/2,y+1/2,-z;-x,-y,-z"},
     {136, 3, 'P', 16, "-x,-y,z;-y+1/2,x+1/2,z+1/2;-x+1/2,y+1/2,-z+1/2;-x,-y,-z"},
+    {137, 3, 'P', 16, "-x+1/2,-y+1/2,z;-y+1/2,x,z+1/2;-x,y+1/2,-z;-x,-y,-z"},
+    {138, 3, 'P', 16, "-x+1/2,-y+1/2,z;-y+1/2,x,z+1/2;-x,y+1/2,-z+1/2;-x,-y,-z"},
     {139, 3, 'I', 32, "-x,-y,z;-y,x,z;-x,y,-z;-x,-y,-z"},
     {140, 3, 'I', 32, "-x,-y,z;-y,x,z;-x,y,-z+1/2;-x,-y,-z"},
     {141, 3, 'I', 32, "-x+1/2,-y,z+1/2;-y+1/4,x+3/4,z+1/4;-x+1/2,y,-z+1/2;-x,-y,-z"},
-    // ---------------- trigonal / hexagonal (selection, hexagonal axes) ----------
+    {142, 3, 'I', 32, "-x+1/2,-y,z+1/2;-y+1/4,x+3/4,z+1/4;-x+1/2,y,-z;-x,-y,-z"},
+    // ---------------- trigonal / hexagonal (all 52, hexagonal axes; R obverse) ----------
     {143, 3, 'P', 3, "-y,x-y,z"},
+    {144, 3, 'P', 3, "-y,x-y,z+1/3"},
+    {145, 3, 'P', 3, "-y,x-y,z+2/3"},
+    {146, 3, 'R', 9, "-y,x-y,z"},
     {147, 3, 'P', 6, "-y,x-y,z;-x,-y,-z"},
     {148, 3, 'R', 18, "-y,x-y,z;-x,-y,-z"},
+    {149, 3, 'P', 6, "-y,x-y,z;-y,-x,-z"},
+    {150, 3, 'P', 6, "-y,x-y,z;y,x,-z"},
+    {151, 3, 'P', 6, "-y,x-y,z+1/3;-y,-x,-z+2/3"},
+    {152, 3, 'P', 6, "-y,x-y,z+1/3;y,x,-z"},
+    {153, 3, 'P', 6, "-y,x-y,z+2/3;-y,-x,-z+1/3"},
+    {154, 3, 'P', 6, "-y,x-y,z+2/3;y,x,-z"},
+    {155, 3, 'R', 18, "-y,x-y,z;y,x,-z"},
+    {156, 3, 'P', 6, "-y,x-y,z;-y,-x,z"},
+    {157, 3, 'P', 6, "-y,x-y,z;y,x,z"},
+    {158, 3, 'P', 6, "-y,x-y,z;-y,-x,z+1/2"},
+    {159, 3, 'P', 6, "-y,x-y,z;y,x,z+1/2"},
+    {160, 3, 'R', 18, "-y,x-y,z;-y,-x,z"},
+    {161, 3, 'R', 18, "-y,x-y,z;-y,-x,z+1/2"},
     {162, 3, 'P', 12, "-y,x-y,z;-y,-x,-z;-x,-y,-z"},
+    {163, 3, 'P', 12, "-y,x-y,z;-y,-x,-z+1/2;-x,-y,-z"},
     {164, 3, 'P', 12, "-y,x-y,z;y,x,-z;-x,-y,-z"},
+    {165, 3, 'P', 12, "-y,x-y,z;y,x,-z+1/2;-x,-y,-z"},
     {166, 3, 'R', 36, "-y,x-y,z;y,x,-z;-x,-y,-z"},
+    {167, 3, 'R', 36, "-y,x-y,z;y,x,-z+1/2;-x,-y,-z"},
     {168, 3, 'P', 6, "-y,x-y,z;-x,-y,z"},
+    {169, 3, 'P', 6, "-y,x-y,z+1/3;-x,-y,z+1/2"},
+    {170, 3, 'P', 6, "-y,x-y,z+2/3;-x,-y,z+1/2"},
+    {171, 3, 'P', 6, "-y,x-y,z+2/3;-x,-y,z"},
+    {172, 3, 'P', 6, "-y,x-y,z+1/3;-x,-y,z"},
+    {173, 3, 'P', 6, "-y,x-y,z;-x,-y,z+1/2"},
+    {174, 3, 'P', 6, "-y,x-y,z;x,y,-z"},
     {175, 3, 'P', 12, "-y,x-y,z;-x,-y,z;-x,-y,-z"},
+    {176, 3, 'P', 12, "-y,x-y,z;-x,-y,z+1/2;-x,-y,-z"},
+    {177, 3, 'P', 12, "-y,x-y,z;-x,-y,z;y,x,-z"},
+    {178, 3, 'P', 12, "-y,x-y,z+1/3;-x,-y,z+1/2;y,x,-z+1/3"},
+    {179, 3, 'P', 12, "-y,x-y,z+2/3;-x,-y,z+1/2;y,x,-z+2/3"},
+    {180, 3, 'P', 12, "-y,x-y,z+2/3;-x,-y,z;y,x,-z+2/3"},
+    {181, 3, 'P', 12, "-y,x-y,z+1/3;-x,-y,z;y,x,-z+1/3"},
+    {182, 3, 'P', 12, "-y,x-y,z;-x,-y,z+1/2;y,x,-z"},
+    {183, 3, 'P', 12, "-y,x-y,z;-x,-y,z;-y,-x,z"},
+    {184, 3, 'P', 12, "-y,x-y,z;-x,-y,z;-y,-x,z+1/2"},
+    {185, 3, 'P', 12, "-y,x-y,z;-x,-y,z+1/2;-y,-x,z+1/2"},
+    {186, 3, 'P', 12, "-y,x-y,z;-x,-y,z+1/2;-y,-x,z"},
+    {187, 3, 'P', 12, "-y,x-y,z;x,y,-z;-y,-x,z"},
+    {188, 3, 'P', 12, "-y,x-y,z;x,y,-z+1/2;-y,-x,z+1/2"},
+    {189, 3, 'P', 12, "-y,x-y,z;x,y,-z;y,x,-z"},
+    {190, 3, 'P', 12, "-y,x-y,z;x,y,-z+1/2;y,x,-z"},
     {191, 3, 'P', 24, "-y,x-y,z;-x,-y,z;y,x,-z;-x,-y,-z"},
+    {192, 3, 'P', 24, "-y,x-y,z;-x,-y,z;y,x,-z+1/2;-x,-y,-z"},
+    {193, 3, 'P', 24, "-y,x-y,z;-x,-y,z+1/2;y,x,-z+1/2;-x,-y,-z"},
     {194, 3, 'P', 24, "-y,x-y,z;-x,-y,z+1/2;y,x,-z;-x,-y,-z"},
     // ---------------- cubic (all 36) ----------------
     {195, 3, 'P', 12, "-x,-y,z;-x,y,-z;z,x,y"},

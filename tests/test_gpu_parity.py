@@ -250,3 +250,22 @@ def test_linearity_and_roundtrip_large(cf, O, prep):
     back = plan.backward(plan.forward(batch))
     assert torch.max(torch.abs(back - batch)).item() / torch.max(torch.abs(batch)).item() < 1e-5
     plan.close()
+
+
+NEW_GROUPS = [76, 78, 88, 92, 98, 110, 122, 130, 142, 144, 152, 161, 167, 169, 176, 178, 186, 193]
+
+
+@pytest.mark.parametrize("precision", [8, 4])
+@pytest.mark.parametrize("sg", NEW_GROUPS)
+def test_tetragonal_trigonal_hexagonal_groups(cf, O, prep, sg, precision):
+    # forward vs full-grid FFT and backward round trip for groups of every crystal
+    # system beyond the orthorhombic and cubic ones (screw axes 4_1, 3_1, 6_1; R lattices)
+    N = (12, 12, 12) if sg >= 143 else N16
+    p = prep(sg, N)
+    plan = make_plan(cf, p, N, precision)
+    f0 = O.pack_stride(p["u"], plan.L)
+    truth = O.spectrum_on_asu(p["u"], O.calc_spectral_asu(p["oops"], 3, N))
+    F = plan.forward(to_dev(f0, precision))
+    assert rel_err(F.cpu().numpy(), truth) < TOL[precision]
+    assert rel_err(from_dev(plan.backward(F), plan.M), f0) < TOL[precision] * 10
+    plan.close()

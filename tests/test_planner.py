@@ -171,3 +171,22 @@ def test_mirror_adaptation_table_matches_reference(cf):
             assert getattr(got, k) == want[k], (sg, k)
         assert cf.needs_dct_path(sg) == (want["has_glide"] and want["n_mirrors"] >= 1)
         assert cf.needs_basis_change(sg) == (not want["all_axial"])
+
+
+# ITA crystal classes by space-group number range -> point-group order
+_CLASSES = [(1, 1, 1), (2, 2, 2), (3, 9, 2), (10, 15, 4), (16, 46, 4), (47, 74, 8), (75, 82, 4), (83, 122, 8),
+            (123, 142, 16), (143, 146, 3), (147, 161, 6), (162, 167, 12), (168, 174, 6), (175, 190, 12),
+            (191, 194, 24), (195, 199, 12), (200, 220, 24), (221, 230, 48)]
+
+
+def test_all_230_groups_orders(cf):
+    # get_ops (src/symmetry_ops.jl:51-53) covers every space group, as Crystalline.jl does:
+    # distinct rotation parts = the crystal class order, pure translations = the centring
+    assert cf.available_groups(3) == list(range(1, 231))
+    table = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "mirror_table.json")))
+    for sg in range(1, 231):
+        ops = cf.get_ops(sg, 3, (12, 12, 12))
+        pg = next(o for lo, hi, o in _CLASSES if lo <= sg <= hi)
+        assert len({op.R for op in ops}) == pg, sg
+        n_cent = 1 + len(table[str(sg)]["centering_vecs"])
+        assert len(ops) == pg * n_cent, sg
