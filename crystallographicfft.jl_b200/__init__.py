@@ -30,4 +30,9 @@ from .variants import (  # noqa: F401
     plan_krfft_sparse, plan_staged_pm3m, plan_staged_pm3m_full,
 )
 
+from .asu import (  # noqa: F401
+    ASUBlock, ASUPoint, CrystallographicASU, InterleavedOrbit, analyze_interleaved_orbits, calc_asu,
+    compute_full_orbit, pack_asu, pack_asu_interleaved, CFFTPlan, plan_cfft, mul, ldiv,
+)
+
 __version__ = "0.1.0"

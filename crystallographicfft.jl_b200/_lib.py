@@ -75,6 +75,12 @@ def _load():
         "cfft_plan_info": (c_int, [c_void_p, ctypes.POINTER(CFFTInfo)]),
         "cfft_plan_spectral_asu": (c_int, [c_void_p, c_int32_p, c_int32_p]),
         "cfft_plan_q_tables": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_double), c_int32_p]),
+        "cfft_block_plan_create": (c_int, [c_int, c_int32_p, c_int, ctypes.POINTER(c_void_p)]),
+        "cfft_block_plan_destroy": (c_int, [c_void_p]),
+        "cfft_block_forward": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+        "cfft_block_backward": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+        "cfft_calc_asu": (c_int, [c_int, ctypes.POINTER(c_int), c_int, c_int32_p, c_int32_p, c_int,
+                                  ctypes.POINTER(c_int), c_int32_p, c_int32_p, c_int32_p]),
         "cfft_subgrid_spectrum": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
         "cfft_plan_rep_ops": (c_int, [c_void_p, c_int32_p, c_int32_p]),
         "cfft_plan_backward_tables": (c_int, [c_void_p, c_int32_p, c_int32_p, c_int32_p]),

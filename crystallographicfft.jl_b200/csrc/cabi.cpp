@@ -204,6 +204,58 @@ cfft_status cfft_plan_info(cfft_plan plan, cfft_info* info) {
   return CFFT_OK;
 }
 
+cfft_status cfft_block_plan_create(int n_blocks, const int32_t* dims, int precision, cfft_block_plan* plan) {
+  if (!plan) return ret(Status::kInvalid, "null argument");
+  *plan = nullptr;
+  std::string err;
+  cfft::BlockPlan* bp = nullptr;
+  const Status s = cfft::block_plan_create(n_blocks, dims, precision, &bp, &err);
+  if (s != Status::kOk) return ret(s, err);
+  *plan = reinterpret_cast<cfft_block_plan>(bp);
+  return CFFT_OK;
+}
+
+cfft_status cfft_block_plan_destroy(cfft_block_plan plan) {
+  cfft::block_plan_destroy(reinterpret_cast<cfft::BlockPlan*>(plan));
+  return CFFT_OK;
+}
+
+cfft_status cfft_block_forward(cfft_block_plan plan, const void* in, void* out, void* stream) {
+  std::string err;
+  return ret(cfft::block_execute(reinterpret_cast<cfft::BlockPlan*>(plan), in, out, false, stream, &err), err);
+}
+
+cfft_status cfft_block_backward(cfft_block_plan plan, const void* in, void* out, void* stream) {
+  std::string err;
+  return ret(cfft::block_execute(reinterpret_cast<cfft::BlockPlan*>(plan), in, out, true, stream, &err), err);
+}
+
+cfft_status cfft_calc_asu(int dim, const int* N, int n_ops, const int32_t* R, const int32_t* t, int cap,
+                          int* n_points, int32_t* idx, int32_t* depth, int32_t* mult) {
+  if (!n_points) return ret(Status::kInvalid, "null argument");
+  std::string err;
+  int n[3];
+  std::vector<cfft::SymOp> ops;
+  if (!read_N(dim, N, n, &err) || !read_ops(dim, n_ops, R, t, &ops, &err)) return ret(Status::kInvalid, err);
+  for (auto& op : ops)
+    for (int d = dim; d < 3; ++d) {
+      op.t[d] = 0;
+      for (int j = 0; j < 3; ++j) op.R[d][j] = op.R[j][d] = (d == j);
+    }
+  const auto pts = cfft::calc_asu(ops, n, dim);
+  *n_points = static_cast<int>(pts.size());
+  if (!idx && !depth && !mult) return CFFT_OK;
+  if (cap < *n_points) return ret(Status::kInvalid, "capacity too small for the ASU");
+  for (size_t k = 0; k < pts.size(); ++k) {
+    for (int d = 0; d < 3; ++d) {
+      if (idx) idx[3 * k + d] = pts[k].idx[d];
+      if (depth) depth[3 * k + d] = pts[k].depth[d];
+    }
+    if (mult) mult[k] = pts[k].mult;
+  }
+  return CFFT_OK;
+}
+
 cfft_status cfft_plan_q_tables(cfft_plan plan, double* Q, int32_t* gather) {
   if (!plan) return ret(Status::kInvalid, "null plan");
   const auto* p = reinterpret_cast<cfft::Plan*>(plan);

@@ -95,6 +95,12 @@ struct PlanTables {
 Status build_tables(const std::vector<SymOp>& shifted_ops, const int* N, int dim, bool want_centered,
                     PlanTables* T, std::string* err, bool full_grid = false);
 void compute_kernel(const PlanTables& T, const double* lattice, double ds, std::vector<double>* K);
+struct AsuPoint {
+  int idx[3];    // grid coordinates (0-based)
+  int depth[3];  // even-split count per dimension
+  int mult;      // orbit size at the leaf
+};
+std::vector<AsuPoint> calc_asu(const std::vector<SymOp>& ops, const int* N, int dim);
 Status build_q_tables(const PlanTables& T, const double* lattice, double ds, std::vector<double>* Q,
                       std::vector<int32_t>* gather, std::string* err);
 

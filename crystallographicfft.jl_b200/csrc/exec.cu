@@ -352,6 +352,63 @@ __global__ void k_unpack_g0(const DevGeom* __restrict__ g, const typename Cx<T>:
   if (2 * slot + 1 < nfields) G0[(2L * slot + 1) * mvol + q] = gb;
 }
 
+// Per-block DFT of the legacy block plan (plan_cfft + mul!/ldiv!, src/cfft_plan.jl,
+// src/execution.jl): blocks are concatenated, each column-major (x fastest) with
+// dims[b] = (n1, n2, n3); one pass transforms one axis of every block, one thread per
+// output element, y(k) = sum_j x(j) e^{-+2 pi i j k / n} along the axis (the angle
+// index j k mod n is exact; the twiddle is sincospi of it).  `scale` multiplies the
+// result (1/(n1 n2 n3) in the last inverse pass).
+template <typename T>
+__global__ void k_block_dft_axis(const int32_t* __restrict__ dims, const long long* __restrict__ off, int n_blocks,
+                                 const typename Cx<T>::type* __restrict__ src, typename Cx<T>::type* __restrict__ dst,
+                                 int axis, T sign, T scale) {
+  using C = typename Cx<T>::type;
+  const long long total = off[n_blocks];
+  for (long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    int lo = 0, hi = n_blocks - 1;  // block of element e: off[b] <= e < off[b + 1]
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) / 2;
+      if (off[mid] <= e) lo = mid; else hi = mid - 1;
+    }
+    const int b = lo;
+    const int n0 = dims[3 * b], n1 = dims[3 * b + 1], n2 = dims[3 * b + 2];
+    const long long l = e - off[b];
+    const int c[3] = {static_cast<int>(l % n0), static_cast<int>((l / n0) % n1), static_cast<int>(l / (static_cast<long long>(n0) * n1))};
+    const int n = axis == 0 ? n0 : axis == 1 ? n1 : n2;
+    const long long stride = axis == 0 ? 1 : axis == 1 ? n0 : static_cast<long long>(n0) * n1;
+    const long long base = off[b] + l - static_cast<long long>(c[axis]) * stride;
+    const int k = c[axis];
+    C acc = mk<C>(static_cast<T>(0), static_cast<T>(0));
+    for (int j = 0; j < n; ++j) {
+      const int m = static_cast<int>((static_cast<long long>(j) * k) % n);
+      T sv, cv;
+      if constexpr (sizeof(T) == 8) sincospi(2.0 * m / n, &sv, &cv);
+      else sincospif(2.0f * m / n, &sv, &cv);
+      const C x = src[base + j * stride];
+      acc = cadd(acc, cmul(x, mk<C>(cv, sign * sv)));
+    }
+    dst[e] = cscale(acc, scale);
+  }
+}
+
+// Inverse normalisation of the block plan: each block's elements times 1/(n1 n2 n3).
+template <typename T>
+__global__ void k_block_scale(const int32_t* __restrict__ dims, const long long* __restrict__ off, int n_blocks,
+                              typename Cx<T>::type* __restrict__ x) {
+  const long long total = off[n_blocks];
+  for (long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
+       e += static_cast<long long>(gridDim.x) * blockDim.x) {
+    int lo = 0, hi = n_blocks - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) / 2;
+      if (off[mid] <= e) lo = mid; else hi = mid - 1;
+    }
+    const T inv = static_cast<T>(1.0 / (static_cast<double>(dims[3 * lo]) * dims[3 * lo + 1] * dims[3 * lo + 2]));
+    x[e] = cscale(x[e], inv);
+  }
+}
+
 template <typename T>
 __global__ void k_full_to_sub(const T* __restrict__ u, T* __restrict__ f0, int N1, int N2, int L1, int L2, int L3,
                               int M1, int M2, size_t mvol, size_t nvol, int B) {
@@ -1094,6 +1151,78 @@ Status exec_full_to_sub(Plan* p, const void* u, void* f0, int B, void* stream, s
                                               T.L[0], T.L[1], T.L[2], T.M[0], T.M[1], mvol, nvol, B);
   ++g_launches;
   CFFT_CUDA(cudaGetLastError(), "fullgrid_to_subgrid launch");
+  return Status::kOk;
+}
+
+// Legacy block plan: device block descriptors and a work buffer of the blocks' size.
+Status block_plan_create(int n_blocks, const int32_t* dims, int precision, BlockPlan** out, std::string* err) {
+  if (n_blocks < 1 || !dims || !out || (precision != 4 && precision != 8)) { *err = "invalid argument"; return Status::kInvalid; }
+  std::vector<long long> off(n_blocks + 1, 0);
+  for (int b = 0; b < n_blocks; ++b) {
+    for (int d = 0; d < 3; ++d)
+      if (dims[3 * b + d] < 1) { *err = "block dimensions must be positive"; return Status::kInvalid; }
+    off[b + 1] = off[b] + static_cast<long long>(dims[3 * b]) * dims[3 * b + 1] * dims[3 * b + 2];
+  }
+  auto* bp = new (std::nothrow) BlockPlan();
+  if (!bp) { *err = "host allocation failed"; return Status::kAlloc; }
+  bp->n_blocks = n_blocks;
+  bp->total = off[n_blocks];
+  bp->precision = precision;
+  cudaError_t e = cudaMalloc(&bp->d_dims, sizeof(int32_t) * 3 * n_blocks);
+  if (e == cudaSuccess) e = cudaMalloc(&bp->d_off, sizeof(long long) * (n_blocks + 1));
+  if (e == cudaSuccess) e = cudaMalloc(&bp->d_work, static_cast<size_t>(bp->total) * 2 * precision);
+  if (e == cudaSuccess) e = cudaMemcpy(bp->d_dims, dims, sizeof(int32_t) * 3 * n_blocks, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(bp->d_off, off.data(), sizeof(long long) * (n_blocks + 1), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    *err = cuda_msg(e, "block plan");
+    block_plan_destroy(bp);
+    return Status::kCuda;
+  }
+  *out = bp;
+  return Status::kOk;
+}
+
+void block_plan_destroy(BlockPlan* bp) {
+  if (!bp) return;
+  for (void* q : {bp->d_dims, bp->d_off, bp->d_work})
+    if (q) cudaFree(q);
+  delete bp;
+}
+
+// mul! (forward, unnormalised) / ldiv! (inverse, 1/n) over every block: x -> out -> work -> out.
+Status block_execute(BlockPlan* bp, const void* in, void* out, bool inverse, void* stream, std::string* err) {
+  if (!bp || !in || !out) { *err = "null argument"; return Status::kInvalid; }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int grid = static_cast<int>(std::min<long long>((bp->total + 255) / 256, 148 * 16));
+  const int32_t* dims = static_cast<const int32_t*>(bp->d_dims);
+  const long long* off = static_cast<const long long*>(bp->d_off);
+  if (bp->precision == 8) {
+    const double sg = inverse ? 1.0 : -1.0;
+    const double2* src[3] = {static_cast<const double2*>(in), static_cast<const double2*>(out), static_cast<const double2*>(bp->d_work)};
+    double2* dst[3] = {static_cast<double2*>(out), static_cast<double2*>(bp->d_work), static_cast<double2*>(out)};
+    for (int a = 0; a < 3; ++a) {
+      // the inverse's 1/n is applied per axis (1/n_axis of each block) through a second pass below
+      k_block_dft_axis<double><<<grid, 256, 0, s>>>(dims, off, bp->n_blocks, src[a], dst[a], a, sg, 1.0);
+      ++g_launches;
+    }
+    if (inverse) {
+      k_block_scale<double><<<grid, 256, 0, s>>>(dims, off, bp->n_blocks, static_cast<double2*>(out));
+      ++g_launches;
+    }
+  } else {
+    const float sg = inverse ? 1.f : -1.f;
+    const float2* src[3] = {static_cast<const float2*>(in), static_cast<const float2*>(out), static_cast<const float2*>(bp->d_work)};
+    float2* dst[3] = {static_cast<float2*>(out), static_cast<float2*>(bp->d_work), static_cast<float2*>(out)};
+    for (int a = 0; a < 3; ++a) {
+      k_block_dft_axis<float><<<grid, 256, 0, s>>>(dims, off, bp->n_blocks, src[a], dst[a], a, sg, 1.f);
+      ++g_launches;
+    }
+    if (inverse) {
+      k_block_scale<float><<<grid, 256, 0, s>>>(dims, off, bp->n_blocks, static_cast<float2*>(out));
+      ++g_launches;
+    }
+  }
+  CFFT_CUDA(cudaGetLastError(), "block transform launch");
   return Status::kOk;
 }
 

@@ -81,6 +81,18 @@ Status exec_step_diffusion(Plan* p, void* q, const void* w, double dt, int n_ste
                            std::string* err);
 Status exec_full_to_sub(Plan* p, const void* u, void* f0, int B, void* stream, std::string* err);
 Status exec_sub_to_full(Plan* p, const void* f0, void* u, int B, void* stream, std::string* err);
+// Legacy block plan (plan_cfft): per-block DFTs of the packed real-space ASU.
+struct BlockPlan {
+  int n_blocks = 0;
+  long long total = 0;  // elements over all blocks
+  int precision = 8;
+  void* d_dims = nullptr;
+  void* d_off = nullptr;
+  void* d_work = nullptr;
+};
+Status block_plan_create(int n_blocks, const int32_t* dims, int precision, BlockPlan** out, std::string* err);
+void block_plan_destroy(BlockPlan* bp);
+Status block_execute(BlockPlan* bp, const void* in, void* out, bool inverse, void* stream, std::string* err);
 Status exec_subgrid_spectrum(Plan* p, const void* f0, void* G0, int B, void* stream, std::string* err);
 Status exec_host(Plan* p, int which, const void* in, void* out, int B, std::string* err);
 Status exec_profile_roundtrip(Plan* p, const void* f0, void* F, void* f0_out, int B, void* stream, float* ms,

@@ -4,6 +4,7 @@
 // integer table (spectral-ASU points, multiplicities, L, M, fold offsets) is
 // identical to the reference's.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <complex>
 #include <numeric>
@@ -658,6 +659,141 @@ Status build_q_tables(const PlanTables& T, const double* lattice, double ds, std
     }
   }
   return Status::kOk;
+}
+
+// Real-space asymmetric unit by recursive parity splitting (calc_asu(N, ops),
+// src/asu.jl:216-324).  A state is a sub-problem on curr_N points with operations
+// acting on it, mapped to the full grid by x = scale .* p + offset.  Each active
+// dimension whose parity every operation preserves splits into its even and odd
+// halves (S = 2); the operations of a half are R' = S^-1 R S, t' = S^-1 (R p + t - p)
+// and the half is dropped when they are not integral.  Odd halves and dimensions that
+// cannot split become general-position leaves; a leaf lists one point per orbit of
+// its operations (the lexicographically smallest member) with the orbit size.  The
+// result is sorted by grid index.
+std::vector<AsuPoint> calc_asu(const std::vector<SymOp>& ops_in, const int* N_in, int dim) {
+  struct State {
+    int n[3], scale[3], offset[3], depth[3];
+    bool gp[3];
+    std::vector<SymOp> ops;
+  };
+  std::vector<AsuPoint> out;
+  std::vector<State> stack;
+  State s0{};
+  for (int d = 0; d < 3; ++d) {
+    s0.n[d] = d < dim ? N_in[d] : 1;
+    s0.scale[d] = 1;
+    s0.offset[d] = 0;
+    s0.depth[d] = 0;
+    s0.gp[d] = d >= dim;  // unused dimensions never split
+  }
+  s0.ops = ops_in;
+  stack.push_back(std::move(s0));
+  auto apply = [&](const SymOp& op, const int* x, const int* n, int* y) {
+    for (int i = 0; i < dim; ++i) {
+      long v = op.t[i];
+      for (int j = 0; j < dim; ++j) v += static_cast<long>(op.R[i][j]) * x[j];
+      y[i] = static_cast<int>(floor_mod(v, n[i]));
+    }
+  };
+  while (!stack.empty()) {
+    State st = std::move(stack.back());
+    stack.pop_back();
+    bool empty = false, all_gp = true, all_small = true;
+    for (int d = 0; d < dim; ++d) {
+      if (st.n[d] == 0) empty = true;
+      if (!st.gp[d]) all_gp = false;
+      if (st.n[d] > 1) all_small = false;
+    }
+    if (empty) continue;
+    if (all_gp || all_small) {
+      const long total = static_cast<long>(st.n[0]) * st.n[1] * st.n[2];
+      std::vector<char> seen(total, 0);
+      std::vector<long> orbit;
+      for (long lin = 0; lin < total; ++lin) {
+        if (seen[lin]) continue;
+        orbit.assign(1, lin);
+        seen[lin] = 1;
+        for (size_t w = 0; w < orbit.size(); ++w) {
+          long r = orbit[w];
+          int x[3] = {static_cast<int>(r % st.n[0]), static_cast<int>((r / st.n[0]) % st.n[1]),
+                      static_cast<int>(r / (static_cast<long>(st.n[0]) * st.n[1]))};
+          for (const auto& op : st.ops) {
+            int y[3] = {0, 0, 0};
+            apply(op, x, st.n, y);
+            const long li = y[0] + static_cast<long>(st.n[0]) * (y[1] + static_cast<long>(st.n[1]) * y[2]);
+            if (!seen[li]) { seen[li] = 1; orbit.push_back(li); }
+          }
+        }
+        // lexicographically smallest member (first coordinate most significant)
+        std::array<int, 3> best{INT32_MAX, INT32_MAX, INT32_MAX};
+        for (long r : orbit) {
+          std::array<int, 3> x{static_cast<int>(r % st.n[0]), static_cast<int>((r / st.n[0]) % st.n[1]),
+                               static_cast<int>(r / (static_cast<long>(st.n[0]) * st.n[1]))};
+          if (x < best) best = x;
+        }
+        AsuPoint pt{};
+        for (int d = 0; d < 3; ++d) {
+          pt.idx[d] = st.scale[d] * best[d] + st.offset[d];
+          pt.depth[d] = st.depth[d];
+        }
+        pt.mult = static_cast<int>(orbit.size());
+        out.push_back(pt);
+      }
+      continue;
+    }
+    bool egp[3] = {st.gp[0], st.gp[1], st.gp[2]};
+    for (int d = 0; d < dim; ++d) {
+      if (st.gp[d]) continue;
+      int pe[3] = {0, 0, 0}, po[3] = {0, 0, 0}, y[3];
+      po[d] = 1;
+      for (const auto& op : st.ops) {
+        apply(op, pe, st.n, y);
+        if (y[d] % 2 != 0) { egp[d] = true; break; }
+        apply(op, po, st.n, y);
+        if (y[d] % 2 != 1) { egp[d] = true; break; }
+      }
+    }
+    int hi[3];
+    for (int d = 0; d < 3; ++d) hi[d] = (egp[d] || st.n[d] <= 1) ? 0 : 1;
+    for (int p2 = 0; p2 <= hi[2]; ++p2)
+      for (int p1 = 0; p1 <= hi[1]; ++p1)
+        for (int p0 = 0; p0 <= hi[0]; ++p0) {
+          const int par[3] = {p0, p1, p2};
+          int S[3];
+          for (int d = 0; d < 3; ++d) S[d] = egp[d] ? 1 : 2;
+          State nx{};
+          bool valid = true;
+          for (const auto& op : st.ops) {
+            SymOp q{};
+            for (int i = 0; i < 3 && valid; ++i) {
+              long t = op.t[i] - par[i];
+              for (int j = 0; j < 3; ++j) {
+                t += static_cast<long>(op.R[i][j]) * par[j];
+                const long rv = static_cast<long>(op.R[i][j]) * S[j];
+                if (rv % S[i] != 0) valid = false;
+                q.R[i][j] = static_cast<int>(rv / S[i]);
+              }
+              if (t % S[i] != 0) valid = false;
+              q.t[i] = static_cast<int>(t / S[i]);
+            }
+            if (!valid) break;
+            nx.ops.push_back(q);
+          }
+          if (!valid) continue;
+          for (int d = 0; d < 3; ++d) {
+            nx.n[d] = egp[d] ? st.n[d] : st.n[d] / 2;
+            nx.gp[d] = egp[d] || par[d] == 1;
+            nx.depth[d] = egp[d] ? st.depth[d] : st.depth[d] + (par[d] == 0 ? 1 : 0);
+            nx.scale[d] = st.scale[d] * S[d];
+            nx.offset[d] = st.scale[d] * par[d] + st.offset[d];
+          }
+          stack.push_back(std::move(nx));
+        }
+  }
+  std::sort(out.begin(), out.end(), [](const AsuPoint& a, const AsuPoint& b) {
+    return std::lexicographical_compare(a.idx, a.idx + 3, b.idx, b.idx + 3);
+  });
+  return out;
 }
 
 }  // namespace cfft

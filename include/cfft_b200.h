@@ -101,6 +101,28 @@ typedef struct cfft_info {
 
 /* ---------------- plan-time functions (host only, no GPU needed) ---------------- */
 
+/* ---------------- legacy block path (plan_cfft, mul! / ldiv!) ----------------
+ * plan_cfft (src/cfft_plan.jl:15-41) packs the real-space ASU (cfft_calc_asu + the
+ * host-side pack_asu) into rectangular blocks and plans one FFT per block shape;
+ * mul! / ldiv! (src/execution.jl:16-60, src/cfft_plan.jl:43-66) transform every block.
+ * A block plan holds n_blocks block shapes dims[3 b + {0, 1, 2}] (unused dimensions 1);
+ * `in` / `out` are device arrays of the blocks' complex data concatenated in plan order,
+ * each block column-major.  Forward is unnormalised, backward divides by the block size,
+ * as FFTW's plan * x and plan \ x.  `in` and `out` must not overlap. */
+typedef struct cfft_block_plan_s* cfft_block_plan;
+cfft_status cfft_block_plan_create(int n_blocks, const int32_t* dims, int precision, cfft_block_plan* plan);
+cfft_status cfft_block_plan_destroy(cfft_block_plan plan);
+cfft_status cfft_block_forward(cfft_block_plan plan, const void* in, void* out, void* stream);
+cfft_status cfft_block_backward(cfft_block_plan plan, const void* in, void* out, void* stream);
+
+/* calc_asu(N, ops) (src/asu.jl:216-324): real-space asymmetric unit by recursive parity
+ * splitting of the grid under shifted operations.  n_points points sorted by grid index,
+ * each with idx[3] (0-based grid coordinates), depth[3] (even splits per dimension) and
+ * mult (orbit size within its leaf).  Call with idx = depth = mult = NULL to query
+ * n_points. */
+cfft_status cfft_calc_asu(int dim, const int* N, int n_ops, const int32_t* R, const int32_t* t, int cap,
+                          int* n_points, int32_t* idx, int32_t* depth, int32_t* mult);
+
 /* _build_q_matrices! (src/q_fused_krfft.jl:182-413) tables of an M2Q / M7 plan (also
  * host plans): Q first row Q[(b * Mvol + q) * 2 + {re, im}] and gather[b * Mvol + q]
  * (0-based column-major subgrid index of R_b^T q mod M), b < n_rep, q < M1 M2 M3.

@@ -922,3 +922,73 @@ def spectrum_on_asu(u, spec):
     F = np.fft.fftn(u)
     idx = spec.idx
     return F[tuple(idx[:, d] for d in range(idx.shape[1]))]
+
+
+# ---------------------------------------------------------------------------
+# Real-space ASU (src/asu.jl:216-324), pure Python (small grids only)
+# ---------------------------------------------------------------------------
+
+
+def calc_asu_points(N, ops):
+    """calc_asu(N, ops) (src/asu.jl:216-324): recursive even/odd splitting of the grid;
+    returns sorted [(idx tuple, depth tuple, orbit size)]."""
+    D = len(N)
+    out = []
+    stack = [(tuple(N), [(np.array(op.Rm), np.array(op.tv)) for op in ops], (1,) * D, (0,) * D, (0,) * D,
+              (False,) * D)]
+
+    def apply(R, t, x, n):
+        return tuple(int(v) for v in np.mod(R @ np.asarray(x) + t, np.asarray(n)))
+
+    while stack:
+        n, cops, scale, offset, depth, gp = stack.pop()
+        if any(v == 0 for v in n):
+            continue
+        if all(gp) or all(v <= 1 for v in n):
+            seen = set()
+            for p in itertools.product(*[range(v) for v in reversed(n)]):
+                p = tuple(reversed(p))  # first axis fastest
+                if p in seen:
+                    continue
+                orbit, work = {p}, [p]
+                while work:
+                    c = work.pop()
+                    for R, t in cops:
+                        y = apply(R, t, c, n)
+                        if y not in orbit:
+                            orbit.add(y)
+                            work.append(y)
+                rep = min(orbit)
+                out.append((tuple(scale[d] * rep[d] + offset[d] for d in range(D)), depth, len(orbit)))
+                seen |= orbit
+            continue
+        egp = list(gp)
+        for d in range(D):
+            if gp[d]:
+                continue
+            e, o = [0] * D, [0] * D
+            o[d] = 1
+            for R, t in cops:
+                if apply(R, t, e, n)[d] % 2 != 0 or apply(R, t, o, n)[d] % 2 != 1:
+                    egp[d] = True
+                    break
+        ranges = [range(1) if (egp[d] or n[d] <= 1) else range(2) for d in range(D)]
+        for par in itertools.product(*reversed(ranges)):
+            par = tuple(reversed(par))
+            S = np.array([1 if egp[d] else 2 for d in range(D)])
+            new, ok = [], True
+            for R, t in cops:
+                Rv = R * S[None, :]
+                tv = R @ np.asarray(par) + t - np.asarray(par)
+                if np.any(Rv % S[:, None] != 0) or np.any(tv % S != 0):
+                    ok = False
+                    break
+                new.append((Rv // S[:, None], tv // S))
+            if not ok:
+                continue
+            stack.append((tuple(n[d] if egp[d] else n[d] // 2 for d in range(D)), new,
+                          tuple(scale[d] * S[d] for d in range(D)),
+                          tuple(scale[d] * par[d] + offset[d] for d in range(D)),
+                          tuple(depth[d] if egp[d] else depth[d] + (par[d] == 0) for d in range(D)),
+                          tuple(egp[d] or par[d] == 1 for d in range(D))))
+    return sorted(out)

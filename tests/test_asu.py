@@ -1,0 +1,69 @@
+"""Real-space ASU, block packing and interleaved orbits (module ASU, src/asu.jl,
+src/pack_asu.jl) against the oracle and the reference's own checks (test/runtests.jl:
+40-78, test/test_asu.jl, test/test_packing.jl, test/test_interleaved_orbits.jl)."""
+import numpy as np
+import pytest
+
+from conftest import to_oracle_ops
+
+
+@pytest.mark.parametrize("sg,dim,N", [(6, 2, (8, 8)), (47, 3, (8, 8, 8)), (221, 3, (8, 8, 8)), (229, 3, (8, 8, 8)),
+                                      (225, 3, (8, 8, 8)), (230, 3, (8, 8, 8)), (10, 3, (8, 8, 8)),
+                                      (63, 3, (8, 8, 8)), (75, 3, (8, 8, 8)), (194, 3, (6, 6, 6)), (1, 3, (4, 4, 4))])
+def test_calc_asu_matches_oracle_and_covers_grid(cf, O, sg, dim, N):
+    pts, shift = cf.calc_asu(sg, dim, N)
+    _, ops_s = cf.find_optimal_shift(cf.get_ops(sg, dim, N), N)
+    want = O.calc_asu_points(N, to_oracle_ops(O, ops_s))
+    assert [(tuple(p.idx), tuple(p.depth), p.multiplicity) for p in pts] == want
+    cover = set()
+    for p in pts:  # disjoint orbits covering the whole grid (test/test_asu.jl:40-66)
+        orb = cf.compute_full_orbit(p.idx, ops_s, N)
+        assert not (cover & orb)
+        cover |= orb
+    assert len(cover) == int(np.prod(N))
+
+
+def test_reference_asu_sizes(cf):
+    # test/runtests.jl:51-66
+    assert len(cf.calc_asu(6, 2, (8, 8))[0]) == 16
+    pts, shift = cf.calc_asu(47, 3, (8, 8, 8))
+    assert len(pts) == 64
+    assert np.allclose(cf.calc_asu(6, 2, (8, 8))[1], (0.5 / 8, 0.5 / 8))
+
+
+@pytest.mark.parametrize("sg,dim,N", [(6, 2, (8, 8)), (7, 2, (8, 8)), (47, 3, (8, 8, 8)), (229, 3, (16, 16, 16))])
+def test_pack_asu_covers_points(cf, sg, dim, N):
+    # test/runtests.jl:69-78, test/test_packing.jl: every ASU point in exactly one block
+    pts, shift = cf.calc_asu(sg, dim, N)
+    c = cf.pack_asu(pts, N, shift=shift)
+    seen = []
+    for eff, blocks in c.dim_blocks.items():
+        for b in blocks:
+            assert sum(len(r) > 1 for r in b.range) == eff
+            seen += [pt for pt in __import__("itertools").product(*b.range)]
+    assert sorted(seen) == sorted(tuple(p.idx) for p in pts)
+
+
+def test_interleaved_orbits_reference_cases(cf):
+    # test/test_interleaved_orbits.jl
+    N = (16, 16, 16)
+    o = cf.analyze_interleaved_orbits(N, [cf.SymOp((1, 0, 0, 0, 1, 0, 0, 0, 1), (0, 0, 0))], L=(2, 2, 2))
+    assert len(o) == 8 and all(x.multiplicity == 1 for x in o)
+    o = cf.analyze_interleaved_orbits(N, cf.get_ops(75, 3, N), L=(2, 2, 2))
+    assert len(o) == 6 and sum(x.multiplicity for x in o) == 8
+    assert len([x for x in o if x.multiplicity == 2]) == 2
+    o = cf.analyze_interleaved_orbits(N, cf.get_ops(47, 3, N), L=(2, 2, 2))
+    assert len(o) == 8 and all(x.multiplicity == 1 for x in o)
+    assert len(cf.analyze_interleaved_orbits(N, cf.get_ops(99, 3, N), L=(2, 2, 2))) <= 6
+
+
+def test_pack_asu_interleaved_gamma0(cf, O):
+    N = (16, 16, 16)
+    ops = cf.get_ops(229, 3, N)
+    _, ops_s = cf.find_optimal_shift(ops, N)
+    u = O.make_symmetric(to_oracle_ops(O, ops_s), N, seed=4)
+    c = cf.pack_asu_interleaved(u, N, ops_s, L=(2, 2, 2))
+    (b,) = c.dim_blocks[3]
+    assert np.array_equal(b.data, u[::2, ::2, ::2]) and b.orbit is None
+    c = cf.pack_asu_interleaved(u, N, ops_s, L=(2, 2, 2), asu_only=False)
+    assert sum(len(b.orbit.members) for b in c.dim_blocks[3]) == 8
