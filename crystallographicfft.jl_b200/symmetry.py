@@ -196,8 +196,9 @@ def calc_spectral_asu(ops_or_sg, dim: int, N) -> SpectralIndexing:
 
 
 def get_k_vector(spec: SpectralIndexing, i: int):
-    """get_k_vector (src/spectral_indexing.jl:195-238) for the 0-based point i:
-    frequencies wrapped to (-N/2, N/2]."""
+    """get_k_vector (src/spectral_indexing.jl:195-238) for the 0-based point i: frequency
+    v >= N - N div 2 maps to v - N, i.e. [-N/2, N/2) for even N (the reference's code maps
+    N/2 to -N/2, whatever its docstring says)."""
     if i < 0 or i >= spec.n_spec:
         raise IndexError(f"Index {i} out of bounds for SpectralIndexing with {spec.n_spec} points")
     out = []

@@ -101,3 +101,39 @@ def test_q_step_diffusion_vs_oracle(cf, O, prep):
         ref = O.step_diffusion(lambda x: O.execute_m2_q(oplan, x), ref, w, 0.02)
     assert np.max(np.abs(from_dev(q, plan.M) - ref)) < 1e-12
     plan.close()
+
+
+def test_matrix_solver_step_on_device(cf):
+    # test/test_diffusion_solver.jl:42-50: the step runs and changes u; the device
+    # operator equals real(M Q M^+ u) on the host
+    solver = cf.plan_diffusion((8, 8), np.eye(2), 6, 2, 0.1)
+    rng = np.random.default_rng(1)
+    u = rng.random(len(solver.real_asu))
+    want = np.real(solver.M @ (solver.Q.diag * (solver.M_inv @ u)))
+    got = cf.apply_diffusion_operator(solver, u.copy())
+    assert np.max(np.abs(got - want)) < 1e-12
+    w = rng.random(len(solver.real_asu))
+    v = u.copy()
+    cf.step_diffusion(solver, v, w, 1.0)
+    assert not np.array_equal(v, u)
+    t = torch.tensor(np.stack([u, 2 * u]), device="cuda:0")
+    solver.apply_diffusion_operator(t)
+    assert np.max(np.abs(t.cpu().numpy() - np.stack([want, 2 * want]))) < 1e-12
+
+
+@pytest.mark.parametrize("sg,n", [(47, 16), (47, 32), (123, 16)])
+def test_qfused_solver_vs_fullgrid(cf, O, sg, n):
+    # test/test_diffusion_solver.jl:52-135: f0 after the operator vs full-grid FFT -> K -> IFFT
+    from conftest import to_oracle_ops
+
+    N = (n, n, n)
+    solver = cf.plan_diffusion(N, LAT, sg, 3, 0.1, method=":qfused")
+    plan = solver.plan
+    _, ops_s = cf.find_optimal_shift(cf.get_ops(sg, 3, N), N)
+    u = O.make_symmetric(to_oracle_ops(O, ops_s), N, seed=2)
+    f0 = O.pack_stride(u, plan.L)
+    q = to_dev(f0, 8)
+    cf.apply_diffusion_operator(solver, q)
+    want = O.fullgrid_reference(u, N, 0.1, LAT, plan.L)
+    assert np.max(np.abs(from_dev(q, plan.M) - want)) < 1e-10
+    plan.close()
