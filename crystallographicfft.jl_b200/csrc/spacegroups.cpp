@@ -53,6 +53,11 @@ const GroupEntry kGroups[] = {
     {10, 2, 'p', 4, "-x,-y;-y,x"},
     {11, 2, 'p', 8, "-x,-y;-y,x;-x,y"},
     {12, 2, 'p', 8, "-x,-y;-y,x;-x+1/2,y+1/2"},
+    {13, 2, 'p', 3, "-y,x-y"},
+    {14, 2, 'p', 6, "-y,x-y;-y,-x"},
+    {15, 2, 'p', 6, "-y,x-y;y,x"},
+    {16, 2, 'p', 6, "-y,x-y;-x,-y"},
+    {17, 2, 'p', 12, "-y,x-y;-x,-y;-y,-x"},
     // ---------------- triclinic / monoclinic ----------------
     {1, 3, 'P', 1, ""},
     {2, 3, 'P', 2, "-x,-y,-z"},

@@ -190,3 +190,14 @@ def test_all_230_groups_orders(cf):
         assert len({op.R for op in ops}) == pg, sg
         n_cent = 1 + len(table[str(sg)]["centering_vecs"])
         assert len(ops) == pg * n_cent, sg
+
+
+def test_all_17_plane_groups(cf):
+    # plane groups 1-17: point-group order per crystal class, centring (c) doubles it
+    pg = {1: 1, 2: 2, 3: 2, 4: 2, 5: 2, 6: 4, 7: 4, 8: 4, 9: 4, 10: 4, 11: 8, 12: 8,
+          13: 3, 14: 6, 15: 6, 16: 6, 17: 12}
+    assert cf.available_groups(2) == list(range(1, 18))
+    for sg, order in pg.items():
+        ops = cf.get_ops(sg, 2, (12, 12))
+        assert len({op.R for op in ops}) == order, sg
+        assert len(ops) == order * (2 if sg in (5, 9) else 1), sg
