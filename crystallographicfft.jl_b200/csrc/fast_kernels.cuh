@@ -332,12 +332,21 @@ __global__ void k_plane_fwd_h(const DevGeom* __restrict__ g, const typename Cx<T
   __syncthreads();
   group_rows<C, false, H>(buf, nch * H, tid, nth);   // x lines
   __syncthreads();
-  group_cols<C, false, H>(buf, nch * H, tid, nth);   // y lines
-  __syncthreads();
+  // y lines: each thread owns the column (c, x) and stores it straight to the
+  // workspace (consecutive threads write consecutive x).
   constexpr int HV = H * H * H;
   C* dst0 = W + static_cast<size_t>(slot) * nch * HV + iz * H * H;
-  for (int c = 0; c < nch; ++c)
-    for (int e = tid; e < H * H; e += nth) dst0[c * HV + e] = buf[c * PL + (e / H) * S + (e % H)];
+  for (int l = tid; l < nch * H; l += nth) {
+    const int c = l / H, x = l % H;
+    const C* p = buf + c * PL + x;
+    C v[H];
+#pragma unroll
+    for (int i = 0; i < H; ++i) v[i] = p[i * S];
+    reg_fft<C, false, H>(v);
+    C* d = dst0 + static_cast<size_t>(c) * HV + x;
+#pragma unroll
+    for (int i = 0; i < H; ++i) d[i * H] = v[i];
+  }
 }
 
 // Backward plane kernel, cubic H: inverse x/y FFT of W[slot][c][iz] + unfold of the two
@@ -358,13 +367,22 @@ __global__ void k_plane_bwd_h(const DevGeom* __restrict__ g, const typename Cx<T
   const bool USE_E = E != nullptr;  // warp-uniform
   const int tid = threadIdx.x, nth = blockDim.x;
   constexpr int HV = H * H * H;
+  // y lines straight from the workspace into registers (coalesced across x), inverse
+  // FFT, into shared memory; then the x lines there.
   const C* src0 = W + static_cast<size_t>(slot) * nch * HV + iz * H * H;
-  for (int c = 0; c < nch; ++c)
-    for (int e = tid; e < H * H; e += nth) buf[c * PL + (e / H) * S + (e % H)] = src0[c * HV + e];
+  for (int l = tid; l < nch * H; l += nth) {
+    const int c = l / H, x = l % H;
+    const C* q = src0 + static_cast<size_t>(c) * HV + x;
+    C v[H];
+#pragma unroll
+    for (int i = 0; i < H; ++i) v[i] = q[i * H];
+    reg_fft<C, true, H>(v);
+    C* p = buf + c * PL + x;
+#pragma unroll
+    for (int i = 0; i < H; ++i) p[i * S] = v[i];
+  }
   __syncthreads();
   group_rows<C, true, H>(buf, nch * H, tid, nth);
-  __syncthreads();
-  group_cols<C, true, H>(buf, nch * H, tid, nth);
   __syncthreads();
   const size_t mvol = static_cast<size_t>(g->M[0]) * g->M[1] * g->M[2];
   T* dsta = f0 + static_cast<size_t>(fa) * mvol;
