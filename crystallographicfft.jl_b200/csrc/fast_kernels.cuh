@@ -677,6 +677,7 @@ __global__ void k_recon_h(const DevGeom* __restrict__ g, const typename Cx<T>::t
 // matrices diag(+-1, +-1, +-1) (any translations): the 8 taps read G0 at the sign
 // images s.h of h, which all lie in one parity channel, and the Hermitian partner
 // X(-q) of tap s is tap ~s.  Eight workspace loads per point and slot.
+constexpr int kDiagSlots = 2;
 template <typename T, int M, bool USE_K>
 __global__ void k_recon_diag8(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
                               const uint32_t* __restrict__ spec_h, const T* __restrict__ K,
@@ -690,10 +691,8 @@ __global__ void k_recon_diag8(const DevGeom* __restrict__ g, const typename Cx<T
   if (tid < 8) sCh[tid] = g->chan_of_parity[tid];
   __syncthreads();
   const int s = blockIdx.x * blockDim.x + tid;
-  const int slot = blockIdx.y;
   if (s >= g->n_spec) return;
-  const int fa = 2 * slot;
-  const bool has_b = fa + 1 < nfields;
+  const int ns = g->n_spec;
   const uint32_t hp = spec_h[s];
   const int h0 = static_cast<int>(hp & 1023u), h1 = static_cast<int>((hp >> 10) & 1023u), h2 = static_cast<int>((hp >> 20) & 1023u);
   const bool cen = g->centered;
@@ -705,38 +704,54 @@ __global__ void k_recon_diag8(const DevGeom* __restrict__ g, const typename Cx<T
   const int m0 = mod_m<M>(M - p0), m1 = mod_m<M>(M - p1), m2 = mod_m<M>(M - p2);
   int c = 0;
   if (cen) c = sCh[(p0 & 1) + 2 * (p1 & 1) + 4 * (p2 & 1)];
+  // This thread serves kDiagSlots consecutive slots (fields 2 slot, 2 slot + 1): the
+  // indices and phases are shared, the gathers of all its slots are in flight together.
+  const int slot0 = blockIdx.y * kDiagSlots;
   if (c < 0) {  // extinct parity class: every tap reads zero
     const C z = mk<C>(static_cast<T>(0), static_cast<T>(0));
-    F[static_cast<size_t>(fa) * g->n_spec + s] = z;
-    if (has_b) F[static_cast<size_t>(fa + 1) * g->n_spec + s] = z;
+    for (int f = 2 * slot0; f < min(nfields, 2 * (slot0 + kDiagSlots)); ++f) F[static_cast<size_t>(f) * ns + s] = z;
     return;
   }
   const int X0[2] = {(p0 >> ls) * Hc * Hc, (m0 >> ls) * Hc * Hc};
   const int X1[2] = {(p1 >> ls) * Hc, (m1 >> ls) * Hc};
   const int X2[2] = {p2 >> ls, m2 >> ls};
-  const C* Wb = WT + (static_cast<size_t>(slot) * g->n_ch + c) * hvol;
-  C X[8];
+  C X[kDiagSlots][8];
 #pragma unroll
-  for (int sg = 0; sg < 8; ++sg) X[sg] = Wb[X0[sg & 1] + X1[(sg >> 1) & 1] + X2[(sg >> 2) & 1]];
+  for (int k = 0; k < kDiagSlots; ++k) {
+    const int slot = min(slot0 + k, (nfields - 1) / 2);  // clamped: beyond the batch the result is dropped
+    const C* Wb = WT + (static_cast<size_t>(slot) * g->n_ch + c) * hvol;
+#pragma unroll
+    for (int sg = 0; sg < 8; ++sg) X[k][sg] = Wb[X0[sg & 1] + X1[(sg >> 1) & 1] + X2[(sg >> 2) & 1]];
+  }
   const C* ph = tables + g->ph_off;
   const int P = g->P, pmask = g->pmask;
-  const T half = static_cast<T>(0.5);
-  C acca = mk<C>(static_cast<T>(0), static_cast<T>(0));
-  C accb = acca;
+  C w[8];
 #pragma unroll
   for (int sg = 0; sg < 8; ++sg) {
-    const C Xs = X[sg], Xn = X[7 - sg];
-    const C Ga = mk<C>(half * (Xs.x + Xn.x), half * (Xs.y - Xn.y));
-    const C Gb = mk<C>(half * (Xs.y + Xn.y), half * (Xn.x - Xs.x));
     int j = h0 * sTP[sg][0] + h1 * sTP[sg][1] + h2 * sTP[sg][2];
     j = pmask >= 0 ? (j & pmask) : ((j % P) + P) % P;
-    const C w = ph[j];
-    acca = cadd(acca, cmul(Ga, w));
-    accb = cadd(accb, cmul(Gb, w));
+    w[sg] = ph[j];
   }
-  if (USE_K) { const T k = K[s]; acca = cscale(acca, k); accb = cscale(accb, k); }
-  F[static_cast<size_t>(fa) * g->n_spec + s] = acca;
-  if (has_b) F[static_cast<size_t>(fa + 1) * g->n_spec + s] = accb;
+  const T half = static_cast<T>(0.5);
+  const T kk = USE_K ? K[s] : static_cast<T>(1);
+#pragma unroll
+  for (int k = 0; k < kDiagSlots; ++k) {
+    const int fa = 2 * (slot0 + k);
+    if (fa >= nfields) break;
+    C acca = mk<C>(static_cast<T>(0), static_cast<T>(0));
+    C accb = acca;
+#pragma unroll
+    for (int sg = 0; sg < 8; ++sg) {
+      const C Xs = X[k][sg], Xn = X[k][7 - sg];
+      const C Ga = mk<C>(half * (Xs.x + Xn.x), half * (Xs.y - Xn.y));
+      const C Gb = mk<C>(half * (Xs.y + Xn.y), half * (Xn.x - Xs.x));
+      acca = cadd(acca, cmul(Ga, w[sg]));
+      accb = cadd(accb, cmul(Gb, w[sg]));
+    }
+    if (USE_K) { acca = cscale(acca, kk); accb = cscale(accb, kk); }
+    F[static_cast<size_t>(fa) * ns + s] = acca;
+    if (fa + 1 < nfields) F[static_cast<size_t>(fa + 1) * ns + s] = accb;
+  }
 }
 
 // G0 at orbit representatives of the two fields of a slot, packed as G_a + i G_b.
@@ -830,16 +845,21 @@ template <typename T>
 __global__ void k_group_spectra(const typename Cx<T>::type* __restrict__ F, typename Cx<T>::type* __restrict__ FT,
                                 int ns, int nb) {
   using C = typename Cx<T>::type;
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= ns) return;
+  const int s0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);  // two spectral points per thread
+  if (s0 >= ns) return;
+  const bool two = s0 + 1 < ns;
   const int q = blockIdx.y;
-  C v[4];
+  C v[2][4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     const int f = 4 * q + k;
-    v[k] = f < nb ? F[static_cast<size_t>(f) * ns + s] : mk<C>(static_cast<T>(0), static_cast<T>(0));
+    const C* row = F + static_cast<size_t>(f) * ns + s0;
+    const C z = mk<C>(static_cast<T>(0), static_cast<T>(0));
+    v[0][k] = f < nb ? __ldg(row) : z;
+    v[1][k] = (f < nb && two) ? __ldg(row + 1) : z;
   }
-  store_quad(FT + (static_cast<size_t>(q) * ns + s) * 4, v);
+  store_quad(FT + (static_cast<size_t>(q) * ns + s0) * 4, v[0]);
+  if (two) store_quad(FT + (static_cast<size_t>(q) * ns + s0 + 1) * 4, v[1]);
 }
 
 // Backward inverse reconstruction for a quad of fields:
@@ -1205,9 +1225,10 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
         const uint32_t* sh = static_cast<const uint32_t*>(a.spec_h);
         const bool use_K = a.use_K, perm = a.rep_perm;
         if (a.rep_diag8) {
+          const dim3 gd((a.n_spec + 255) / 256, (nslots + kDiagSlots - 1) / kDiagSlots);
           CFFT_FOR_M(M, {
-            if (use_K) k_recon_diag8<T, MM, true><<<gr, 256, 0, st>>>(g, tab, sh, K, W, F, nb);
-            else k_recon_diag8<T, MM, false><<<gr, 256, 0, st>>>(g, tab, sh, nullptr, W, F, nb);
+            if (use_K) k_recon_diag8<T, MM, true><<<gd, 256, 0, st>>>(g, tab, sh, K, W, F, nb);
+            else k_recon_diag8<T, MM, false><<<gd, 256, 0, st>>>(g, tab, sh, nullptr, W, F, nb);
           });
           break;
         }
@@ -1235,7 +1256,7 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
         if (a.reps_quad) {
           const int nq = (nb + 3) / 4;
           C* FT = static_cast<C*>(a.FT);
-          k_group_spectra<T><<<dim3((a.n_spec + 255) / 256, nq), 256, 0, st>>>(Fin, FT, a.n_spec, nb);
+          k_group_spectra<T><<<dim3((a.n_spec + 511) / 512, nq), 256, 0, st>>>(Fin, FT, a.n_spec, nb);
           const dim3 gq((4 * no + 255) / 256, nq);
           const uint32_t* pk = static_cast<const uint32_t*>(a.inv_pk);
           switch (a.d) {
