@@ -2,8 +2,13 @@
 FP32 with the centring fold, batched fields resident in HBM.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl ours|reference]
+                    [--workload im3m128|pmmm64|ia3d96-step|mixed]
 
 One step = one forward + backward KRFFT over B fields (f0 -> spectral ASU -> f0).
+The default workload is the headline line; --workload selects a secondary single-GPU
+measurement (Pmmm 64^3 FP64 forward + backward; the Ia-3d 96^3 FP32 diffusion contour
+step; 64 fields over four cubic groups and four grid edges, forward + backward and a
+50-step diffusion solve each).
 Prints ONE JSON line on rank 0.  Under torchrun each rank runs its own batch
 (fields are independent: replicas / weak scaling); the step time is the max over
 ranks.  `--impl reference` times the FP64 CPU restatement of the reference's
@@ -381,6 +386,123 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- other workloads
+WORKLOADS = {
+    "pmmm64": dict(sg=47, n=64, precision=8, batch=512, op="fwdbwd",
+                   desc="Pmmm (No. 47) KRFFT forward+backward, 64^3 FP64"),
+    "ia3d96-step": dict(sg=230, n=96, precision=4, batch=512, op="step",
+                        desc="Ia-3d (No. 230) diffusion contour step exp(-w ds/2) IFFT(K FFT(exp(-w ds/2) q)), 96^3 FP32"),
+    "mixed": dict(op="mixed", precision=4, batch=64,
+                  desc="64 fields drawn from Pm-3m, Im-3m, Fd-3m (origin 2), Ia-3d with edges {32,48,64,96}^3, "
+                       "FP32: forward+backward and a 50-step diffusion solve each (one plan and stream per "
+                       "group and edge; the 50-step loop replays a CUDA graph)"),
+}
+
+
+def _field_bytes(plan, rs):
+    return 2 * (rs * int(np.prod(plan.M)) + 2 * rs * plan.n_spec)
+
+
+def run_workload(args):
+    """Secondary measurements (one GPU): the same device-event timing as the main arm."""
+    import torch
+
+    cf = load_package()
+    W = WORKLOADS[args.workload]
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    rs = W["precision"]
+    rdt = torch.float32 if rs == 4 else torch.float64
+    jobs = []  # (plan, q, w or None, F or None, fields, algorithmic bytes per step)
+    if W["op"] == "mixed":
+        rng = np.random.default_rng(64)
+        groups = rng.choice([221, 229, 227, 230], size=W["batch"])
+        edges = rng.choice([32, 48, 64, 96], size=W["batch"])
+        for sg in sorted(set(groups.tolist())):
+            for n in sorted(set(edges.tolist())):
+                count = int(np.sum((groups == sg) & (edges == n)))
+                if count:
+                    jobs.append((int(sg), int(n), count))
+        built = []
+        for sg, n, count in jobs:
+            N = (n,) * 3
+            _, ops_s = cf.find_optimal_shift(cf.get_ops(sg, 3, N), N)
+            spec = cf.calc_spectral_asu(ops_s, 3, N)
+            plan = cf.KRFFTPlan(spec, ops_s, precision=rs, max_batch=count, ds=0.01)
+            q = symmetric_fields(cf, torch, ops_s, N, plan.L, count, seed=sg * 1000 + n, device=dev).to(rdt).contiguous()
+            w = 0.1 * symmetric_fields(cf, torch, ops_s, N, plan.L, count, seed=sg + n, device=dev).to(rdt).contiguous()
+            F = torch.empty((count, plan.n_spec), dtype=torch.complex64 if rs == 4 else torch.complex128, device=dev)
+            built.append((plan, q, w, F, count, (_field_bytes(plan, rs) * 51 + 3 * rs * int(np.prod(plan.M)) * 50) * count))
+        jobs = built
+    else:
+        N = (W["n"],) * 3
+        _, ops_s = cf.find_optimal_shift(cf.get_ops(W["sg"], 3, N), N)
+        spec = cf.calc_spectral_asu(ops_s, 3, N)
+        B = W["batch"]
+        plan = cf.KRFFTPlan(spec, ops_s, precision=rs, max_batch=B, ds=0.01)
+        q = symmetric_fields(cf, torch, ops_s, N, plan.L, B, seed=7, device=dev).to(rdt).contiguous()
+        w = 0.1 * symmetric_fields(cf, torch, ops_s, N, plan.L, B, seed=8, device=dev).to(rdt).contiguous() \
+            if W["op"] == "step" else None
+        F = torch.empty((B, plan.n_spec), dtype=torch.complex64 if rs == 4 else torch.complex128, device=dev)
+        per = _field_bytes(plan, rs) + (3 * rs * int(np.prod(plan.M)) if W["op"] == "step" else 0)
+        jobs = [(plan, q, w, F, B, per * B)]
+    fields = sum(j[4] for j in jobs)
+    qs = [j[1].clone() for j in jobs]
+    main = torch.cuda.current_stream()
+    # independent plans run on their own streams (each plan owns its workspaces)
+    streams = [torch.cuda.Stream() for _ in jobs] if len(jobs) > 1 else [main]
+
+    def step():
+        for st in streams:
+            st.wait_stream(main)
+        for (plan, q, w, F, count, _), qc, st in zip(jobs, qs, streams):
+            with torch.cuda.stream(st):
+                if W["op"] == "step":
+                    plan.step_diffusion(qc, w, 0.01, 1)
+                else:
+                    plan.forward(q, out=F)
+                    plan.backward(F, out=qc)
+                    if W["op"] == "mixed":
+                        plan.step_diffusion(qc, w, 0.01, 50)
+        for st in streams:
+            main.wait_stream(st)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(0.3)
+    cf.LIB.cfft_launch_count(1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        step()
+    e1.record()
+    torch.cuda.synchronize()
+    launches = int(cf.LIB.cfft_launch_count(1))
+    ms_step = e0.elapsed_time(e1) / args.steps
+    clk = clocks.stop()
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    alg = sum(j[5] for j in jobs)
+    achieved = alg / (ms_step * 1e-3) / 1e9
+    line = {"metric": f"{W['desc']}: us per field", "value": ms_step * 1000.0 / fields, "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if rs == 4 else "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "description": W["desc"], "fields": fields,
+                       "plans": [{"N": list(j[0].N), "centering": j[0].centering, "centered": j[0].centered,
+                                  "fields": j[4]} for j in jobs]},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "peak_source": "measured" if "hbm_gbs" in peaks else "fallback", "traffic": None},
+            "gpu_launches": launches, "clocks": clk, "e2e": None}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -390,10 +512,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing (profiling runs)")
+    ap.add_argument("--workload", default="im3m128", choices=["im3m128"] + sorted(WORKLOADS),
+                    help="im3m128 is the headline line; the others are secondary single-GPU measurements")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload != "im3m128":
+        run_workload(args)
     else:
         run_ours(args)
 

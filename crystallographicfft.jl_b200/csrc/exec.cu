@@ -1017,6 +1017,8 @@ void plan_device_free(Plan* p) {
                    &p->d_qt, &p->d_gt, &p->d_work_Q};
   for (void** b : bufs)
     if (*b) { cudaFree(*b); *b = nullptr; }
+  for (auto& gph : p->step_graphs) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(gph.exec));
+  p->step_graphs.clear();
   if (p->own_stream) { cudaStreamDestroy(static_cast<cudaStream_t>(p->own_stream)); p->own_stream = nullptr; }
   for (int l = 0; l < Plan::kMaxLanes; ++l) {
     if (p->lane_stream[l]) { cudaStreamDestroy(static_cast<cudaStream_t>(p->lane_stream[l])); p->lane_stream[l] = nullptr; }
@@ -1071,6 +1073,70 @@ Status exec_scft_step(Plan* p, void* f0, int B, void* stream, std::string* err) 
   return run_chunks<float>(p, true, true, static_cast<const float*>(f0), static_cast<float2*>(p->d_work_F), static_cast<float*>(f0), nullptr, true, B, s, err);
 }
 
+// The n_steps contour steps (forward + K + backward with the interaction factors E on
+// both sides) on field buffer q.
+template <typename T>
+Status contour_steps(Plan* p, T* q, int n_steps, int B, cudaStream_t s, std::string* err) {
+  using C = typename Cx<T>::type;
+  for (int i = 0; i < n_steps; ++i) {
+    Status st = run_chunks<T>(p, true, true, q, static_cast<C*>(p->d_work_F), q, static_cast<const T*>(p->d_work_E),
+                              true, B, s, err);
+    if (st != Status::kOk) return st;
+  }
+  return Status::kOk;
+}
+
+// Contour loops of at least kGraphMinSteps steps run as a CUDA graph: captured on the
+// plan's own stream the first time a (q, B, n_steps) combination is seen, then replayed
+// on the caller's stream (one launch instead of ~7 per step and chunk).  The graph
+// reads only plan-owned buffers besides q, so a new kernel (update_kernel) or new
+// interaction factors are picked up on replay.  CFFT_STEP_GRAPH=0 launches directly.
+constexpr int kGraphMinSteps = 4;
+constexpr size_t kMaxStepGraphs = 8;
+
+template <typename T>
+Status step_graph_run(Plan* p, T* q, int n_steps, int B, cudaStream_t s, bool* done, std::string* err) {
+  *done = false;
+  for (auto& gph : p->step_graphs)
+    if (gph.q == q && gph.batch == B && gph.n_steps == n_steps) {
+      CFFT_CUDA(cudaGraphLaunch(static_cast<cudaGraphExec_t>(gph.exec), s), "step graph launch");
+      gph.last_use = ++p->graph_clock;
+      g_launches += gph.kernels;
+      *done = true;
+      return Status::kOk;
+    }
+  cudaStream_t cs = static_cast<cudaStream_t>(p->own_stream);
+  const int64_t before = g_launches;
+  if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+    cudaGetLastError();
+    return Status::kOk;  // not capturable here: the caller launches directly
+  }
+  std::string cerr;
+  const Status st = contour_steps<T>(p, q, n_steps, B, cs, &cerr);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ee = cudaStreamEndCapture(cs, &graph);
+  const int64_t kernels = g_launches - before;
+  g_launches = before;  // captured, not launched
+  cudaGraphExec_t exec = nullptr;
+  if (st != Status::kOk || ee != cudaSuccess || !graph || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return Status::kOk;  // direct launches instead
+  }
+  cudaGraphDestroy(graph);
+  if (p->step_graphs.size() >= kMaxStepGraphs) {
+    auto oldest = std::min_element(p->step_graphs.begin(), p->step_graphs.end(),
+                                   [](const Plan::StepGraph& a, const Plan::StepGraph& b) { return a.last_use < b.last_use; });
+    cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(oldest->exec));
+    p->step_graphs.erase(oldest);
+  }
+  p->step_graphs.push_back({q, B, n_steps, exec, kernels, ++p->graph_clock});
+  CFFT_CUDA(cudaGraphLaunch(exec, s), "step graph launch");
+  g_launches += kernels;
+  *done = true;
+  return Status::kOk;
+}
+
 Status exec_step_diffusion(Plan* p, void* q, const void* w, double dt, int n_steps, int B, void* stream,
                            std::string* err) {
   Status st = check_batch(p, B, err);
@@ -1079,23 +1145,22 @@ Status exec_step_diffusion(Plan* p, void* q, const void* w, double dt, int n_ste
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const size_t n = static_cast<size_t>(B) * p->T.M[0] * p->T.M[1] * p->T.M[2];
   const int grid = static_cast<int>(std::min<size_t>((n + 255) / 256, 148 * 16));
+  const char* ge = std::getenv("CFFT_STEP_GRAPH");
+  const bool graph = n_steps >= kGraphMinSteps && !(ge && ge[0] == '0');
+  bool done = false;
   if (p->precision == 8) {
     k_interaction<double><<<grid, 256, 0, s>>>(static_cast<const double*>(w), static_cast<double*>(p->d_work_E), dt / 2, n);
     ++g_launches;
-    for (int i = 0; i < n_steps; ++i) {
-      st = run_chunks<double>(p, true, true, static_cast<const double*>(q), static_cast<double2*>(p->d_work_F),
-                              static_cast<double*>(q), static_cast<const double*>(p->d_work_E), true, B, s, err);
-      if (st != Status::kOk) return st;
-    }
+    if (graph && (st = step_graph_run<double>(p, static_cast<double*>(q), n_steps, B, s, &done, err)) != Status::kOk)
+      return st;
+    if (!done && (st = contour_steps<double>(p, static_cast<double*>(q), n_steps, B, s, err)) != Status::kOk) return st;
   } else {
     k_interaction<float><<<grid, 256, 0, s>>>(static_cast<const float*>(w), static_cast<float*>(p->d_work_E),
                                               static_cast<float>(dt / 2), n);
     ++g_launches;
-    for (int i = 0; i < n_steps; ++i) {
-      st = run_chunks<float>(p, true, true, static_cast<const float*>(q), static_cast<float2*>(p->d_work_F),
-                             static_cast<float*>(q), static_cast<const float*>(p->d_work_E), true, B, s, err);
-      if (st != Status::kOk) return st;
-    }
+    if (graph && (st = step_graph_run<float>(p, static_cast<float*>(q), n_steps, B, s, &done, err)) != Status::kOk)
+      return st;
+    if (!done && (st = contour_steps<float>(p, static_cast<float*>(q), n_steps, B, s, err)) != Status::kOk) return st;
   }
   CFFT_CUDA(cudaGetLastError(), "step_diffusion launch");
   return Status::kOk;

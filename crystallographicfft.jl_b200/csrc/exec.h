@@ -60,6 +60,17 @@ struct Plan {
   bool cluster = false;         // fused cluster kernels: fold+xyz FFT and expand+xyz IFFT+unfold
   // Q-matrix diffusion step (M2Q: plain path, M7: centred path): host tables and their
   // channel-point ordered device copies, plus a second channel workspace per lane.
+  // Contour-loop graphs of cfft_step_diffusion: the n_steps forward + K + backward
+  // steps on a fixed field buffer, captured once and replayed (a cudaGraphExec_t each).
+  struct StepGraph {
+    void* q;
+    int batch, n_steps;
+    void* exec;
+    int64_t kernels;   // kernel launches one replay stands for
+    uint64_t last_use;
+  };
+  std::vector<StepGraph> step_graphs;
+  uint64_t graph_clock = 0;
   int qmode = 0;                // 0 none, 3 M2Q, 4 M7 (the cfft_path value)
   std::vector<double> q_host;   // d x Mvol complex (re, im)
   std::vector<int32_t> q_gather;  // d x Mvol

@@ -269,3 +269,43 @@ def test_tetragonal_trigonal_hexagonal_groups(cf, O, prep, sg, precision):
     assert rel_err(F.cpu().numpy(), truth) < TOL[precision]
     assert rel_err(from_dev(plan.backward(F), plan.M), f0) < TOL[precision] * 10
     plan.close()
+
+
+def test_step_diffusion_graph_replay(cf, O, prep):
+    # cfft_step_diffusion runs loops of >= 4 steps as a captured CUDA graph: replays
+    # (same buffer), a new buffer and a kernel update must match direct launches exactly
+    import os
+
+    p = prep(229, (32, 32, 32))
+    plan = make_plan(cf, p, (32, 32, 32), 4, max_batch=3)
+    g = torch.Generator(device="cuda:0").manual_seed(5)
+    shape = (3,) + tuple(reversed(plan.M))
+    q0 = torch.randn(shape, generator=g, device="cuda:0")
+    w = 0.2 * torch.randn(shape, generator=g, device="cuda:0")
+
+    def direct(q, n):
+        for _ in range(n):
+            plan.step_diffusion(q, w, 0.02, n_steps=1)  # one step: never a graph
+        return q
+
+    want = direct(q0.clone(), 6)
+    a = q0.clone()
+    plan.step_diffusion(a, w, 0.02, n_steps=6)        # captured + replayed
+    assert torch.equal(a, want)
+    a.copy_(q0)
+    plan.step_diffusion(a, w, 0.02, n_steps=6)        # cache hit
+    assert torch.equal(a, want)
+    b = q0.clone()
+    plan.step_diffusion(b, w, 0.02, n_steps=6)        # another buffer: another graph
+    assert torch.equal(b, want)
+    plan.update_kernel(0.07, LAT)                     # the graph reads the new kernel
+    a.copy_(q0)
+    plan.step_diffusion(a, w, 0.02, n_steps=6)
+    os.environ["CFFT_STEP_GRAPH"] = "0"
+    try:
+        c = q0.clone()
+        plan.step_diffusion(c, w, 0.02, n_steps=6)
+    finally:
+        del os.environ["CFFT_STEP_GRAPH"]
+    assert torch.equal(a, c) and not torch.equal(a, want)
+    plan.close()
