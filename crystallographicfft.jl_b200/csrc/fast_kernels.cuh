@@ -527,21 +527,27 @@ k_bwd_cluster_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __res
 }
 
 constexpr int kZB = kFastZB;
+// Threads of the z kernels that take one (y, x) line each: kZB y values x H lines, in
+// whole warps, at least 64.
+template <int H> constexpr int z_threads() { return ((kZB * H + 31) / 32) * 32 < 64 ? 64 : ((kZB * H + 31) / 32) * 32; }
 
 // Forward z FFT, cubic H: W[slot][c][z][y][x] (in) -> WT[slot][c][x][y][z] (z fastest,
 // out, same storage: each CTA reads and writes exactly the same addresses).  Thread
 // (yy, x) loads its z line straight into registers (coalesced across x); the
-// transposed store goes through shared memory.
+// transposed store goes through shared memory.  Launched with z_threads<H>() threads;
+// when kZB divides H every CTA holds kZB y values and the store loop's bounds and
+// divisors are compile-time constants.
 template <typename T, int H>
 __global__ void k_fft_z_fwd_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* W,
                               typename Cx<T>::type* WT) {
   using C = typename Cx<T>::type;
   constexpr int S = H + 1;
   constexpr int HV = H * H * H;
+  constexpr int kThr = z_threads<H>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf = reinterpret_cast<C*>(smem_raw);  // [yy][x][z] padded
   const int y0 = blockIdx.x * kZB, c = blockIdx.y, slot = blockIdx.z;
-  const int ny = min(kZB, H - y0);
+  const int ny = H % kZB == 0 ? kZB : min(kZB, H - y0);
   const int tid = threadIdx.x;
   const size_t base = (static_cast<size_t>(slot) * g->n_ch + c) * HV;
   const int yy = tid / H, x = tid % H;
@@ -557,11 +563,21 @@ __global__ void k_fft_z_fwd_h(const DevGeom* __restrict__ g, const typename Cx<T
   }
   __syncthreads();
   C* dst = WT + base;
-  const int run = ny * H;  // contiguous (yy, z) run per x
-  for (int e = tid; e < H * run; e += blockDim.x) {
-    const int xx = e / run, r = e % run;
-    const int y2 = r / H, z = r % H;
-    dst[(xx * H + y0) * H + r] = buf[(y2 * H + xx) * S + z];
+  if constexpr (H % kZB == 0) {
+    constexpr int run = kZB * H;  // contiguous (yy, z) run per x
+#pragma unroll 4
+    for (int e = tid; e < H * run; e += kThr) {
+      const int xx = e / run, r = e % run;
+      const int y2 = r / H, z = r % H;
+      dst[(xx * H + y0) * H + r] = buf[(y2 * H + xx) * S + z];
+    }
+  } else {
+    const int run = ny * H;
+    for (int e = tid; e < H * run; e += kThr) {
+      const int xx = e / run, r = e % run;
+      const int y2 = r / H, z = r % H;
+      dst[(xx * H + y0) * H + r] = buf[(y2 * H + xx) * S + z];
+    }
   }
 }
 
@@ -732,7 +748,18 @@ __global__ void k_recon_diag8(const DevGeom* __restrict__ g, const typename Cx<T
     j = pmask >= 0 ? (j & pmask) : ((j % P) + P) % P;
     w[sg] = ph[j];
   }
+  // Taps sg and 7 - sg are Hermitian partners: with u = w[sg], v = w[7 - sg] and
+  // 2 G = (a, b), G u + conj(G) v = (a Pw.x + b Qw.x, a Pw.y + b Qw.y) for
+  // Pw = (u + v) / 2, Qw = ((v.y - u.y) / 2, (u.x - v.x) / 2), shared by every slot
+  // and both fields.
   const T half = static_cast<T>(0.5);
+  C Pw[4], Qw[4];
+#pragma unroll
+  for (int sg = 0; sg < 4; ++sg) {
+    const C u = w[sg], v = w[7 - sg];
+    Pw[sg] = mk<C>(half * (u.x + v.x), half * (u.y + v.y));
+    Qw[sg] = mk<C>(half * (v.y - u.y), half * (u.x - v.x));
+  }
   const T kk = USE_K ? K[s] : static_cast<T>(1);
 #pragma unroll
   for (int k = 0; k < kDiagSlots; ++k) {
@@ -741,12 +768,14 @@ __global__ void k_recon_diag8(const DevGeom* __restrict__ g, const typename Cx<T
     C acca = mk<C>(static_cast<T>(0), static_cast<T>(0));
     C accb = acca;
 #pragma unroll
-    for (int sg = 0; sg < 8; ++sg) {
+    for (int sg = 0; sg < 4; ++sg) {
       const C Xs = X[k][sg], Xn = X[k][7 - sg];
-      const C Ga = mk<C>(half * (Xs.x + Xn.x), half * (Xs.y - Xn.y));
-      const C Gb = mk<C>(half * (Xs.y + Xn.y), half * (Xn.x - Xs.x));
-      acca = cadd(acca, cmul(Ga, w[sg]));
-      accb = cadd(accb, cmul(Gb, w[sg]));
+      const T a = Xs.x + Xn.x, b = Xs.y - Xn.y;    // 2 G_a
+      const T a2 = Xs.y + Xn.y, b2 = Xn.x - Xs.x;  // 2 G_b
+      acca.x = fma(a, Pw[sg].x, fma(b, Qw[sg].x, acca.x));
+      acca.y = fma(a, Pw[sg].y, fma(b, Qw[sg].y, acca.y));
+      accb.x = fma(a2, Pw[sg].x, fma(b2, Qw[sg].x, accb.x));
+      accb.y = fma(a2, Pw[sg].y, fma(b2, Qw[sg].y, accb.y));
     }
     if (USE_K) { acca = cscale(acca, kk); accb = cscale(accb, kk); }
     F[static_cast<size_t>(fa) * ns + s] = acca;
@@ -1216,7 +1245,7 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
     const dim3 gz((H + kZB - 1) / kZB, nch, nslots);
     switch (a.stage) {
       case 1:
-        CFFT_FOR_H(H, { k_fft_z_fwd_h<T, HH><<<gz, thr_z, smem_z, st>>>(g, W, W); });
+        CFFT_FOR_H(H, { k_fft_z_fwd_h<T, HH><<<gz, z_threads<HH>(), smem_z, st>>>(g, W, W); });
         break;
       case 2: {
         const dim3 gr((a.n_spec + 255) / 256, nslots);
