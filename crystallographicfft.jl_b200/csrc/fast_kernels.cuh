@@ -142,6 +142,41 @@ __device__ __forceinline__ void group_cols(C* buf, int nlines, int tid, int nth)
   }
 }
 
+// Fold of VW consecutive x values (ix0 .. ix0 + VW - 1) of channel row iy: the eight
+// octant values of fields a and b (va[k], vb[k], octant k = kx + 2 ky + 4 kz) go through
+// the WHT8, each alive channel takes its fold twiddle, and the results land in the
+// padded planes at buf.
+template <typename T, int H, int CT, int VW>
+__device__ __forceinline__ void fold_emit(const T (&va)[8][VW], const T (&vb)[8][VW], int ix0, int iy,
+                                          const typename Cx<T>::type* __restrict__ ftx,
+                                          typename Cx<T>::type ftz, typename Cx<T>::type* buf) {
+  using C = typename Cx<T>::type;
+  constexpr int S = H + 1;
+  constexpr int PL = H * S;
+  constexpr int nch = Cent<CT>::n;
+  const T zero = static_cast<T>(0);
+  const C ty = ftx[iy];
+#pragma unroll
+  for (int l = 0; l < VW; ++l) {
+    T a8[8], b8[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) { a8[k] = va[k][l]; b8[k] = vb[k][l]; }
+    wht8(a8);
+    wht8(b8);
+    const int ix = ix0 + l;
+    const C tx = ftx[ix];
+#pragma unroll
+    for (int c = 0; c < nch; ++c) {
+      const int o = Cent<CT>::off(c);
+      C w = mk<C>(static_cast<T>(1), zero);
+      if (o & 1) w = tx;
+      if (o & 2) w = cmul(w, ty);
+      if (o & 4) w = cmul(w, ftz);
+      buf[c * PL + iy * S + ix] = cmul(mk<C>(a8[o], b8[o]), w);
+    }
+  }
+}
+
 // Fold (or plain load, CT = 0) of the two fields of one slot at channel z-plane iz into
 // the nch padded planes at buf (channel c at buf + c * H * (H + 1)), with the fold
 // twiddles e^{-2 pi i off.n / M} and the interaction factors E when given.  Work is
@@ -197,26 +232,7 @@ __device__ __forceinline__ void fold_plane(const DevGeom* __restrict__ g, const 
             }
           }
         }
-        const C ty = ftx[iy];
-#pragma unroll
-        for (int l = 0; l < VW; ++l) {
-          T a8[8], b8[8];
-#pragma unroll
-          for (int k = 0; k < 8; ++k) { a8[k] = va[k][l]; b8[k] = vb[k][l]; }
-          wht8(a8);
-          wht8(b8);
-          const int ix = ix0 + l;
-          const C tx = ftx[ix];
-#pragma unroll
-          for (int c = 0; c < nch; ++c) {
-            const int o = Cent<CT>::off(c);
-            C w = mk<C>(static_cast<T>(1), zero);
-            if (o & 1) w = tx;
-            if (o & 2) w = cmul(w, ty);
-            if (o & 4) w = cmul(w, ftz);
-            buf[c * PL + iy * S + ix] = cmul(mk<C>(a8[o], b8[o]), w);
-          }
-        }
+        fold_emit<T, H, CT, VW>(va, vb, ix0, iy, ftx, ftz, buf);
       }
     } else {
       for (int e = tid; e < H * H; e += nth) {
@@ -308,6 +324,27 @@ __device__ __forceinline__ void unfold_plane(const DevGeom* __restrict__ g, cons
   }
 }
 
+// y lines of the nch padded planes at buf: each thread owns the column (c, x),
+// transforms it and stores it straight to the workspace plane dst0 (channel stride
+// H^3, consecutive threads write consecutive x).
+template <typename C, int H, int nch>
+__device__ __forceinline__ void y_lines_to_workspace(const C* buf, C* __restrict__ dst0, int tid, int nth) {
+  constexpr int S = H + 1;
+  constexpr int PL = H * S;
+  constexpr int HV = H * H * H;
+  for (int l = tid; l < nch * H; l += nth) {
+    const int c = l / H, x = l % H;
+    const C* p = buf + c * PL + x;
+    C v[H];
+#pragma unroll
+    for (int i = 0; i < H; ++i) v[i] = p[i * S];
+    reg_fft<C, false, H>(v);
+    C* d = dst0 + static_cast<size_t>(c) * HV + x;
+#pragma unroll
+    for (int i = 0; i < H; ++i) d[i * H] = v[i];
+  }
+}
+
 // Forward plane kernel, cubic H: fold (or plain load) of two fields + x FFT + y FFT
 // -> W[slot][c][z][y][x].
 template <typename T, int H, int CT>
@@ -315,8 +352,6 @@ __global__ void k_plane_fwd_h(const DevGeom* __restrict__ g, const typename Cx<T
                               const T* __restrict__ f0, const T* __restrict__ E, typename Cx<T>::type* __restrict__ W,
                               int nfields) {
   using C = typename Cx<T>::type;
-  constexpr int S = H + 1;
-  constexpr int PL = H * S;  // padded plane
   constexpr int nch = Cent<CT>::n;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* buf = reinterpret_cast<C*>(smem_raw);
@@ -332,21 +367,8 @@ __global__ void k_plane_fwd_h(const DevGeom* __restrict__ g, const typename Cx<T
   __syncthreads();
   group_rows<C, false, H>(buf, nch * H, tid, nth);   // x lines
   __syncthreads();
-  // y lines: each thread owns the column (c, x) and stores it straight to the
-  // workspace (consecutive threads write consecutive x).
   constexpr int HV = H * H * H;
-  C* dst0 = W + static_cast<size_t>(slot) * nch * HV + iz * H * H;
-  for (int l = tid; l < nch * H; l += nth) {
-    const int c = l / H, x = l % H;
-    const C* p = buf + c * PL + x;
-    C v[H];
-#pragma unroll
-    for (int i = 0; i < H; ++i) v[i] = p[i * S];
-    reg_fft<C, false, H>(v);
-    C* d = dst0 + static_cast<size_t>(c) * HV + x;
-#pragma unroll
-    for (int i = 0; i < H; ++i) d[i * H] = v[i];
-  }
+  y_lines_to_workspace<C, H, nch>(buf, W + static_cast<size_t>(slot) * nch * HV + iz * H * H, tid, nth);
 }
 
 // Backward plane kernel, cubic H: inverse x/y FFT of W[slot][c][iz] + unfold of the two
@@ -894,11 +916,12 @@ __global__ void k_group_spectra(const typename Cx<T>::type* __restrict__ F, type
 // Backward inverse reconstruction for a quad of fields:
 //   G0(q_o) = (1/d) sum_a ph_a F(spec_a)   (F conjugated where flagged)
 // from the packed alias rows (spec+1 in bits 0-19, conj in bit 20, phase numerator in
-// bits 21-31; 0 = no alias).  Four consecutive lanes take the four fields of one
-// orbit, so every alias gather of a warp reads whole 32-byte quads; the d loads of a
-// lane are independent and in flight together.  The field pairs of each workspace
-// slot are combined as the slot's transform input X = G_a + i G_b and stored as
-// G0P[q][o][pair] (pair 0: fields 4q, 4q+1; pair 1: fields 4q+2, 4q+3).
+// bits 21-31; 0 = no alias).  Two consecutive lanes take one orbit: lane k reads fields
+// 4q + 2k and 4q + 2k + 1, one 16-byte half (float) of the spectral point's 32-byte
+// quad in FT, so every alias gather of a warp reads whole quads and the two fields of
+// a workspace slot sit in the same lane.  The d loads of a lane are independent and in
+// flight together.  Lane k stores the slot input X = G_a + i G_b of its pair as
+// G0P[q][o][k] (pair 0: fields 4q, 4q+1; pair 1: fields 4q+2, 4q+3).
 template <typename T, int D>
 __global__ void __launch_bounds__(256)
 k_inv_recon_quad(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
@@ -907,34 +930,46 @@ k_inv_recon_quad(const DevGeom* __restrict__ g, const typename Cx<T>::type* __re
   using C = typename Cx<T>::type;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int no = g->n_orbits;
-  const int o = t >> 2, k = t & 3;
-  const bool valid = o < no;  // no early return: lanes exchange values below
-  const int oc = valid ? o : no - 1;
+  const int o = t >> 1, k = t & 1;
+  if (o >= no) return;
   const int q = blockIdx.y;
-  const C* ft = FT + static_cast<size_t>(q) * g->n_spec * 4 + k;
+  const C* ft = FT + static_cast<size_t>(q) * g->n_spec * 4 + 2 * k;
   const C* ph = tables + g->ph_off;
   uint32_t e[D];
-  load_alias_row<D>(inv_pk, oc, e);
-  C v[D];
+  load_alias_row<D>(inv_pk, o, e);
+  C v[D][2];
 #pragma unroll
   for (int a = 0; a < D; ++a) {
     const uint32_t sp = e[a] & 0xFFFFFu;
-    v[a] = __ldg(ft + static_cast<size_t>(sp ? sp - 1 : 0) * 4);
+    const C* src = ft + static_cast<size_t>(sp ? sp - 1 : 0) * 4;
+    if constexpr (sizeof(C) == 8) {
+      const float4 u = __ldg(reinterpret_cast<const float4*>(src));
+      v[a][0] = mk<C>(u.x, u.y);
+      v[a][1] = mk<C>(u.z, u.w);
+    } else {
+      v[a][0] = __ldg(src);
+      v[a][1] = __ldg(src + 1);
+    }
   }
-  C acc = mk<C>(static_cast<T>(0), static_cast<T>(0));
+  const T zero = static_cast<T>(0);
+  T re[2] = {zero, zero}, im[2] = {zero, zero};
 #pragma unroll
   for (int a = 0; a < D; ++a) {
+    // term = v conj(w), or conj(v) conj(w) when flagged: with s = -1 if flagged,
+    // re = v.x w.x + v.y (s w.y), im = v.y (s w.x) - v.x w.y.
     C w = ph[e[a] >> 21];
-    if ((e[a] & 0xFFFFFu) == 0) w = mk<C>(static_cast<T>(0), static_cast<T>(0));
-    acc = cadd(acc, cmulc(((e[a] >> 20) & 1u) ? cconj(v[a]) : v[a], w));
+    if ((e[a] & 0xFFFFFu) == 0) w = mk<C>(zero, zero);
+    const T sg = ((e[a] >> 20) & 1u) ? static_cast<T>(-1) : static_cast<T>(1);
+    const T cA = w.x, cB = sg * w.y, cC = sg * w.x, cD = -w.y;
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+      re[f] = fma(v[a][f].x, cA, fma(v[a][f].y, cB, re[f]));
+      im[f] = fma(v[a][f].y, cC, fma(v[a][f].x, cD, im[f]));
+    }
   }
   const T inv_d = static_cast<T>(1.0 / static_cast<double>(D));
-  acc = cscale(acc, inv_d);
-  // lane k (even) takes G_b from lane k + 1; fields past the batch were zero-filled.
-  const T bx = __shfl_down_sync(0xffffffffu, acc.x, 1);
-  const T by = __shfl_down_sync(0xffffffffu, acc.y, 1);
-  if (valid && !(k & 1))
-    G0P[(static_cast<size_t>(q) * no + o) * 2 + (k >> 1)] = mk<C>(acc.x - by, acc.y + bx);
+  // X = G_a + i G_b; fields past the batch were zero-filled.
+  G0P[(static_cast<size_t>(q) * no + o) * 2 + k] = mk<C>(inv_d * (re[0] - im[1]), inv_d * (im[0] + re[1]));
 }
 
 // Backward orbit expansion + inverse z FFT for a quad of fields (two workspace
@@ -1016,6 +1051,7 @@ __global__ void k_qmul_ifft_z_h(const DevGeom* __restrict__ g, const typename Cx
 }
 
 constexpr int kMaxDynSmemFast = 227 * 1024;
+
 
 #define CFFT_FOR_H(H, ...)                                                        \
   switch (H) {                                                                    \
@@ -1286,7 +1322,7 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
           const int nq = (nb + 3) / 4;
           C* FT = static_cast<C*>(a.FT);
           k_group_spectra<T><<<dim3((a.n_spec + 511) / 512, nq), 256, 0, st>>>(Fin, FT, a.n_spec, nb);
-          const dim3 gq((4 * no + 255) / 256, nq);
+          const dim3 gq((2 * no + 255) / 256, nq);
           const uint32_t* pk = static_cast<const uint32_t*>(a.inv_pk);
           switch (a.d) {
             case 1: k_inv_recon_quad<T, 1><<<gq, 256, 0, st>>>(g, tab, pk, FT, G0R); break;
