@@ -498,6 +498,78 @@ std::vector<unsigned char> make_table_bytes(const Plan& p, DevGeom* g) {
   return bytes;
 }
 
+// Units of the fused z FFT + diagonal-sign gather (stage 6): in each channel, every
+// channel row y is paired with its mirror y' = (M - p1) >> ls (p1 = 2 y + the channel's
+// y parity when centred, p1 = y otherwise); self-mirrored rows are paired with each
+// other.  Every spectral point joins the unit holding its row, so all eight taps of the
+// point lie in that unit's two rows.  Units are ordered by point count, largest first.
+// Leaves the fusion off (plan unchanged) when a point falls in a parity class without
+// a channel or CFFT_ZRECON=0.
+Status build_zrecon_units(Plan* p, std::string* err) {
+  if (const char* e = std::getenv("CFFT_ZRECON")) if (e[0] == '0') return Status::kOk;
+  const PlanTables& T = p->T;
+  const int H = p->fast_h, nch = T.n_ch;
+  const int M = T.M[0];
+  const int ls = T.centered ? 1 : 0;
+  if (M != (T.centered ? 2 * H : H) || H > 255 || nch > 255) return Status::kOk;
+  struct Unit { int c, ya, yb; std::vector<uint32_t> pts; };
+  std::vector<Unit> units;
+  std::vector<int> unit_of_row(static_cast<size_t>(nch) * H, -1);
+  for (int c = 0; c < nch; ++c) {
+    int ypar = 0;
+    if (T.centered) {
+      int o = -1;
+      for (int k = 0; k < 8; ++k)
+        if (T.chan_of_parity[k] == c) { o = k; break; }
+      if (o < 0) return Status::kOk;
+      ypar = (o >> 1) & 1;
+    }
+    std::vector<int> singles;
+    for (int y = 0; y < H; ++y) {
+      if (unit_of_row[static_cast<size_t>(c) * H + y] >= 0) continue;
+      const int p1 = T.centered ? 2 * y + ypar : y;
+      const int y2 = (p1 ? M - p1 : 0) >> ls;
+      if (y2 == y) { singles.push_back(y); continue; }
+      units.push_back({c, y, y2, {}});
+      unit_of_row[static_cast<size_t>(c) * H + y] = unit_of_row[static_cast<size_t>(c) * H + y2] =
+          static_cast<int>(units.size()) - 1;
+    }
+    for (size_t i = 0; i < singles.size(); i += 2) {
+      const int yb = i + 1 < singles.size() ? singles[i + 1] : -1;
+      units.push_back({c, singles[i], yb, {}});
+      unit_of_row[static_cast<size_t>(c) * H + singles[i]] = static_cast<int>(units.size()) - 1;
+      if (yb >= 0) unit_of_row[static_cast<size_t>(c) * H + yb] = static_cast<int>(units.size()) - 1;
+    }
+  }
+  for (size_t sidx = 0; sidx < T.spec.size(); ++sidx) {
+    int pp[3];
+    for (int d = 0; d < 3; ++d) pp[d] = static_cast<int>(floor_mod(T.spec[sidx].h[d], M));
+    const int c = T.centered ? T.chan_of_parity[(pp[0] & 1) + 2 * (pp[1] & 1) + 4 * (pp[2] & 1)] : 0;
+    if (c < 0) return Status::kOk;
+    const int u = unit_of_row[static_cast<size_t>(c) * H + (pp[1] >> ls)];
+    if (u < 0) { *err = "fused gather: spectral point outside the unit rows"; return Status::kInvalid; }
+    units[u].pts.push_back(static_cast<uint32_t>(sidx));
+  }
+  std::stable_sort(units.begin(), units.end(), [](const Unit& a, const Unit& b) { return a.pts.size() > b.pts.size(); });
+  std::vector<uint4> ut;
+  std::vector<uint32_t> pts;
+  for (const Unit& u : units) {
+    if (u.pts.empty()) continue;
+    ut.push_back(make_uint4(static_cast<uint32_t>(u.c) | (static_cast<uint32_t>(u.ya) << 8) |
+                                (static_cast<uint32_t>(u.yb + 1) << 16),
+                            static_cast<uint32_t>(pts.size()), static_cast<uint32_t>(u.pts.size()), 0u));
+    pts.insert(pts.end(), u.pts.begin(), u.pts.end());
+  }
+  if (ut.empty()) return Status::kOk;
+  CFFT_CUDA(cudaMalloc(&p->d_zr_units, ut.size() * sizeof(uint4)), "fused gather units");
+  CFFT_CUDA(cudaMalloc(&p->d_zr_pts, pts.size() * 4), "fused gather points");
+  CFFT_CUDA(cudaMemcpy(p->d_zr_units, ut.data(), ut.size() * sizeof(uint4), cudaMemcpyHostToDevice), "upload units");
+  CFFT_CUDA(cudaMemcpy(p->d_zr_pts, pts.data(), pts.size() * 4, cudaMemcpyHostToDevice), "upload unit points");
+  p->zr_units = static_cast<int>(ut.size());
+  p->zrecon = true;
+  return Status::kOk;
+}
+
 // Stages of one forward + backward: 0 plane/fold + x/y FFT, 1 z FFT, 2 reconstruct,
 // 3 inverse reconstruct (+ orbit expansion), 4 inverse z FFT, 5 inverse x/y FFT + unfold.
 // `nb` fields starting at the caller's pointers; the workspace holds one chunk.
@@ -523,6 +595,7 @@ Status launch_stage(Plan* p, int stage, const T* f0, typename Cx<T>::type* F, co
     a.cent_type = p->cent_type; a.d = T_.d;
     a.n_spec = static_cast<int>(T_.spec.size()); a.n_orbits = static_cast<int>(T_.orbit_rep.size());
     a.use_K = use_K; a.rep_diag8 = p->rep_diag8; a.rep_perm = p->rep_perm; a.reps_quad = p->reps_quad;
+    a.zr_units = p->d_zr_units; a.zr_pts = p->d_zr_pts; a.zr_n_units = p->zr_units;
     a.cluster = p->cluster;
     a.cluster_ctas = p->cluster_ctas;
     if (q_step) {  // stage 4: Q-multiply + inverse z FFT into the Q workspace; stage 5 reads it
@@ -613,8 +686,9 @@ Status run_chunks(Plan* p, bool fwd, bool bwd, const T* f0, typename Cx<T>::type
       continue;
     }
     if (fwd)
-      for (int s = 0; s < 3; ++s) {
-        Status r = launch_stage<T>(p, s, fin, Fc, nullptr, nullptr, Ec, use_K, nb, ls, err, lane);
+      for (int s : {0, 1, 2}) {
+        if (p->zrecon && s == 1) continue;  // stage 6 = z FFT + gather
+        Status r = launch_stage<T>(p, p->zrecon && s == 2 ? 6 : s, fin, Fc, nullptr, nullptr, Ec, use_K, nb, ls, err, lane);
         if (r != Status::kOk) return r;
       }
     if (bwd)
@@ -645,8 +719,12 @@ Status profile_roundtrip(Plan* p, const T* f0, typename Cx<T>::type* F, T* f0_ou
     const int nb = std::min(p->chunk, B - b0);
     CFFT_CUDA(cudaEventRecord(ev[0], st), "event record");
     for (int s = 0; s < 6; ++s) {
-      Status r = launch_stage<T>(p, s, f0 + b0 * mvol, F + b0 * ns, F + b0 * ns, f0_out + b0 * mvol, nullptr, false, nb, st, err);
-      if (r != Status::kOk) return r;
+      // With the fused stage 6 the z FFT and the gather are one launch, timed as stage 1.
+      if (!(p->zrecon && s == 2)) {
+        Status r = launch_stage<T>(p, p->zrecon && s == 1 ? 6 : s, f0 + b0 * mvol, F + b0 * ns, F + b0 * ns,
+                                   f0_out + b0 * mvol, nullptr, false, nb, st, err);
+        if (r != Status::kOk) return r;
+      }
       CFFT_CUDA(cudaEventRecord(ev[s + 1], st), "event record");
     }
     CFFT_CUDA(cudaGetLastError(), "profile launch");
@@ -921,6 +999,10 @@ Status plan_device_init(Plan* p, std::string* err) {
   }
   if (p->reps_quad)
     CFFT_CUDA(cudaMemcpy(p->d_inv_pk, inv_pk.data(), inv_pk.size() * 4, cudaMemcpyHostToDevice), "upload packed table");
+  if (p->fast_h && p->rep_diag8 && !p->qmode) {
+    Status zs = build_zrecon_units(p, err);
+    if (zs != Status::kOk) return zs;
+  }
   // Orbit expansion writes only alive positions; channel positions never written stay zero.
   CFFT_CUDA(cudaMemset(p->d_work_T, 0, p->lanes * p->w_lane_bytes), "clear workspace");
   if (p->precision == 8) set_smem_attrs<double>();
@@ -957,6 +1039,7 @@ Status plan_device_init(Plan* p, std::string* err) {
       p->cluster = mc >= 1;
     }
   }
+  if (p->cluster) p->zrecon = false;  // the cluster forward writes the z-fastest workspace for stage 2
   cudaStream_t s;
   CFFT_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "create stream");
   p->own_stream = s;
@@ -1014,7 +1097,7 @@ void plan_device_free(Plan* p) {
   void** bufs[] = {&p->d_geom, &p->d_tables, &p->d_spec_h, &p->d_K, &p->d_orbit_rep, &p->d_inv_spec,
                    &p->d_inv_phase, &p->d_img_mask, &p->d_fill_map, &p->d_work_T, &p->d_work_F,
                    &p->d_work_E, &p->d_stage_in, &p->d_stage_out, &p->d_expand, &p->d_g0r, &p->d_inv_pk, &p->d_ft,
-                   &p->d_qt, &p->d_gt, &p->d_work_Q};
+                   &p->d_qt, &p->d_gt, &p->d_work_Q, &p->d_zr_units, &p->d_zr_pts};
   for (void** b : bufs)
     if (*b) { cudaFree(*b); *b = nullptr; }
   for (auto& gph : p->step_graphs) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(gph.exec));

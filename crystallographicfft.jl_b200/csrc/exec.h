@@ -34,6 +34,8 @@ struct Plan {
   void* d_g0r = nullptr;        // fast path: G0 at orbit representatives (per lane)
   void* d_ft = nullptr;         // packed backward path: spectra regrouped in quads of fields (per lane)
   void* d_inv_pk = nullptr;     // fast path: packed alias table for the shared-memory gather
+  void* d_zr_units = nullptr;   // fused z FFT + gather: uint4 per unit (c | ya | yb, first point, count)
+  void* d_zr_pts = nullptr;     // fused z FFT + gather: spectral indices grouped by unit
   void* own_stream = nullptr;
   static constexpr int kMaxLanes = 4;
   void* lane_stream[kMaxLanes] = {};  // concurrent chunk lanes (fork/join on the caller's stream)
@@ -57,6 +59,8 @@ struct Plan {
   bool rep_perm = false;        // representative ops are signed permutations
   bool rep_diag8 = false;       // representative ops are the 8 diagonal sign matrices
   bool reps_quad = false;       // packed alias rows; fields gathered and expanded in quads
+  bool zrecon = false;          // forward z FFT fused with the diagonal-sign gather (stage 6)
+  int zr_units = 0;             // units of the fused kernel (channel + mirrored row pair)
   bool cluster = false;         // fused cluster kernels: fold+xyz FFT and expand+xyz IFFT+unfold
   // Q-matrix diffusion step (M2Q: plain path, M7: centred path): host tables and their
   // channel-point ordered device copies, plus a second channel workspace per lane.

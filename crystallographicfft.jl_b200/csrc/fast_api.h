@@ -32,6 +32,10 @@ struct FastArgs {
   int stage = 0, nb = 0, H = 0, n_ch = 1, centered = 0, cent_type = 0, d = 1;
   int n_spec = 0, n_orbits = 0;
   bool use_K = false, rep_diag8 = false, rep_perm = false, reps_quad = false;
+  // Stage 6 (fused z FFT + diagonal-sign gather): unit table and spectral points.
+  const void* zr_units = nullptr;
+  const void* zr_pts = nullptr;
+  int zr_n_units = 0;
   bool cluster = false;   // fused cluster kernels for stages 0 (with 1) and 5 (with 4)
   int cluster_ctas = 8;   // CTAs per cluster (8, or 16 where the device allows it)
   // Q-matrix step: stage 4 reads W (forward G0, z-fastest) and writes W2

@@ -805,6 +805,118 @@ __global__ void k_recon_diag8(const DevGeom* __restrict__ g, const typename Cx<T
   }
 }
 
+// Forward z FFT fused with the spectral-ASU gather, for diagonal-sign representative
+// operations (the taps of a spectral point h read G0 at the sign images of h, which lie
+// in one channel c on the rows y = p1 >> ls and its mirror y' = m1 >> ls).  A CTA
+// takes one unit (channel c and a mirrored pair of channel rows y_a, y_b; y_b < 0 when
+// the unit has one row) and ZR_SLOTS workspace slots:
+//   1. thread (slot, row, x) loads the z line W[slot][c][z][y_row][x] (coalesced across
+//      x), transforms it in registers and keeps it in shared memory [slot][row][x][z];
+//   2. the unit's spectral points (a list built at plan time) are gathered from shared
+//      memory as in k_recon_diag8 and written to F.
+// The transposed workspace of the separate z kernel is never written or read back.
+// Unit entry: x = c | y_a << 8 | (y_b + 1) << 16, y = first point, z = point count.
+template <int H> constexpr int zr_threads(int slots) { return slots * 2 * H < 32 ? 32 : ((slots * 2 * H + 31) / 32) * 32; }
+template <typename T, int H, int SL, bool USE_K>
+__global__ void k_fft_z_recon_diag8(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                                    const uint32_t* __restrict__ spec_h, const T* __restrict__ K,
+                                    const uint4* __restrict__ units, const uint32_t* __restrict__ pts,
+                                    const typename Cx<T>::type* __restrict__ W, typename Cx<T>::type* __restrict__ F,
+                                    int nfields) {
+  using C = typename Cx<T>::type;
+  constexpr int S = H + 1;
+  constexpr int HV = H * H * H;
+  constexpr int RS = H * S;  // one row of (x, z) lines
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf = reinterpret_cast<C*>(smem_raw);  // [slot][row][x][z] padded
+  __shared__ int sTP[8][3];
+  const int tid = threadIdx.x, nth = blockDim.x;
+  if (tid < 24) sTP[tid / 3][tid % 3] = g->rep_tp[g->sign_op[tid / 3]][tid % 3];
+  const uint4 un = units[blockIdx.x];
+  const int c = static_cast<int>(un.x & 0xFFu), ya = static_cast<int>((un.x >> 8) & 0xFFu);
+  const int yb = static_cast<int>((un.x >> 16) & 0xFFu) - 1;
+  const int slot0 = blockIdx.y * SL;
+  const int nslots = (nfields + 1) / 2;
+  const int nch = g->n_ch;
+  if (tid < SL * 2 * H) {
+    const int k = tid / (2 * H), r = (tid / H) & 1, x = tid % H;
+    const int slot = slot0 + k;
+    const int y = r ? yb : ya;
+    if (slot < nslots && y >= 0) {
+      const C* src = W + (static_cast<size_t>(slot) * nch + c) * HV + y * H + x;
+      C v[H];
+#pragma unroll
+      for (int z = 0; z < H; ++z) v[z] = src[static_cast<size_t>(z) * H * H];
+      reg_fft<C, false, H>(v);
+      C* row = buf + (k * 2 + r) * RS + x * S;
+#pragma unroll
+      for (int z = 0; z < H; ++z) row[z] = v[z];
+    }
+  }
+  __syncthreads();
+  const bool cen = g->centered;
+  const int M = cen ? 2 * H : H;
+  const int ls = cen ? 1 : 0;
+  const int ns = g->n_spec;
+  const C* ph = tables + g->ph_off;
+  const int P = g->P, pmask = g->pmask;
+  const T half = static_cast<T>(0.5);
+  const int nvalid = min(SL, nslots - slot0);
+  for (int i = tid; i < static_cast<int>(un.z); i += nth) {
+    const uint32_t sidx = __ldg(pts + un.y + i);
+    const uint32_t hp = __ldg(spec_h + sidx);
+    const int h0 = static_cast<int>(hp & 1023u), h1 = static_cast<int>((hp >> 10) & 1023u), h2 = static_cast<int>((hp >> 20) & 1023u);
+    const int p0 = cen ? mod_m<2 * H>(h0) : mod_m<H>(h0);
+    const int p1 = cen ? mod_m<2 * H>(h1) : mod_m<H>(h1);
+    const int p2 = cen ? mod_m<2 * H>(h2) : mod_m<H>(h2);
+    const int m0 = p0 ? M - p0 : 0, m1 = p1 ? M - p1 : 0, m2 = p2 ? M - p2 : 0;
+    const int X0[2] = {(p0 >> ls) * S, (m0 >> ls) * S};
+    const int X1[2] = {((p1 >> ls) != ya) * RS, ((m1 >> ls) != ya) * RS};
+    const int X2[2] = {p2 >> ls, m2 >> ls};
+    C Pw[4], Qw[4];
+    {
+      C w[8];
+#pragma unroll
+      for (int sg = 0; sg < 8; ++sg) {
+        int j = h0 * sTP[sg][0] + h1 * sTP[sg][1] + h2 * sTP[sg][2];
+        j = pmask >= 0 ? (j & pmask) : ((j % P) + P) % P;
+        w[sg] = ph[j];
+      }
+      // Hermitian tap pairs (sg, 7 - sg), as in k_recon_diag8.
+#pragma unroll
+      for (int sg = 0; sg < 4; ++sg) {
+        const C u = w[sg], v = w[7 - sg];
+        Pw[sg] = mk<C>(half * (u.x + v.x), half * (u.y + v.y));
+        Qw[sg] = mk<C>(half * (v.y - u.y), half * (u.x - v.x));
+      }
+    }
+    const T kk = USE_K ? K[sidx] : static_cast<T>(1);
+#pragma unroll
+    for (int k = 0; k < SL; ++k) {
+      if (k >= nvalid) break;
+      const C* b = buf + k * 2 * RS;
+      C X[8];
+#pragma unroll
+      for (int sg = 0; sg < 8; ++sg) X[sg] = b[X0[sg & 1] + X1[(sg >> 1) & 1] + X2[(sg >> 2) & 1]];
+      C acca = mk<C>(static_cast<T>(0), static_cast<T>(0)), accb = acca;
+#pragma unroll
+      for (int sg = 0; sg < 4; ++sg) {
+        const C Xs = X[sg], Xn = X[7 - sg];
+        const T a = Xs.x + Xn.x, bq = Xs.y - Xn.y;
+        const T a2 = Xs.y + Xn.y, b2 = Xn.x - Xs.x;
+        acca.x = fma(a, Pw[sg].x, fma(bq, Qw[sg].x, acca.x));
+        acca.y = fma(a, Pw[sg].y, fma(bq, Qw[sg].y, acca.y));
+        accb.x = fma(a2, Pw[sg].x, fma(b2, Qw[sg].x, accb.x));
+        accb.y = fma(a2, Pw[sg].y, fma(b2, Qw[sg].y, accb.y));
+      }
+      if (USE_K) { acca = cscale(acca, kk); accb = cscale(accb, kk); }
+      const int fa = 2 * (slot0 + k);
+      F[static_cast<size_t>(fa) * ns + sidx] = acca;
+      if (fa + 1 < nfields) F[static_cast<size_t>(fa + 1) * ns + sidx] = accb;
+    }
+  }
+}
+
 // G0 at orbit representatives of the two fields of a slot, packed as G_a + i G_b.
 // Each thread serves SPT consecutive slots, reusing the table entries and keeping
 // several independent spectrum gathers in flight.
@@ -1052,6 +1164,16 @@ __global__ void k_qmul_ifft_z_h(const DevGeom* __restrict__ g, const typename Cx
 
 constexpr int kMaxDynSmemFast = 227 * 1024;
 
+// Workspace slots per CTA of the fused z FFT + gather: 4, or 2 with CFFT_ZR_SLOTS=2
+// (measured on Im-3m 128^3 FP32: 4 slots slightly ahead).
+inline int zr_slots() {
+  static const int n = [] {
+    const char* e = std::getenv("CFFT_ZR_SLOTS");
+    return (e && e[0] == '2') ? 2 : 4;
+  }();
+  return n;
+}
+
 
 #define CFFT_FOR_H(H, ...)                                                        \
   switch (H) {                                                                    \
@@ -1191,6 +1313,16 @@ Status fast_unit_init(std::string* err) {
         }
       } else {
         cudaFuncSetAttribute(k_fft_z_fwd_h<T, HH>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
+        // The fused kernel also holds 96 bytes of static shared memory; its dynamic
+        // share above 48 KB (FP64, 4 slots) needs the attribute, so failures are reported.
+        {
+          constexpr int kZr = kMaxDynSmemFast - 1024;
+          cudaError_t ze = cudaFuncSetAttribute(k_fft_z_recon_diag8<T, HH, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kZr);
+          if (ze == cudaSuccess) ze = cudaFuncSetAttribute(k_fft_z_recon_diag8<T, HH, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kZr);
+          if (ze == cudaSuccess) ze = cudaFuncSetAttribute(k_fft_z_recon_diag8<T, HH, 4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kZr);
+          if (ze == cudaSuccess) ze = cudaFuncSetAttribute(k_fft_z_recon_diag8<T, HH, 4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kZr);
+          if (ze != cudaSuccess) return fast_cuda(ze, "fused z FFT + gather shared-memory attribute", err);
+        }
         cudaFuncSetAttribute(k_expand_ifft_z_h<T, HH>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
       }
     });
@@ -1314,6 +1446,27 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
           default: CFFT_RECON_D(8); break;
         }
 #undef CFFT_RECON_D
+        break;
+      }
+      case 6: {
+        // fused z FFT + diagonal-sign gather, ZR_SLOTS workspace slots per CTA
+        const int sl = zr_slots();
+        const T* K = static_cast<const T*>(a.K);
+        const uint32_t* sh = static_cast<const uint32_t*>(a.spec_h);
+        const uint4* un = static_cast<const uint4*>(a.zr_units);
+        const uint32_t* pt = static_cast<const uint32_t*>(a.zr_pts);
+        const C* Wc = W;
+        CFFT_FOR_H(H, {
+          const size_t sm = static_cast<size_t>(sl) * 2 * HH * (HH + 1) * cs;
+          const dim3 gzr(a.zr_n_units, (nslots + sl - 1) / sl);
+          if (sl == 4) {
+            if (a.use_K) k_fft_z_recon_diag8<T, HH, 4, true><<<gzr, zr_threads<HH>(4), sm, st>>>(g, tab, sh, K, un, pt, Wc, F, nb);
+            else k_fft_z_recon_diag8<T, HH, 4, false><<<gzr, zr_threads<HH>(4), sm, st>>>(g, tab, sh, nullptr, un, pt, Wc, F, nb);
+          } else {
+            if (a.use_K) k_fft_z_recon_diag8<T, HH, 2, true><<<gzr, zr_threads<HH>(2), sm, st>>>(g, tab, sh, K, un, pt, Wc, F, nb);
+            else k_fft_z_recon_diag8<T, HH, 2, false><<<gzr, zr_threads<HH>(2), sm, st>>>(g, tab, sh, nullptr, un, pt, Wc, F, nb);
+          }
+        });
         break;
       }
       case 3: {
