@@ -265,7 +265,7 @@ __device__ __forceinline__ void fold_plane(const DevGeom* __restrict__ g, const 
 // Unfold of the nch inverse-transformed planes at buf (channel z-plane iz) into the two
 // fields of the slot: conjugate fold twiddle, inverse WHT8 / 8, real part -> field a,
 // imaginary part -> field b, times E when given.
-template <typename T, int H, int CT>
+template <typename T, int H, int CT, bool VEC = false>
 __device__ __forceinline__ void unfold_plane(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
                                              const typename Cx<T>::type* buf, T* __restrict__ dsta, T* __restrict__ dstb,
                                              const T* __restrict__ Ea, const T* __restrict__ Eb, bool has_b, bool USE_E,
@@ -291,7 +291,58 @@ __device__ __forceinline__ void unfold_plane(const DevGeom* __restrict__ g, cons
     const T scale = static_cast<T>(1.0 / (8.0 * static_cast<double>(hvol)));
     const C* ftx = tables + g->ftw_off[0];
     const C ftz = tables[g->ftw_off[2] + iz];
-    {
+    constexpr int VW = 16 / static_cast<int>(sizeof(T));  // elements per 16-byte vector
+    const bool vec = VEC && (H % VW == 0) && (reinterpret_cast<uintptr_t>(dsta) % 16 == 0) &&
+                     (!has_b || reinterpret_cast<uintptr_t>(dstb) % 16 == 0) &&
+                     (!USE_E || (reinterpret_cast<uintptr_t>(Ea) % 16 == 0 && (!has_b || reinterpret_cast<uintptr_t>(Eb) % 16 == 0)));
+    if (vec) {
+      // VW consecutive x values per thread; each octant row piece leaves as one 16-byte store.
+      for (int e = tid; e < H * H / VW; e += nth) {
+        const int ix0 = (e % (H / VW)) * VW, iy = e / (H / VW);
+        const C ty = ftx[iy];
+        T oa[8][VW], ob[8][VW];
+#pragma unroll
+        for (int l = 0; l < VW; ++l) {
+          const int ix = ix0 + l;
+          const C tx = ftx[ix];
+          T va[8], vb[8];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) { va[k] = static_cast<T>(0); vb[k] = static_cast<T>(0); }
+#pragma unroll
+          for (int c = 0; c < nch; ++c) {
+            const int o = Cent<CT>::off(c);
+            C w = mk<C>(static_cast<T>(1), static_cast<T>(0));
+            if (o & 1) w = tx;
+            if (o & 2) w = cmul(w, ty);
+            if (o & 4) w = cmul(w, ftz);
+            const C y = cmulc(buf[c * PL + iy * S + ix], w);
+            va[o] = y.x;
+            vb[o] = y.y;
+          }
+          wht8(va);
+          wht8(vb);
+#pragma unroll
+          for (int k = 0; k < 8; ++k) { oa[k][l] = va[k] * scale; ob[k][l] = vb[k] * scale; }
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const int idx = ((iz + ((k >> 2) & 1) * H) * M + iy + ((k >> 1) & 1) * H) * M + ix0 + (k & 1) * H;
+          if (USE_E) {
+            T ea[VW];
+            vload<T>(ea, Ea + idx);
+#pragma unroll
+            for (int l = 0; l < VW; ++l) oa[k][l] *= ea[l];
+            if (has_b) {
+              vload<T>(ea, Eb + idx);
+#pragma unroll
+              for (int l = 0; l < VW; ++l) ob[k][l] *= ea[l];
+            }
+          }
+          vstore<T>(dsta + idx, oa[k]);
+          if (has_b) vstore<T>(dstb + idx, ob[k]);
+        }
+      }
+    } else {
       for (int e = tid; e < H * H; e += nth) {
         const int ix = e % H, iy = e / H;
         T va[8], vb[8];
@@ -373,7 +424,7 @@ __global__ void k_plane_fwd_h(const DevGeom* __restrict__ g, const typename Cx<T
 
 // Backward plane kernel, cubic H: inverse x/y FFT of W[slot][c][iz] + unfold of the two
 // fields (real part -> field a, imaginary part -> field b).
-template <typename T, int H, int CT>
+template <typename T, int H, int CT, bool VEC>
 __global__ void k_plane_bwd_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
                               const typename Cx<T>::type* __restrict__ W, const T* __restrict__ E, T* __restrict__ f0,
                               int nfields) {
@@ -409,7 +460,7 @@ __global__ void k_plane_bwd_h(const DevGeom* __restrict__ g, const typename Cx<T
   const size_t mvol = static_cast<size_t>(g->M[0]) * g->M[1] * g->M[2];
   T* dsta = f0 + static_cast<size_t>(fa) * mvol;
   const T* Ea = USE_E ? E + static_cast<size_t>(fa) * mvol : nullptr;
-  unfold_plane<T, H, CT>(g, tables, buf, dsta, dsta + mvol, Ea, USE_E ? Ea + mvol : nullptr, has_b, USE_E, iz, tid, nth);
+  unfold_plane<T, H, CT, VEC>(g, tables, buf, dsta, dsta + mvol, Ea, USE_E ? Ea + mvol : nullptr, has_b, USE_E, iz, tid, nth);
 }
 
 // ---------------------------------------------------------------- cluster kernels
@@ -1003,23 +1054,36 @@ __device__ __forceinline__ void store_quad(C* __restrict__ p, const C (&v)[4]) {
 
 // Regroup the spectra of nb fields into quads: FT[q][s][k] = F[4q + k][s] (zero past
 // the last field), so one gather of a spectral point serves four fields with one
-// fully used 32-byte sector (float).  Coalesced on both sides.
+// fully used 32-byte sector (float).  Coalesced on both sides; two spectral points per
+// thread, read as one 16-byte vector per field where the row allows it.
 template <typename T>
 __global__ void k_group_spectra(const typename Cx<T>::type* __restrict__ F, typename Cx<T>::type* __restrict__ FT,
                                 int ns, int nb) {
   using C = typename Cx<T>::type;
-  const int s0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);  // two spectral points per thread
+  const int s0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   if (s0 >= ns) return;
   const bool two = s0 + 1 < ns;
   const int q = blockIdx.y;
+  const C z = mk<C>(static_cast<T>(0), static_cast<T>(0));
   C v[2][4];
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     const int f = 4 * q + k;
     const C* row = F + static_cast<size_t>(f) * ns + s0;
-    const C z = mk<C>(static_cast<T>(0), static_cast<T>(0));
-    v[0][k] = f < nb ? __ldg(row) : z;
-    v[1][k] = (f < nb && two) ? __ldg(row + 1) : z;
+    bool done = f >= nb;
+    if (done) { v[0][k] = z; v[1][k] = z; }
+    if constexpr (sizeof(C) == 8) {
+      if (!done && two && (reinterpret_cast<uintptr_t>(row) & 15u) == 0) {
+        const float4 u = __ldg(reinterpret_cast<const float4*>(row));
+        v[0][k] = make_float2(u.x, u.y);
+        v[1][k] = make_float2(u.z, u.w);
+        done = true;
+      }
+    }
+    if (!done) {
+      v[0][k] = __ldg(row);
+      v[1][k] = two ? __ldg(row + 1) : z;
+    }
   }
   store_quad(FT + (static_cast<size_t>(q) * ns + s0) * 4, v[0]);
   if (two) store_quad(FT + (static_cast<size_t>(q) * ns + s0 + 1) * 4, v[1]);
@@ -1090,19 +1154,19 @@ k_inv_recon_quad(const DevGeom* __restrict__ g, const typename Cx<T>::type* __re
 // expansion entries (orbit in bits 0-20, phase numerator in bits 21-31) and the
 // combined representatives G0P[q][o][pair]; both halves read the same entries and
 // 16-byte pairs (the second read hits L1).  The line is transformed in registers and
-// stored coalesced across x.  No shared memory.
-template <typename T, int H>
+// stored coalesced across x.  No shared memory.  A CTA covers YB y values.
+template <typename T, int H, int YB>
 __global__ void k_expand4_ifft_z_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
                                    const uint32_t* __restrict__ ETP, const typename Cx<T>::type* __restrict__ G0P,
                                    typename Cx<T>::type* __restrict__ W, int nfields) {
   using C = typename Cx<T>::type;
   constexpr int HV = H * H * H;
-  constexpr int kHalf = ((kZB * H + 31) / 32) * 32;
-  const int y0 = blockIdx.x * kZB, c = blockIdx.y, q = blockIdx.z;
+  constexpr int kHalf = ((YB * H + 31) / 32) * 32;
+  const int y0 = blockIdx.x * YB, c = blockIdx.y, q = blockIdx.z;
   const int half = threadIdx.x / kHalf, r = threadIdx.x % kHalf;
   const int slot = 2 * q + half;
   if (2 * slot >= nfields) return;
-  const int ny = min(kZB, H - y0);
+  const int ny = min(YB, H - y0);
   const int yy = r / H, x = r % H;
   if (yy >= ny) return;
   const int y = y0 + yy;
@@ -1306,7 +1370,7 @@ Status fast_unit_init(std::string* err) {
         for (int ct = 0; ct < 5; ++ct) {
           CFFT_FOR_CT(ct, {
             cudaFuncSetAttribute(k_plane_fwd_h<T, HH, CTT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
-            cudaFuncSetAttribute(k_plane_bwd_h<T, HH, CTT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
+            cudaFuncSetAttribute(k_plane_bwd_h<T, HH, CTT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
             cluster_attrs<T, HH, CTT, 8>();
             cluster_attrs<T, HH, CTT, 16>();
           });
@@ -1403,7 +1467,7 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
     } else {
       CFFT_FOR_H(H, {
         CFFT_FOR_CT(a.cent_type, {
-          k_plane_bwd_h<T, HH, CTT><<<dim3(H, nslots), thr_plane, smem_plane, st>>>(g, tab, W, E, f0_out, nb);
+          k_plane_bwd_h<T, HH, CTT, true><<<dim3(H, nslots), thr_plane, smem_plane, st>>>(g, tab, W, E, f0_out, nb);
         });
       });
     }
@@ -1500,8 +1564,9 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
         }
         CFFT_FOR_H(H, {
           if (a.reps_quad) {
-            constexpr int half = ((kZB * HH + 31) / 32) * 32;
-            k_expand4_ifft_z_h<T, HH><<<dim3((HH + kZB - 1) / kZB, nch, (nb + 3) / 4), 2 * half, 0, st>>>(
+            // two y values per CTA (128 threads at H = 32): 5 CTAs per SM at this kernel's registers
+            constexpr int half = ((2 * HH + 31) / 32) * 32;
+            k_expand4_ifft_z_h<T, HH, 2><<<dim3((HH + 1) / 2, nch, (nb + 3) / 4), 2 * half, 0, st>>>(
                 g, tab, static_cast<const uint32_t*>(a.expand), G0R, W, nb);
           } else
             k_expand_ifft_z_h<T, HH><<<gz, thr_z, smem_z, st>>>(g, tab, static_cast<const int2*>(a.expand), G0R, W);
