@@ -359,7 +359,7 @@ def run_ours(args):
                    "parallelism": f"replicas x{world}", "roundtrip_rel_err": rt_err},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_source": peak_src, "traffic": None,
-                     "scope": "whole forward+backward (6 launches) per batch; algorithmic bytes 2*(4*M^3 + 8*n_spec) per field",
+                     "scope": "whole forward+backward per batch (6 launches per 64-field chunk); algorithmic bytes 2*(4*M^3 + 8*n_spec) per field",
                      "stage_ms": {n: float(v) for n, v in zip(names, stage)}, "dominant_stage": names[top]},
         "gpu_launches": launches,
         "clocks": clk,
