@@ -28,6 +28,15 @@ namespace {
 // inside an FFT.  Shared-memory rows are padded to an odd stride (H + 1 complex) so
 // row and column accesses of a warp are bank-conflict free.
 
+// Programmatic dependent launch: wait until the previous kernel of the stream has
+// completed and its writes are visible (a no-op when the kernel was launched without
+// the attribute), then let the next kernel of the stream start launching.  Called first
+// in every kernel that launch_k starts, before any global memory access.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 constexpr int kTwOff4 = 0, kTwOff6 = 4, kTwOff8 = 10, kTwOff12 = 18, kTwOff16 = 30, kTwOff24 = 46,
               kTwOff32 = 70, kTwOff48 = 102, kTwTotal = 150;
 __constant__ float2 c_tw_f[kTwTotal];
@@ -402,6 +411,7 @@ template <typename T, int H, int CT>
 __global__ void k_plane_fwd_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
                               const T* __restrict__ f0, const T* __restrict__ E, typename Cx<T>::type* __restrict__ W,
                               int nfields) {
+  pdl_enter();
   using C = typename Cx<T>::type;
   constexpr int nch = Cent<CT>::n;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -428,6 +438,7 @@ template <typename T, int H, int CT, bool VEC>
 __global__ void k_plane_bwd_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
                               const typename Cx<T>::type* __restrict__ W, const T* __restrict__ E, T* __restrict__ f0,
                               int nfields) {
+  pdl_enter();
   using C = typename Cx<T>::type;
   constexpr int S = H + 1;
   constexpr int PL = H * S;
@@ -613,6 +624,7 @@ template <int H> constexpr int z_threads() { return ((kZB * H + 31) / 32) * 32 <
 template <typename T, int H>
 __global__ void k_fft_z_fwd_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* W,
                               typename Cx<T>::type* WT) {
+  pdl_enter();
   using C = typename Cx<T>::type;
   constexpr int S = H + 1;
   constexpr int HV = H * H * H;
@@ -660,6 +672,7 @@ template <typename T, int H>
 __global__ void k_expand_ifft_z_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
                                   const int2* __restrict__ ET, const typename Cx<T>::type* __restrict__ G0R,
                                   typename Cx<T>::type* __restrict__ W) {
+  pdl_enter();
   using C = typename Cx<T>::type;
   constexpr int S = H + 1;
   constexpr int PL = H * S;
@@ -696,6 +709,7 @@ __global__ void k_recon_h(const DevGeom* __restrict__ g, const typename Cx<T>::t
                           const uint32_t* __restrict__ spec_h, const T* __restrict__ K,
                           const typename Cx<T>::type* __restrict__ WT, typename Cx<T>::type* __restrict__ F,
                           int nfields) {
+  pdl_enter();
   using C = typename Cx<T>::type;
   __shared__ int sR[D][9];
   __shared__ int sPS[D][3];
@@ -772,6 +786,7 @@ __global__ void k_recon_diag8(const DevGeom* __restrict__ g, const typename Cx<T
                               const uint32_t* __restrict__ spec_h, const T* __restrict__ K,
                               const typename Cx<T>::type* __restrict__ WT, typename Cx<T>::type* __restrict__ F,
                               int nfields) {
+  pdl_enter();
   using C = typename Cx<T>::type;
   __shared__ int sTP[8][3];  // indexed by sign pattern
   __shared__ int sCh[8];
@@ -874,6 +889,7 @@ __global__ void k_fft_z_recon_diag8(const DevGeom* __restrict__ g, const typenam
                                     const uint4* __restrict__ units, const uint32_t* __restrict__ pts,
                                     const typename Cx<T>::type* __restrict__ W, typename Cx<T>::type* __restrict__ F,
                                     int nfields) {
+  pdl_enter();
   using C = typename Cx<T>::type;
   constexpr int S = H + 1;
   constexpr int HV = H * H * H;
@@ -977,6 +993,7 @@ __global__ void k_inv_recon_reps(const DevGeom* __restrict__ g, const typename C
                                  const int32_t* __restrict__ inv_spec, const int32_t* __restrict__ inv_phase,
                                  const typename Cx<T>::type* __restrict__ F, typename Cx<T>::type* __restrict__ G0R,
                                  int nfields) {
+  pdl_enter();
   using C = typename Cx<T>::type;
   const int o = blockIdx.x * blockDim.x + threadIdx.x;
   if (o >= g->n_orbits) return;
@@ -1059,6 +1076,7 @@ __device__ __forceinline__ void store_quad(C* __restrict__ p, const C (&v)[4]) {
 template <typename T>
 __global__ void k_group_spectra(const typename Cx<T>::type* __restrict__ F, typename Cx<T>::type* __restrict__ FT,
                                 int ns, int nb) {
+  pdl_enter();
   using C = typename Cx<T>::type;
   const int s0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
   if (s0 >= ns) return;
@@ -1103,6 +1121,7 @@ __global__ void __launch_bounds__(256)
 k_inv_recon_quad(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
                  const uint32_t* __restrict__ inv_pk, const typename Cx<T>::type* __restrict__ FT,
                  typename Cx<T>::type* __restrict__ G0P) {
+  pdl_enter();
   using C = typename Cx<T>::type;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int no = g->n_orbits;
@@ -1159,6 +1178,7 @@ template <typename T, int H, int YB>
 __global__ void k_expand4_ifft_z_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
                                    const uint32_t* __restrict__ ETP, const typename Cx<T>::type* __restrict__ G0P,
                                    typename Cx<T>::type* __restrict__ W, int nfields) {
+  pdl_enter();
   using C = typename Cx<T>::type;
   constexpr int HV = H * H * H;
   constexpr int kHalf = ((YB * H + 31) / 32) * 32;
@@ -1196,6 +1216,7 @@ template <typename T, int H>
 __global__ void k_qmul_ifft_z_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ QT,
                                 const int32_t* __restrict__ GT, const typename Cx<T>::type* __restrict__ WT,
                                 typename Cx<T>::type* __restrict__ W2) {
+  pdl_enter();
   using C = typename Cx<T>::type;
   constexpr int HV = H * H * H;
   const int y0 = blockIdx.x * kZB, c = blockIdx.y, slot = blockIdx.z;
@@ -1227,6 +1248,35 @@ __global__ void k_qmul_ifft_z_h(const DevGeom* __restrict__ g, const typename Cx
 }
 
 constexpr int kMaxDynSmemFast = 227 * 1024;
+
+// Programmatic dependent launch of the fast-path kernels (off with CFFT_PDL=0): each
+// kernel of a lane may launch while its predecessor in the stream is finishing, and
+// waits for it in hardware (griddepcontrol.wait, pdl_wait below) before touching memory.
+inline bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("CFFT_PDL");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+template <typename... KArgs, typename... Args>
+inline void launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
+  if (pdl_enabled()) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+  } else {
+    k<<<grid, block, smem, st>>>(std::forward<Args>(args)...);
+  }
+}
 
 // Workspace slots per CTA of the fused z FFT + gather: 4, or 2 with CFFT_ZR_SLOTS=2
 // (measured on Im-3m 128^3 FP32: 4 slots slightly ahead).
@@ -1461,13 +1511,13 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
     if (a.stage == 0) {
       CFFT_FOR_H(H, {
         CFFT_FOR_CT(a.cent_type, {
-          k_plane_fwd_h<T, HH, CTT><<<dim3(H, nslots), thr_plane, smem_plane, st>>>(g, tab, f0, E, W, nb);
+          launch_k(k_plane_fwd_h<T, HH, CTT>, dim3(H, nslots), thr_plane, smem_plane, st, g, tab, f0, E, W, nb);
         });
       });
     } else {
       CFFT_FOR_H(H, {
         CFFT_FOR_CT(a.cent_type, {
-          k_plane_bwd_h<T, HH, CTT, true><<<dim3(H, nslots), thr_plane, smem_plane, st>>>(g, tab, W, E, f0_out, nb);
+          launch_k(k_plane_bwd_h<T, HH, CTT, true>, dim3(H, nslots), thr_plane, smem_plane, st, g, tab, W, E, f0_out, nb);
         });
       });
     }
@@ -1477,7 +1527,7 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
     const dim3 gz((H + kZB - 1) / kZB, nch, nslots);
     switch (a.stage) {
       case 1:
-        CFFT_FOR_H(H, { k_fft_z_fwd_h<T, HH><<<gz, z_threads<HH>(), smem_z, st>>>(g, W, W); });
+        CFFT_FOR_H(H, { launch_k(k_fft_z_fwd_h<T, HH>, gz, z_threads<HH>(), smem_z, st, g, W, W); });
         break;
       case 2: {
         const dim3 gr((a.n_spec + 255) / 256, nslots);
@@ -1488,19 +1538,19 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
         if (a.rep_diag8) {
           const dim3 gd((a.n_spec + 255) / 256, (nslots + kDiagSlots - 1) / kDiagSlots);
           CFFT_FOR_M(M, {
-            if (use_K) k_recon_diag8<T, MM, true><<<gd, 256, 0, st>>>(g, tab, sh, K, W, F, nb);
-            else k_recon_diag8<T, MM, false><<<gd, 256, 0, st>>>(g, tab, sh, nullptr, W, F, nb);
+            if (use_K) launch_k(k_recon_diag8<T, MM, true>, gd, 256, 0, st, g, tab, sh, K, W, F, nb);
+            else launch_k(k_recon_diag8<T, MM, false>, gd, 256, 0, st, g, tab, sh, nullptr, W, F, nb);
           });
           break;
         }
 #define CFFT_RECON_D(DD)                                                                                  \
   CFFT_FOR_M(M, {                                                                                         \
     if (use_K) {                                                                                          \
-      if (perm) k_recon_h<T, MM, DD, true, true><<<gr, 256, 0, st>>>(g, tab, sh, K, W, F, nb);            \
-      else k_recon_h<T, MM, DD, true, false><<<gr, 256, 0, st>>>(g, tab, sh, K, W, F, nb);                \
+      if (perm) launch_k(k_recon_h<T, MM, DD, true, true>, gr, 256, 0, st, g, tab, sh, K, W, F, nb);            \
+      else launch_k(k_recon_h<T, MM, DD, true, false>, gr, 256, 0, st, g, tab, sh, K, W, F, nb);                \
     } else {                                                                                              \
-      if (perm) k_recon_h<T, MM, DD, false, true><<<gr, 256, 0, st>>>(g, tab, sh, nullptr, W, F, nb);     \
-      else k_recon_h<T, MM, DD, false, false><<<gr, 256, 0, st>>>(g, tab, sh, nullptr, W, F, nb);         \
+      if (perm) launch_k(k_recon_h<T, MM, DD, false, true>, gr, 256, 0, st, g, tab, sh, nullptr, W, F, nb);     \
+      else launch_k(k_recon_h<T, MM, DD, false, false>, gr, 256, 0, st, g, tab, sh, nullptr, W, F, nb);         \
     }                                                                                                     \
   })
         switch (a.d) {
@@ -1524,11 +1574,11 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
           const size_t sm = static_cast<size_t>(sl) * 2 * HH * (HH + 1) * cs;
           const dim3 gzr(a.zr_n_units, (nslots + sl - 1) / sl);
           if (sl == 4) {
-            if (a.use_K) k_fft_z_recon_diag8<T, HH, 4, true><<<gzr, zr_threads<HH>(4), sm, st>>>(g, tab, sh, K, un, pt, Wc, F, nb);
-            else k_fft_z_recon_diag8<T, HH, 4, false><<<gzr, zr_threads<HH>(4), sm, st>>>(g, tab, sh, nullptr, un, pt, Wc, F, nb);
+            if (a.use_K) launch_k(k_fft_z_recon_diag8<T, HH, 4, true>, gzr, zr_threads<HH>(4), sm, st, g, tab, sh, K, un, pt, Wc, F, nb);
+            else launch_k(k_fft_z_recon_diag8<T, HH, 4, false>, gzr, zr_threads<HH>(4), sm, st, g, tab, sh, nullptr, un, pt, Wc, F, nb);
           } else {
-            if (a.use_K) k_fft_z_recon_diag8<T, HH, 2, true><<<gzr, zr_threads<HH>(2), sm, st>>>(g, tab, sh, K, un, pt, Wc, F, nb);
-            else k_fft_z_recon_diag8<T, HH, 2, false><<<gzr, zr_threads<HH>(2), sm, st>>>(g, tab, sh, nullptr, un, pt, Wc, F, nb);
+            if (a.use_K) launch_k(k_fft_z_recon_diag8<T, HH, 2, true>, gzr, zr_threads<HH>(2), sm, st, g, tab, sh, K, un, pt, Wc, F, nb);
+            else launch_k(k_fft_z_recon_diag8<T, HH, 2, false>, gzr, zr_threads<HH>(2), sm, st, g, tab, sh, nullptr, un, pt, Wc, F, nb);
           }
         });
         break;
@@ -1538,25 +1588,25 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
         if (a.reps_quad) {
           const int nq = (nb + 3) / 4;
           C* FT = static_cast<C*>(a.FT);
-          k_group_spectra<T><<<dim3((a.n_spec + 511) / 512, nq), 256, 0, st>>>(Fin, FT, a.n_spec, nb);
+          launch_k(k_group_spectra<T>, dim3((a.n_spec + 511) / 512, nq), 256, 0, st, Fin, FT, a.n_spec, nb);
           const dim3 gq((2 * no + 255) / 256, nq);
           const uint32_t* pk = static_cast<const uint32_t*>(a.inv_pk);
           switch (a.d) {
-            case 1: k_inv_recon_quad<T, 1><<<gq, 256, 0, st>>>(g, tab, pk, FT, G0R); break;
-            case 2: k_inv_recon_quad<T, 2><<<gq, 256, 0, st>>>(g, tab, pk, FT, G0R); break;
-            case 4: k_inv_recon_quad<T, 4><<<gq, 256, 0, st>>>(g, tab, pk, FT, G0R); break;
-            default: k_inv_recon_quad<T, 8><<<gq, 256, 0, st>>>(g, tab, pk, FT, G0R); break;
+            case 1: launch_k(k_inv_recon_quad<T, 1>, gq, 256, 0, st, g, tab, pk, FT, G0R); break;
+            case 2: launch_k(k_inv_recon_quad<T, 2>, gq, 256, 0, st, g, tab, pk, FT, G0R); break;
+            case 4: launch_k(k_inv_recon_quad<T, 4>, gq, 256, 0, st, g, tab, pk, FT, G0R); break;
+            default: launch_k(k_inv_recon_quad<T, 8>, gq, 256, 0, st, g, tab, pk, FT, G0R); break;
           }
           break;
         }
-        k_inv_recon_reps<T><<<dim3((no + 127) / 128, (nslots + kRepSlots - 1) / kRepSlots), 128, 0, st>>>(
+        launch_k(k_inv_recon_reps<T>, dim3((no + 127) / 128, (nslots + kRepSlots - 1) / kRepSlots), 128, 0, st, 
             g, tab, static_cast<const int32_t*>(a.inv_spec), static_cast<const int32_t*>(a.inv_phase), Fin, G0R, nb);
         break;
       }
       default:
         if (a.q_step) {
           CFFT_FOR_H(H, {
-            k_qmul_ifft_z_h<T, HH><<<gz, thr_z, 0, st>>>(g, static_cast<const C*>(a.QT),
+            launch_k(k_qmul_ifft_z_h<T, HH>, gz, thr_z, 0, st, g, static_cast<const C*>(a.QT),
                                                          static_cast<const int32_t*>(a.GT), W,
                                                          static_cast<C*>(a.W2));
           });
@@ -1566,10 +1616,10 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
           if (a.reps_quad) {
             // two y values per CTA (128 threads at H = 32): 5 CTAs per SM at this kernel's registers
             constexpr int half = ((2 * HH + 31) / 32) * 32;
-            k_expand4_ifft_z_h<T, HH, 2><<<dim3((HH + 1) / 2, nch, (nb + 3) / 4), 2 * half, 0, st>>>(
+            launch_k(k_expand4_ifft_z_h<T, HH, 2>, dim3((HH + 1) / 2, nch, (nb + 3) / 4), 2 * half, 0, st, 
                 g, tab, static_cast<const uint32_t*>(a.expand), G0R, W, nb);
           } else
-            k_expand_ifft_z_h<T, HH><<<gz, thr_z, smem_z, st>>>(g, tab, static_cast<const int2*>(a.expand), G0R, W);
+            launch_k(k_expand_ifft_z_h<T, HH>, gz, thr_z, smem_z, st, g, tab, static_cast<const int2*>(a.expand), G0R, W);
         });
         break;
     }
