@@ -1259,6 +1259,11 @@ inline bool pdl_enabled() {
   }();
   return on;
 }
+// First failure of a launch_k launch on this thread since fast_unit_launch last read it.
+inline cudaError_t& launch_error() {
+  static thread_local cudaError_t e = cudaSuccess;
+  return e;
+}
 template <typename... KArgs, typename... Args>
 inline void launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st, Args&&... args) {
   if (pdl_enabled()) {
@@ -1272,7 +1277,8 @@ inline void launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cu
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, k, std::forward<Args>(args)...);
+    if (e != cudaSuccess && launch_error() == cudaSuccess) launch_error() = e;
   } else {
     k<<<grid, block, smem, st>>>(std::forward<Args>(args)...);
   }
@@ -1624,7 +1630,10 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
         break;
     }
   }
-  return fast_cuda(cudaGetLastError(), "fast-path launch", err);
+  const cudaError_t le = launch_error();
+  launch_error() = cudaSuccess;
+  const cudaError_t ge = cudaGetLastError();
+  return fast_cuda(le != cudaSuccess ? le : ge, "fast-path launch", err);
 }
 
 }  // namespace
