@@ -286,6 +286,35 @@ def run_ours(args):
         stage += np.array([ms_arr[i] for i in range(6)])
     stage /= reps
     clk = clocks.stop()
+    # single-field latency: forward + backward of one field on its own plan, device time
+    lat = None
+    try:
+        plan1 = cf.KRFFTPlan(spec, ops_s, precision=4, max_batch=1, path=cf.PATH_CENTERED)
+        x1 = f0[:1].contiguous()
+        F1 = torch.empty((1, plan1.n_spec), dtype=torch.complex64, device=dev)
+        o1 = torch.empty_like(x1)
+        h1 = plan1.handle
+
+        def one():
+            lib.cfft_forward(h1, ctypes.c_void_p(x1.data_ptr()), ctypes.c_void_p(F1.data_ptr()), 1, sptr)
+            lib.cfft_backward(h1, ctypes.c_void_p(F1.data_ptr()), ctypes.c_void_p(o1.data_ptr()), 1, sptr)
+
+        for _ in range(5):
+            one()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(20):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            one()
+            b.record(stream)
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        lat = {"value": float(np.median(ts)) * 1000.0, "unit": "us",
+               "note": "forward + backward of one field (B = 1 plan), device time by CUDA events, median of 20"}
+        plan1.close()
+    except Exception as exc:  # reported, never required
+        lat = {"error": repr(exc)}
     t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -346,8 +375,19 @@ def run_ours(args):
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     alg = algorithmic_bytes_per_field(M, plan.n_spec) * B
     achieved = alg / (ms_step * 1e-3) / 1e9
-    names = ["plane_fwd (fold+xy FFT)", "fft_z fwd", "recon", "inv_recon+expand", "fft_z inv", "plane_bwd (xy IFFT+unfold)"]
+    names = ["plane_fwd (fold+xy FFT)", "z FFT fwd (+ spectral gather when fused)", "spectral gather (separate kernel)",
+             "regroup + inverse gather", "expansion + inverse z FFT", "plane_bwd (xy IFFT+unfold)"]
     top = int(np.argmax(stage))
+    # The largest stage as a kernel roofline.  The plane kernels move the path's f0 bytes
+    # (4 M^3 per field, read by the forward fold, written by the backward unfold); the
+    # workspace they write or read is an intermediate and does not count.
+    kern = None
+    if top in (0, 5) and stage[top] > 0:
+        kb = 4.0 * float(np.prod(M)) * B
+        ka = kb / (stage[top] * 1e-3) / 1e9
+        kern = {"name": "k_plane_fwd_h" if top == 0 else "k_plane_bwd_h", "algorithmic_bytes": kb,
+                "ms": float(stage[top]), "achieved": ka, "frac": ka / hbm,
+                "note": "f0 bytes of the batch over the stage's CUDA-event time (chunks back to back on one stream)"}
     line = {
         "metric": METRIC, "value": us_field, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
@@ -360,7 +400,9 @@ def run_ours(args):
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_source": peak_src, "traffic": None,
                      "scope": "whole forward+backward per batch (6 launches per 64-field chunk); algorithmic bytes 2*(4*M^3 + 8*n_spec) per field",
-                     "stage_ms": {n: float(v) for n, v in zip(names, stage)}, "dominant_stage": names[top]},
+                     "stage_ms": {n: float(v) for n, v in zip(names, stage)}, "dominant_stage": names[top],
+                     "dominant_kernel": kern},
+        "latency_1field": lat,
         "gpu_launches": launches,
         "clocks": clk,
         "e2e": e2e,
