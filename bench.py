@@ -219,6 +219,23 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- ranks
+def max_over_ranks(value, device, dist=None, world=1):
+    """The largest value over all ranks (one float64 all-reduce MAX); the value itself
+    on a single rank.  Every rank must call it at the same point."""
+    import torch
+
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.item()
+
+
+def whole_job_us_per_field(ms_step, fields_per_rank, world):
+    """Whole-job time per field: the slowest rank's step time over all ranks' fields."""
+    return ms_step * 1000.0 / (fields_per_rank * world)
+
+
 # ----------------------------------------------------------------------------- our arm
 def run_ours(args):
     import torch
@@ -315,13 +332,10 @@ def run_ours(args):
         plan1.close()
     except Exception as exc:  # reported, never required
         lat = {"error": repr(exc)}
-    t = torch.tensor([ms_total], device=dev, dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = t.item()
+    ms_max = max_over_ranks(ms_total, dev, dist if world > 1 else None, world)
     ms_step = ms_max / args.steps
     fields_total = B * world
-    us_field = ms_step * 1000.0 / fields_total  # whole-job time per field
+    us_field = whole_job_us_per_field(ms_step, B, world)
     # e2e through the host-buffer C entry points with pinned host memory
     e2e = None
     if not args.no_e2e:
@@ -342,10 +356,7 @@ def run_ours(args):
         for _ in range(ke):
             e2e_step()
         e2e_s = (time.perf_counter() - t0) / ke
-        te = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
-        if world > 1:
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-        e2e_us = te.item() * 1e6 / fields_total
+        e2e_us = max_over_ranks(e2e_s, dev, dist if world > 1 else None, world) * 1e6 / fields_total
         fb = 4 * int(np.prod(M)) * B
         sb = 8 * plan.n_spec * B
         # Host-link bound of this step: each call is limited by its larger direction

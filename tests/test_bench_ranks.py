@@ -1,0 +1,52 @@
+"""Multi-rank host logic of bench.py on CPU (gloo, world size 2): the step time is the
+maximum over ranks, the whole-job value divides it by every rank's fields, and the
+reference arm prints only on rank 0."""
+import json
+import os
+import socket
+import subprocess
+import sys
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_max_over_ranks_two_gloo_ranks():
+    port = _free_port()
+    procs = []
+    for rank in range(2):
+        env = dict(os.environ, RANK=str(rank), WORLD_SIZE="2", MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, os.path.join(ROOT, "tests", "ranks_worker.py")], env=env,
+                                      stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    outs = []
+    for p in procs:
+        out, err = p.communicate(timeout=180)
+        assert p.returncode == 0, err
+        outs.append(json.loads(out.strip().splitlines()[-1]))
+    for o in outs:
+        assert o["ms"] == 5.0          # the slower rank's time, on both ranks
+        assert o["e2e"] == 0.5
+        assert abs(o["us_field"] - 0.5 * 1000.0 / 256) < 1e-12  # 5.0 ms / 10 steps over 2 x 128 fields
+
+
+def test_whole_job_value_single_rank():
+    spec_path = os.path.join(ROOT, "bench.py")
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("bench_under_test", spec_path)
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    assert bench.whole_job_us_per_field(0.16, 128, 1) == 0.16 * 1000.0 / 128
+
+
+def test_reference_arm_is_silent_on_other_ranks():
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "0"], env=env, capture_output=True, text=True, timeout=180, cwd=ROOT)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.strip() == ""
