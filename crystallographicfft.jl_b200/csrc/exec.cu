@@ -23,6 +23,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <mutex>
+#include <tuple>
 
 #include "device_common.cuh"
 #include "exec.h"
@@ -561,8 +562,14 @@ Status build_zrecon_units(Plan* p, std::string* err) {
     pts.insert(pts.end(), u.pts.begin(), u.pts.end());
   }
   if (ut.empty()) return Status::kOk;
-  CFFT_CUDA(cudaMalloc(&p->d_zr_units, ut.size() * sizeof(uint4)), "fused gather units");
-  CFFT_CUDA(cudaMalloc(&p->d_zr_pts, pts.size() * 4), "fused gather points");
+  // Plan-owned device tables: counted in the plan's device bytes, allocation failures
+  // reported as such (like the other plan buffers).
+  for (auto [ptr, bytes, what] : {std::tuple<void**, size_t, const char*>{&p->d_zr_units, ut.size() * sizeof(uint4), "fused gather units"},
+                                  std::tuple<void**, size_t, const char*>{&p->d_zr_pts, pts.size() * 4, "fused gather points"}}) {
+    const cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) { *err = cuda_msg(e, what); return Status::kAlloc; }
+    p->workspace_bytes += bytes;
+  }
   CFFT_CUDA(cudaMemcpy(p->d_zr_units, ut.data(), ut.size() * sizeof(uint4), cudaMemcpyHostToDevice), "upload units");
   CFFT_CUDA(cudaMemcpy(p->d_zr_pts, pts.data(), pts.size() * 4, cudaMemcpyHostToDevice), "upload unit points");
   p->zr_units = static_cast<int>(ut.size());
