@@ -104,9 +104,13 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------- inputs
-def symmetric_fields(cf, torch, ops_s, N, L, B, seed, device):
+def symmetric_fields(cf, torch, ops_s, N, L, B, seed, device, with_bases=False):
     """B seeded fields symmetric under ops_s (averaged over the group on the GPU),
-    returned as the stride-L subgrid batch (B, M3, M2, M1) in x-fastest layout."""
+    returned as the stride-L subgrid batch (B, M3, M2, M1) in x-fastest layout.
+    Each field is a seeded combination of a few symmetric full-grid bases; with
+    with_bases=True the bases (n_base, N3, N2, N1) and the coefficients (B, n_base)
+    are returned as well, so the FP64 truth of every field is the same combination of
+    the bases' FFTs."""
     g = torch.Generator(device=device).manual_seed(seed)
     n1, n2, n3 = N
     z, y, x = torch.meshgrid(torch.arange(n3, device=device), torch.arange(n2, device=device),
@@ -128,7 +132,19 @@ def symmetric_fields(cf, torch, ops_s, N, L, B, seed, device):
         bases.append((s / len(maps)).view(n3, n2, n1))
     coef = torch.randn(B, n_base, generator=g, device=device, dtype=torch.float64)
     sub = torch.stack([b[::L[2], ::L[1], ::L[0]] for b in bases])  # (n_base, M3, M2, M1)
-    return torch.einsum("bk,kzyx->bzyx", coef, sub).contiguous()
+    out = torch.einsum("bk,kzyx->bzyx", coef, sub).contiguous()
+    return (out, torch.stack(bases), coef) if with_bases else out
+
+
+def forward_truth_error(F, bases, coef, spec_idx):
+    """Max over fields of the forward spectrum's relative error against FP64 truth:
+    field b's spectrum on the spectral ASU is sum_k coef[b, k] fftn(base_k)[h]."""
+    u = bases.cpu().numpy()                                   # (n_base, N3, N2, N1)
+    T = np.stack([np.fft.fftn(x)[spec_idx[:, 2], spec_idx[:, 1], spec_idx[:, 0]] for x in u])
+    truth = coef.cpu().numpy() @ T                            # (B, n_spec)
+    got = F.cpu().numpy().astype(np.complex128)
+    err = np.max(np.abs(got - truth), axis=1) / np.max(np.abs(truth), axis=1)
+    return float(err.max()), int(np.argmax(err))
 
 
 # ----------------------------------------------------------------------------- reference arm
@@ -137,15 +153,14 @@ _REF = {}
 
 def _oracle_plans():
     """The FP64 CPU restatement of the reference's centred path for Im-3m 128^3
-    (plan_krfft_centered + plan_centered_ikrfft), built once per process."""
+    (plan_krfft_centered + plan_centered_ikrfft), built once per process from the
+    oracle alone (its own operations, shift and tables): the library is not loaded."""
     if not _REF:
         sys.path.insert(0, ROOT)
         from oracle import krfft_oracle as O
 
-        cf = load_package()
         N = (NEDGE,) * 3
-        _, ops_s = cf.find_optimal_shift(cf.get_ops(SG, 3, N), N)
-        oops = [O.SymOp(op.R, op.t) for op in ops_s]
+        _, oops = O.find_optimal_shift(O.get_ops(SG, 3, N), N)  # the oracle's own operation table
         spec = O.calc_spectral_asu(oops, 3, N)
         fwd = O.plan_krfft_centered(spec, oops)
         _REF.update(O=O, fwd=fwd, bwd=O.plan_centered_ikrfft(spec, oops, fwd),
@@ -258,7 +273,8 @@ def run_ours(args):
     B = args.batch
     plan = cf.KRFFTPlan(spec, ops_s, precision=4, max_batch=B, path=cf.PATH_CENTERED)
     M = plan.M
-    f0 = symmetric_fields(cf, torch, ops_s, N, plan.L, B, seed=1234 + rank, device=dev).float().contiguous()
+    f0, bases, coef = symmetric_fields(cf, torch, ops_s, N, plan.L, B, seed=1234 + rank, device=dev, with_bases=True)
+    f0 = f0.float().contiguous()
     F = torch.empty((B, plan.n_spec), dtype=torch.complex64, device=dev)
     out = torch.empty_like(f0)
     stream = torch.cuda.current_stream()
@@ -270,10 +286,16 @@ def run_ours(args):
         lib.cfft_forward(h, ctypes.c_void_p(f0.data_ptr()), ctypes.c_void_p(F.data_ptr()), B, sptr)
         lib.cfft_backward(h, ctypes.c_void_p(F.data_ptr()), ctypes.c_void_p(out.data_ptr()), B, sptr)
 
-    # correctness guard on the real workload: backward(forward(x)) == x
+    # correctness guard on the real workload: every field's forward spectrum against
+    # FP64 truth, and backward(forward(x)) == x
     step()
     torch.cuda.synchronize()
     rt_err = (torch.max(torch.abs(out - f0)) / torch.max(torch.abs(f0))).item()
+    fwd_err, fwd_worst = forward_truth_error(F, bases, coef, plan.spectral_asu()[0])
+    del bases
+    if fwd_err > 1e-5 or rt_err > 1e-5:
+        raise SystemExit(f"parity guard failed: forward max rel err {fwd_err:.3e} (field {fwd_worst}), "
+                         f"round trip {rt_err:.3e}")
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -407,7 +429,8 @@ def run_ours(args):
                    "group": SG, "N": NEDGE, "batch_per_gpu": B, "fields_total": fields_total,
                    "n_spec": plan.n_spec, "M": list(M), "channels": plan.n_channels,
                    "l2": "inputs larger than L2 (f0 batch %.0f MiB + output %.0f MiB)" % (4 * np.prod(M) * B / 2**20, 4 * np.prod(M) * B / 2**20),
-                   "parallelism": f"replicas x{world}", "roundtrip_rel_err": rt_err},
+                   "parallelism": f"replicas x{world}", "roundtrip_rel_err": rt_err,
+                   "forward_rel_err_vs_fp64": fwd_err},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                      "peak_source": peak_src, "traffic": None,
                      "scope": "whole forward+backward per batch (6 launches per 64-field chunk); algorithmic bytes 2*(4*M^3 + 8*n_spec) per field",

@@ -14,8 +14,7 @@ from .symmetry import (  # noqa: F401
 from .plans import (  # noqa: F401
     DiffusionSolver, KRFFTPlan, PATH_AUTO, PATH_CENTERED, PATH_M2, PATH_M2Q, PATH_M7, execute_centered_ikrfft,
     execute_centered_krfft, execute_m2_q, execute_m7_scft, plan_m2_q, plan_m7_scft, PATH_FULLGRID,
-    Diagonal, MatrixDiffusionSolver, apply_diffusion_operator, calc_gradient_term, calc_matrix_q,
-    calc_transform_matrix,
+    Diagonal, apply_diffusion_operator, calc_gradient_term, calc_matrix_q,
     CenteringPreFoldPlan, plan_centering_prefold, plan_krfft_prefold, execute_prefold_krfft,
     execute_centered_scft, execute_krfft, execute_m2_backward, execute_m2_scft, fft_reconstruct,
     fft_reconstruct_centered, fullgrid_to_subgrid, ifft_unrecon_centered, plan_centered_ikrfft, plan_centered_scft,

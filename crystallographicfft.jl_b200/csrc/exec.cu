@@ -1535,27 +1535,68 @@ constexpr size_t kNoAllocBytes = static_cast<size_t>(32) << 20;  // 32 MiB per d
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 std::mutex g_noalloc_mu;
 constexpr int kNoAllocMaxDevices = 64;
-unsigned char* g_noalloc_addr[kNoAllocMaxDevices] = {nullptr};
+// Per device: the context the set-up ran in and the array's device address there.  A
+// new primary context (after cudaDeviceReset) gets the set-up again.
+struct NoAllocSlot {
+  void* ctx = nullptr;
+  unsigned char* addr = nullptr;
+};
+NoAllocSlot g_noalloc_slot[kNoAllocMaxDevices];
 
 size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 
-// Device address of the static scratch for the current device, looked up once per
-// device (the array's name is only a host-side stand-in in host code).
+// The calling thread's current context (CUcontext), through the driver entry point so
+// the library does not link libcuda; null when the entry point is unavailable.
+void* current_context() {
+  using GetCtx = int (*)(void**);
+  static GetCtx fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<GetCtx>(p);
+  }();
+  void* ctx = nullptr;
+  if (fn && fn(&ctx) != 0) ctx = nullptr;
+  return ctx;
+}
+
+// Device address of the static scratch for the current device.  In host code the
+// array's name is only a host-side stand-in, so the address is looked up with the
+// device current, once per device and context, together with the kernels'
+// shared-memory attributes.
 Status noalloc_scratch_for_current_device(unsigned char** out, std::string* err) {
   int dev = 0;
   CFFT_CUDA(cudaGetDevice(&dev), "cudaGetDevice");
   if (dev < 0 || dev >= kNoAllocMaxDevices) { *err = "device ordinal above the supported range"; return Status::kUnsupported; }
+  void* ctx = current_context();  // null before the device's first runtime call
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_addr[dev]) {
+  NoAllocSlot& slot = g_noalloc_slot[dev];
+  if (!slot.addr || !ctx || slot.ctx != ctx) {
     void* ptr = nullptr;
     CFFT_CUDA(cudaGetSymbolAddress(&ptr, g_noalloc_scratch), "cudaGetSymbolAddress(static scratch)");
     set_smem_attrs<float>();
     set_smem_attrs<double>();
     CFFT_CUDA(cudaGetLastError(), "set shared-memory attributes");
-    g_noalloc_addr[dev] = static_cast<unsigned char*>(ptr);
+    slot.addr = static_cast<unsigned char*>(ptr);
+    slot.ctx = current_context();
   }
-  *out = g_noalloc_addr[dev];
+  *out = slot.addr;
   return Status::kOk;
+}
+
+// Geometry, twiddle tables and spectral points reach the static array as kernel
+// parameters: each launch carries up to kUploadWords words by value (parameter blocks
+// up to 32,764 bytes are accepted on sm_70 and newer since CUDA 12.1), so no host
+// buffer is referenced once the launch call has returned and nothing is staged
+// through host memory the call would have to allocate.
+constexpr int kUploadWords = 7680;
+struct UploadBlock {
+  uint32_t w[kUploadWords];
+};
+__global__ void k_noalloc_upload(uint32_t* __restrict__ dst, const __grid_constant__ UploadBlock blk, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = blk.w[i];
 }
 
 template <typename T>
@@ -1610,10 +1651,18 @@ Status noalloc_forward(const Plan* p, const T* f0, typename Cx<T>::type* F, int 
   unsigned char* base = nullptr;
   Status s = noalloc_scratch_for_current_device(&base, err);
   if (s != Status::kOk) return s;
-  // Pageable-source copies return once the host data is staged, so the locals may go.
-  CFFT_CUDA(cudaMemcpyAsync(base, &g, sizeof(g), cudaMemcpyHostToDevice, st), "upload geometry");
-  CFFT_CUDA(cudaMemcpyAsync(base + off_tab, tab.data(), tab.size(), cudaMemcpyHostToDevice, st), "upload tables");
-  CFFT_CUDA(cudaMemcpyAsync(base + off_spec, hp.data(), hp.size() * 4, cudaMemcpyHostToDevice, st), "upload points");
+  // [geometry | tables | spectral points] at their 256-byte aligned offsets, as words.
+  std::vector<uint32_t> blob(off_W / 4, 0u);
+  std::memcpy(blob.data(), &g, sizeof(g));
+  std::memcpy(blob.data() + off_tab / 4, tab.data(), tab.size());
+  std::memcpy(blob.data() + off_spec / 4, hp.data(), hp.size() * 4);
+  UploadBlock blk;
+  for (size_t w0 = 0; w0 < blob.size(); w0 += kUploadWords) {
+    const int n = static_cast<int>(std::min<size_t>(kUploadWords, blob.size() - w0));
+    std::memcpy(blk.w, blob.data() + w0, static_cast<size_t>(n) * 4);
+    k_noalloc_upload<<<(n + 255) / 256, 256, 0, st>>>(reinterpret_cast<uint32_t*>(base) + w0, blk, n);
+    ++g_launches;
+  }
   const DevGeom* dg = reinterpret_cast<const DevGeom*>(base);
   const C* dtab = reinterpret_cast<const C*>(base + off_tab);
   const uint32_t* dspec = reinterpret_cast<const uint32_t*>(base + off_spec);

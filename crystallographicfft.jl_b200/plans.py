@@ -545,88 +545,21 @@ def calc_matrix_q(indexing, kernel_func):
     return Diagonal([kernel_func(sym.get_k_vector(indexing, i)) for i in range(indexing.n_spec)])
 
 
-def calc_transform_matrix(real_pts, spec, direct_ops, N, shift):
-    """calc_transform_matrix (src/diffusion_solver.jl:30-64):
-    M[i, j] = (1/|G|) sum_g exp(2 pi i ((R*_g k_j).(r_i / N + s) - (R*_g k_j).t_g / N))."""
-    D = len(N)
-    Nv = np.asarray(N, dtype=np.float64)
-    K = np.array([sym.get_k_vector(spec, j) for j in range(spec.n_spec)], dtype=np.float64)  # (n_spec, D)
-    r = np.array([p.idx for p in real_pts], dtype=np.float64)                              # (n_real, D)
-    s = np.asarray(shift, dtype=np.float64)[:D]
-    M = np.zeros((len(real_pts), spec.n_spec), dtype=np.complex128)
-    for op, rop in zip(direct_ops, sym.dual_ops(direct_ops)):
-        kp = K @ rop.Rm.T.astype(np.float64)                          # (R* k) per spectral point
-        shift_ph = -(kp * (np.asarray(op.t, dtype=np.float64) / Nv)).sum(axis=1)
-        wave = (r / Nv) @ kp.T + (kp @ s)[None, :]
-        M += np.exp(2j * np.pi * (wave + shift_ph[None, :]))
-    return M / len(direct_ops)
-
-
-class MatrixDiffusionSolver:
-    """MatrixDiffusionSolver (src/diffusion_solver.jl:20-80): the dense symmetry-adapted
-    transform M (real ASU x spectral ASU) and its pseudo-inverse, built on the host; the
-    operator u <- real(M Q M^+ u) runs as two device GEMMs (batched over fields)."""
-
-    def __init__(self, real_asu, spec_asu, Q, M, M_inv):
-        self.real_asu, self.spec_asu, self.Q, self.M, self.M_inv = real_asu, spec_asu, Q, M, M_inv
-        self._dev = None
-
-    def _device(self, dtype):
-        torch = _torch()
-        cdt = torch.complex64 if dtype == torch.float32 else torch.complex128
-        if self._dev is None or self._dev[0] != cdt:
-            self._dev = (cdt, torch.as_tensor(self.M, device="cuda").to(cdt),
-                         torch.as_tensor(self.M_inv, device="cuda").to(cdt),
-                         torch.as_tensor(self.Q.diag, device="cuda").to(cdt))
-        return self._dev
-
-    def apply_diffusion_operator(self, u):
-        """apply_diffusion_operator! (src/diffusion_solver.jl:66-71) on (n_real,) or
-        (B, n_real) fields, in place (numpy arrays and CUDA tensors)."""
-        torch = _torch()
-        host = not _is_tensor(u)
-        t = torch.as_tensor(np.asarray(u), device="cuda") if host else u
-        _, M, Mi, q = self._device(t.dtype)
-        x = t.to(M.dtype).reshape(-1, M.shape[0]).T                    # (n_real, B)
-        y = torch.real(M @ (q[:, None] * (Mi @ x))).T.reshape(t.shape)
-        if host:
-            out = y.cpu().numpy()
-            if isinstance(u, np.ndarray):
-                np.copyto(u, out)
-            return out
-        t.copy_(y)
-        return t
-
-    def step(self, u, w, dt, n_steps=1):
-        torch = _torch()
-        for _ in range(n_steps):
-            e = np.exp(-np.asarray(w) * dt / 2) if not _is_tensor(u) else torch.exp(-w * dt / 2)
-            u *= e
-            self.apply_diffusion_operator(u)
-            u *= e
-        return u
-
-
-def plan_diffusion(N, lattice, sg_num, dim, ds, *, method="matrix", precision=8, max_batch=1):
-    """plan_diffusion (src/diffusion_solver.jl:165-252).  :matrix (the reference's default)
-    builds the dense solver on the real ASU; :qfused the M2Q subgrid solver.  The
-    reference's :krfft branch calls a plan_krfft(real_asu, spec_asu, ops) signature that
-    its own krfft.jl does not define, so it is refused here."""
+def plan_diffusion(N, lattice, sg_num, dim, ds, *, method="qfused", precision=8, max_batch=1):
+    """plan_diffusion (src/diffusion_solver.jl:165-252) on the device: :qfused, the M2Q
+    subgrid solver.  The reference's :matrix branch (a dense real-ASU x spectral-ASU
+    transform and its pseudo-inverse, src/diffusion_solver.jl:20-80) is a host-side
+    dense solve outside the KRFFT path this library accelerates, and is refused, as is
+    the :krfft branch, which calls a plan_krfft(real_asu, spec_asu, ops) signature that
+    the reference's own krfft.jl does not define."""
     method = str(method).lstrip(":")
-    ops = sym.get_ops(sg_num, dim, N)
-    shift, ops_s = sym.find_optimal_shift(ops, N)
-    spec = sym.calc_spectral_asu(ops_s, dim, N)
-    if method == "matrix":
-        from .asu import calc_asu
-
-        pts = calc_asu(tuple(N), ops_s)
-        Q = calc_matrix_q(spec, calc_gradient_term(N, ds, lattice))
-        M = calc_transform_matrix(pts, spec, ops_s, N, shift)
-        return MatrixDiffusionSolver(pts, spec, Q, M, np.linalg.pinv(M))
     if method == "qfused":
+        ops = sym.get_ops(sg_num, dim, N)
+        _, ops_s = sym.find_optimal_shift(ops, N)
+        spec = sym.calc_spectral_asu(ops_s, dim, N)
         return DiffusionSolver(KRFFTPlan(spec, ops_s, N=N, ds=ds, lattice=lattice, precision=precision,
                                          max_batch=max_batch, path=PATH_M2Q))
-    raise CFFTError(4, f"method {method!r}: supported are :matrix and :qfused")
+    raise CFFTError(4, f"method {method!r}: the device solver is :qfused (:matrix and :krfft are not built)")
 
 
 def step_diffusion(solver, u, w, dt, n_steps=1):

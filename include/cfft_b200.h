@@ -224,9 +224,11 @@ cfft_status cfft_subgrid_spectrum(cfft_plan plan, const void* f0, void* G0, int 
  * library holds it until the process exits), so a plan from cfft_plan_create_host is
  * enough; f0 and F are the caller's device buffers.  Any batch size is processed in
  * chunks that fit the array; a problem whose single field needs more scratch than
- * 32 MiB is rejected with CFFT_ERR_UNSUPPORTED.  The first call on each device looks
- * up the array's device address and sets kernel attributes, so make that first call
- * before any stream capture.  It never calls cudaMalloc or cudaFree.  All calls share
+ * 32 MiB is rejected with CFFT_ERR_UNSUPPORTED.  The first call on each device (and
+ * the first after the device's primary context was reset) looks up the array's
+ * device address and sets kernel attributes, so make that first call before any
+ * stream capture.  Geometry and tables reach the array as kernel parameters, with no
+ * host staging buffer.  It never calls cudaMalloc or cudaFree.  All calls share
  * the one array: calls that overlap on the GPU (other streams, other host threads)
  * race and must be serialised by the caller. */
 cfft_status cfft_forward_noalloc(cfft_plan plan, const void* f0, void* F, int batch, void* stream);

@@ -11,6 +11,10 @@ the reference's own tests pin the reference against FFTW (test/runtests.jl,
 test/test_centering_fold.jl, test/test_centered_*.jl, test/test_m2_*.jl,
 test/test_q_fused.jl), and (b) against the integer pins those tests hold
 (ASU sizes, centering classes, fold metadata, stripped op counts, auto-L).
+Its space-group operations come from its own Hall-symbol table (hall_groups.py),
+pinned to the reference's Crystalline-derived mirror/centring table
+(src/mirror_table.jl, tests/golden/mirror_table.json) and to the ITA group
+orders; nothing here loads the library under test.
 
 Layout conventions follow the reference: grids are indexed [x, y, z] with x
 fastest in memory (Julia column-major == numpy order='F'); the oracle stores
@@ -44,6 +48,14 @@ class SymOp:
     @property
     def tv(self):
         return np.array(self.t, dtype=np.int64)
+
+
+def get_ops(sg, dim, N):
+    """get_ops (src/symmetry_ops.jl:51-53) with convert_op (:38-46), from the oracle's own
+    Hall-symbol table (oracle/hall_groups.py), independent of the library's table."""
+    from . import hall_groups
+
+    return hall_groups.get_ops(sg, dim, tuple(N), SymOp)
 
 
 def make_op(R, t):

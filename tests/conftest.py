@@ -52,6 +52,18 @@ def to_oracle_ops(O, ops):
     return [O.SymOp(op.R, op.t) for op in ops]
 
 
+def oracle_group(cf, O, sg, N):
+    """Operations of group `sg` from the oracle's own Hall-symbol table, shifted by the
+    oracle's find_optimal_shift.  Returns (ops, ops_s) in the library's SymOp form (what
+    a caller hands the plan) and the oracle's shifted ops, so the field, the truth and
+    the plan all rest on operations that the library under test did not produce."""
+    dim = len(N)
+    oops = O.get_ops(sg, dim, N)
+    _, oops_s = O.find_optimal_shift(oops, N)
+    lib = lambda ops: [cf.SymOp(op.R, op.t) for op in ops]
+    return lib(oops), lib(oops_s), oops_s
+
+
 @pytest.fixture(scope="session")
 def prep(cf, O):
     """Per-group fixtures like test/runtests.jl:111-127: shifted ops, spectral ASU,
@@ -62,15 +74,26 @@ def prep(cf, O):
         key = (sg, tuple(N), seed)
         if key not in cache:
             dim = len(N)
-            ops = cf.get_ops(sg, dim, N)
-            _, ops_s = cf.find_optimal_shift(ops, N)
+            ops, ops_s, oops = oracle_group(cf, O, sg, N)
             spec = cf.calc_spectral_asu(ops_s, dim, N)
-            oops = to_oracle_ops(O, ops_s)
             u = O.make_symmetric(oops, N, seed=seed)
             cache[key] = dict(ops=ops, ops_s=ops_s, spec=spec, oops=oops, u=u)
         return cache[key]
 
     return get
+
+
+def oracle_shifted_ops(cf, sg, N):
+    """The library-form shifted operations of oracle_group (oracle imported here)."""
+    from oracle import krfft_oracle as O
+
+    return oracle_group(cf, O, sg, N)[1]
+
+
+def q_plan(cf, p, path, ds, lattice, **kw):
+    """An M2Q / M7 plan (plan_m2_q / plan_m7_scft, src/q_fused_krfft.jl:83,822) on the
+    prep fixture's (oracle) operations, so its Q tables compare with the oracle's."""
+    return cf.KRFFTPlan(p["spec"], p["ops_s"], N=p["spec"].N, ds=ds, lattice=lattice, path=path, **kw)
 
 
 def rel_err(a, b):

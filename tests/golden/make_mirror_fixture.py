@@ -7,8 +7,8 @@ centring vectors and -- per mirror/glide normal -- the translation of the first
 such operation in Crystalline's order.  The space-group tests compare the
 library's generated operation tables against it.
 
-Run in a checkout that has the reference mounted:
-    python tests/golden/make_mirror_fixture.py /root/reference/src/mirror_table.jl
+Run with the path of the reference's src/mirror_table.jl:
+    python tests/golden/make_mirror_fixture.py <reference checkout>/src/mirror_table.jl
 """
 import json
 import os
@@ -74,4 +74,6 @@ def main(path):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src/mirror_table.jl")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: make_mirror_fixture.py <reference checkout>/src/mirror_table.jl")
+    main(sys.argv[1])

@@ -4,7 +4,7 @@ src/pack_asu.jl) against the oracle and the reference's own checks (test/runtest
 import numpy as np
 import pytest
 
-from conftest import to_oracle_ops
+from conftest import to_oracle_ops, oracle_shifted_ops
 
 
 @pytest.mark.parametrize("sg,dim,N", [(6, 2, (8, 8)), (47, 3, (8, 8, 8)), (221, 3, (8, 8, 8)), (229, 3, (8, 8, 8)),
@@ -12,7 +12,7 @@ from conftest import to_oracle_ops
                                       (63, 3, (8, 8, 8)), (75, 3, (8, 8, 8)), (194, 3, (6, 6, 6)), (1, 3, (4, 4, 4))])
 def test_calc_asu_matches_oracle_and_covers_grid(cf, O, sg, dim, N):
     pts, shift = cf.calc_asu(sg, dim, N)
-    _, ops_s = cf.find_optimal_shift(cf.get_ops(sg, dim, N), N)
+    ops_s = oracle_shifted_ops(cf, sg, N)
     want = O.calc_asu_points(N, to_oracle_ops(O, ops_s))
     assert [(tuple(p.idx), tuple(p.depth), p.multiplicity) for p in pts] == want
     cover = set()
@@ -59,8 +59,7 @@ def test_interleaved_orbits_reference_cases(cf):
 
 def test_pack_asu_interleaved_gamma0(cf, O):
     N = (16, 16, 16)
-    ops = cf.get_ops(229, 3, N)
-    _, ops_s = cf.find_optimal_shift(ops, N)
+    ops_s = oracle_shifted_ops(cf, 229, N)
     u = O.make_symmetric(to_oracle_ops(O, ops_s), N, seed=4)
     c = cf.pack_asu_interleaved(u, N, ops_s, L=(2, 2, 2))
     (b,) = c.dim_blocks[3]

@@ -10,7 +10,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import rel_err
+from conftest import rel_err, oracle_shifted_ops
 
 pytestmark = pytest.mark.gpu
 
@@ -39,7 +39,7 @@ CASES = [
 
 def _plans(cf, sg, n, precision, batch):
     N = (n,) * 3
-    _, ops_s = cf.find_optimal_shift(cf.get_ops(sg, 3, N), N)
+    ops_s = oracle_shifted_ops(cf, sg, N)
     spec = cf.calc_spectral_asu(ops_s, 3, N)
     outer = os.environ.get("CFFT_CLUSTER")
     try:

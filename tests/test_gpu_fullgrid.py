@@ -11,7 +11,7 @@ The diffusion step on the full grid is checked against IFFT(K FFT(u))."""
 import numpy as np
 import pytest
 
-from conftest import rel_err, to_oracle_ops
+from conftest import rel_err, to_oracle_ops, oracle_shifted_ops
 
 pytestmark = pytest.mark.gpu
 
@@ -34,7 +34,7 @@ def from_dev(t, N):
 
 
 def _plan(cf, sg, N, precision):
-    _, ops_s = cf.find_optimal_shift(cf.get_ops(sg, 3, N), N)
+    ops_s = oracle_shifted_ops(cf, sg, N)
     spec = cf.calc_spectral_asu(ops_s, 3, N)
     plan = cf.plan_krfft_prefold(ops_s, N, precision=precision, ds=DS, lattice=LAT)
     return plan, ops_s, spec

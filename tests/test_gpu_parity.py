@@ -6,7 +6,7 @@ for transforms, 1e-10 absolute for the diffusion step); FP32 max relative error
 import numpy as np
 import pytest
 
-from conftest import rel_err
+from conftest import rel_err, oracle_shifted_ops
 
 pytestmark = pytest.mark.gpu
 
@@ -137,7 +137,7 @@ def test_host_pipeline_pieces(cf, B):
     # several pieces (ragged for 5 and 11 fields) whose copies overlap.  The host
     # path must agree with the device-tensor path on the same fields.
     N = (128, 128, 128)
-    _, ops_s = cf.find_optimal_shift(cf.get_ops(229, 3, N), N)
+    ops_s = oracle_shifted_ops(cf, 229, N)
     spec = cf.calc_spectral_asu(ops_s, 3, N)
     plan = cf.KRFFTPlan(spec, ops_s, precision=4, max_batch=B, ds=DS, lattice=LAT)
     g = torch.Generator(device="cuda:0").manual_seed(B)

@@ -4,7 +4,7 @@ test/runtests.jl:220-287 (M2Q vs full grid 1e-10, M7 vs M2Q 1e-12)."""
 import numpy as np
 import pytest
 
-from conftest import rel_err
+from conftest import q_plan, rel_err, oracle_shifted_ops
 
 pytestmark = pytest.mark.gpu
 
@@ -29,7 +29,7 @@ def from_dev(t, M):
 @pytest.mark.parametrize("sg", [47, 225, 229, 221, 227, 230, 63])
 def test_m2q_vs_oracle_and_fullgrid(cf, O, prep, sg):
     p = prep(sg, N16)
-    plan = cf.plan_m2_q(N16, sg, 3, DS, LAT)
+    plan = q_plan(cf, p, cf.PATH_M2Q, DS, LAT)
     oplan = O.plan_m2_q_ops(p["oops"], N16, DS, LAT)
     f0 = O.pack_stride(p["u"], plan.L)
     q = to_dev(f0, 8)
@@ -43,7 +43,7 @@ def test_m2q_vs_oracle_and_fullgrid(cf, O, prep, sg):
 @pytest.mark.parametrize("sg", [225, 229, 227, 230, 63])
 def test_m7_vs_m2q_and_oracle(cf, O, prep, sg):
     p = prep(sg, N16)
-    m7 = cf.plan_m7_scft(N16, sg, 3, DS, LAT)
+    m7 = q_plan(cf, p, cf.PATH_M7, DS, LAT)
     assert m7.centered
     oplan = O.plan_m2_q_ops(p["oops"], N16, DS, LAT)
     fold = O.plan_centering_fold(m7.centering, m7.M)
@@ -58,10 +58,10 @@ def test_m7_vs_m2q_and_oracle(cf, O, prep, sg):
 
 def test_q_step_fp32_batched_64(cf, O, prep):
     # Im-3m 64^3 (M7: H = 16) and Pm-3m 64^3 (M2Q: H = 32), FP32, three fields per call
-    for sg, make in ((229, cf.plan_m7_scft), (221, cf.plan_m2_q)):
+    for sg, path in ((229, cf.PATH_M7), (221, cf.PATH_M2Q)):
         N = (64, 64, 64)
         p = prep(sg, N, seed=5)
-        plan = make(N, sg, 3, DS, LAT, precision=4, max_batch=3)
+        plan = q_plan(cf, p, path, DS, LAT, precision=4, max_batch=3)
         oplan = O.plan_m2_q_ops(p["oops"], N, DS, LAT)
         f0 = O.pack_stride(p["u"], plan.L)
         fields = [f0, 0.5 * f0, -f0]
@@ -75,9 +75,9 @@ def test_q_step_fp32_batched_64(cf, O, prep):
 
 def test_q_update_kernel_equals_fresh_plan(cf, O, prep):
     p = prep(229, N16)
-    plan = cf.plan_m2_q(N16, 229, 3, DS, LAT)
+    plan = q_plan(cf, p, cf.PATH_M2Q, DS, LAT)
     plan.update_kernel(0.10, LAT)
-    fresh = cf.plan_m2_q(N16, 229, 3, 0.10, LAT)
+    fresh = q_plan(cf, p, cf.PATH_M2Q, 0.10, LAT)
     f0 = O.pack_stride(p["u"], plan.L)
     a, b = to_dev(f0, 8), to_dev(f0, 8)
     plan.scft_step(a)
@@ -90,7 +90,7 @@ def test_q_update_kernel_equals_fresh_plan(cf, O, prep):
 def test_q_step_diffusion_vs_oracle(cf, O, prep):
     # step_diffusion! (src/diffusion_solver.jl:254-267) with the Q-fused operator
     p = prep(225, N16)
-    plan = cf.plan_m7_scft(N16, 225, 3, DS, LAT)
+    plan = q_plan(cf, p, cf.PATH_M7, DS, LAT)
     oplan = O.plan_m2_q_ops(p["oops"], N16, DS, LAT)
     f0 = O.pack_stride(p["u"], plan.L)
     w = O.pack_stride(O.make_symmetric(p["oops"], N16, seed=99), plan.L)
@@ -103,24 +103,6 @@ def test_q_step_diffusion_vs_oracle(cf, O, prep):
     plan.close()
 
 
-def test_matrix_solver_step_on_device(cf):
-    # test/test_diffusion_solver.jl:42-50: the step runs and changes u; the device
-    # operator equals real(M Q M^+ u) on the host
-    solver = cf.plan_diffusion((8, 8), np.eye(2), 6, 2, 0.1)
-    rng = np.random.default_rng(1)
-    u = rng.random(len(solver.real_asu))
-    want = np.real(solver.M @ (solver.Q.diag * (solver.M_inv @ u)))
-    got = cf.apply_diffusion_operator(solver, u.copy())
-    assert np.max(np.abs(got - want)) < 1e-12
-    w = rng.random(len(solver.real_asu))
-    v = u.copy()
-    cf.step_diffusion(solver, v, w, 1.0)
-    assert not np.array_equal(v, u)
-    t = torch.tensor(np.stack([u, 2 * u]), device="cuda:0")
-    solver.apply_diffusion_operator(t)
-    assert np.max(np.abs(t.cpu().numpy() - np.stack([want, 2 * want]))) < 1e-12
-
-
 @pytest.mark.parametrize("sg,n", [(47, 16), (47, 32), (123, 16)])
 def test_qfused_solver_vs_fullgrid(cf, O, sg, n):
     # test/test_diffusion_solver.jl:52-135: f0 after the operator vs full-grid FFT -> K -> IFFT
@@ -129,7 +111,7 @@ def test_qfused_solver_vs_fullgrid(cf, O, sg, n):
     N = (n, n, n)
     solver = cf.plan_diffusion(N, LAT, sg, 3, 0.1, method=":qfused")
     plan = solver.plan
-    _, ops_s = cf.find_optimal_shift(cf.get_ops(sg, 3, N), N)
+    ops_s = oracle_shifted_ops(cf, sg, N)
     u = O.make_symmetric(to_oracle_ops(O, ops_s), N, seed=2)
     f0 = O.pack_stride(u, plan.L)
     q = to_dev(f0, 8)

@@ -16,7 +16,7 @@ DS = 0.05
 def test_shift_p2mm(cf, O):
     # test/runtests.jl:43-50
     N = (8, 8)
-    ops = to_oracle_ops(O, cf.get_ops(6, 2, N))
+    ops = O.get_ops(6, 2, N)
     shift, _ = O.find_optimal_shift(ops, N)
     assert np.allclose(shift, [0.5 / 8, 0.5 / 8])
     ok, _ = O.check_shift_invariance(ops, shift, N)
@@ -28,17 +28,17 @@ def test_centering_classification(cf, O):
     N = N16
     expect = {1: "P", 221: "P", 229: "I", 225: "F", 70: "F", 35: "C", 139: "I", 69: "F"}
     for sg, c in expect.items():
-        assert O.detect_centering_type(to_oracle_ops(O, cf.get_ops(sg, 3, N)), N) == c
+        assert O.detect_centering_type(O.get_ops(sg, 3, N), N) == c
 
 
 def test_strip_centering_counts(cf, O):
     # test/test_centering_prefold.jl:58-75
     N = N16
-    sub, Ns = O.strip_centering(to_oracle_ops(O, cf.get_ops(229, 3, N)), "I", N)
+    sub, Ns = O.strip_centering(O.get_ops(229, 3, N), "I", N)
     assert Ns == (8, 8, 8) and len(sub) == 48
-    sub, Ns = O.strip_centering(to_oracle_ops(O, cf.get_ops(225, 3, N)), "F", N)
+    sub, Ns = O.strip_centering(O.get_ops(225, 3, N), "F", N)
     assert Ns == (8, 8, 8) and len(sub) == 48
-    _, Ns = O.strip_centering(to_oracle_ops(O, cf.get_ops(35, 3, N)), "C", N)
+    _, Ns = O.strip_centering(O.get_ops(35, 3, N), "C", N)
     assert Ns == (8, 8, 16)
 
 
@@ -54,9 +54,9 @@ def test_fold_plan_metadata(O):
 
 def test_spectral_completeness(cf, O):
     # test/test_spectral_indexing.jl:40-70
-    spec = O.calc_spectral_asu(to_oracle_ops(O, cf.get_ops(1, 2, (4, 4))), 2, (4, 4))
+    spec = O.calc_spectral_asu(O.get_ops(1, 2, (4, 4)), 2, (4, 4))
     assert spec.n_spec == 16 and spec.mult.sum() == 16
-    spec = O.calc_spectral_asu(to_oracle_ops(O, cf.get_ops(6, 2, (16, 16))), 2, (16, 16))
+    spec = O.calc_spectral_asu(O.get_ops(6, 2, (16, 16)), 2, (16, 16))
     assert spec.mult.sum() == 256
     gamma = [i for i in range(spec.n_spec) if O.get_k_vector(spec, i) == [0, 0]]
     assert len(gamma) == 1 and spec.mult[gamma[0]] == 1
