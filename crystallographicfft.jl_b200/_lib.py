@@ -98,6 +98,8 @@ def _load():
         "cfft_profile_roundtrip": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p,
                                            ctypes.POINTER(ctypes.c_float), c_int_p]),
         "cfft_forward_noalloc": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+        "cfft_plan_device_status": (c_int, [c_void_p, c_int]),
+        "cfft_wait_selftest": (c_int, [c_void_p, ctypes.c_ulonglong, c_void_p]),
         "cfft_status_string": (ctypes.c_char_p, [c_int]),
         "cfft_last_error": (ctypes.c_char_p, []),
         "cfft_version": (c_int, []),

@@ -6,6 +6,7 @@
 
 #include "../../include/cfft_b200.h"
 #include "exec.h"
+#include "fast_api.h"
 
 using cfft::Status;
 
@@ -198,7 +199,15 @@ cfft_status cfft_plan_info(cfft_plan plan, cfft_info* info) {
   info->max_batch = p->max_batch;
   info->P = T.P;
   info->workspace_bytes = static_cast<int64_t>(p->workspace_bytes);
-  info->exec_path = (p->fast_h > 0 ? 1 : 0) | (p->reps_quad ? 2 : 0) | (p->cluster ? 4 : 0);
+  int tma = 0;
+  if (p->fast_h > 0 && !p->cluster && p->d_geom) {
+    bool fw = false, fwe = false, bw = false;
+    if (p->precision == 8) cfft::fast_tma_planes_f64(p->fast_h, p->cent_type, &fw, &fwe, &bw);
+    else cfft::fast_tma_planes_f32(p->fast_h, p->cent_type, &fw, &fwe, &bw);
+    tma = (fw ? 8 : 0) | (bw ? 16 : 0);
+  }
+  info->exec_path = (p->fast_h > 0 ? 1 : 0) | (p->reps_quad ? 2 : 0) | (p->cluster ? 4 : 0) | tma |
+                    (p->reps_wide && !p->cluster ? 32 : 0);
   info->chunk = p->chunk;
   info->lanes = p->lanes;
   return CFFT_OK;
@@ -329,6 +338,20 @@ cfft_status cfft_update_kernel(cfft_plan plan, double ds, const double* lattice)
     Status s_ = (expr);                                               \
     return ret(s_, err);                                              \
   } while (0)
+
+cfft_status cfft_plan_device_status(cfft_plan plan, int clear) {
+  if (!plan) return ret(Status::kInvalid, "null plan");
+  std::string err;
+  const Status s = cfft::plan_device_status(reinterpret_cast<cfft::Plan*>(plan), clear != 0, &err);
+  return ret(s, err);
+}
+
+cfft_status cfft_wait_selftest(cfft_plan plan, unsigned long long timeout_ns, void* stream) {
+  if (!plan) return ret(Status::kInvalid, "null plan");
+  std::string err;
+  const Status s = cfft::plan_wait_selftest(reinterpret_cast<cfft::Plan*>(plan), timeout_ns, stream, &err);
+  return ret(s, err);
+}
 
 cfft_status cfft_forward(cfft_plan plan, const void* f0, void* F, int batch, void* stream) {
   CFFT_EXEC(cfft::exec_forward(p, f0, F, batch, stream, &err));

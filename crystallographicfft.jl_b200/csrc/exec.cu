@@ -602,9 +602,12 @@ Status launch_stage(Plan* p, int stage, const T* f0, typename Cx<T>::type* F, co
     a.cent_type = p->cent_type; a.d = T_.d;
     a.n_spec = static_cast<int>(T_.spec.size()); a.n_orbits = static_cast<int>(T_.orbit_rep.size());
     a.use_K = use_K; a.rep_diag8 = p->rep_diag8; a.rep_perm = p->rep_perm; a.reps_quad = p->reps_quad;
+    a.reps_wide = p->reps_wide && !p->cluster;
     a.zr_units = p->d_zr_units; a.zr_pts = p->d_zr_pts; a.zr_n_units = p->zr_units;
     a.cluster = p->cluster;
     a.cluster_ctas = p->cluster_ctas;
+    a.status = p->d_status;
+    a.timeout_ns = p->timeout_ns;
     if (q_step) {  // stage 4: Q-multiply + inverse z FFT into the Q workspace; stage 5 reads it
       a.q_step = true;
       a.QT = p->d_qt;
@@ -749,6 +752,10 @@ Status profile_roundtrip(Plan* p, const T* f0, typename Cx<T>::type* F, T* f0_ou
 
 Status check_batch(const Plan* p, int B, std::string* err) {
   if (B < 1 || B > p->max_batch) { *err = "batch must be in [1, max_batch]"; return Status::kInvalid; }
+  if (p->h_status && *static_cast<volatile int*>(p->h_status) != 0) {
+    *err = "a bounded device wait of an earlier call on this plan gave up (cfft_plan_device_status clears it)";
+    return Status::kTimeout;
+  }
   return Status::kOk;
 }
 
@@ -947,7 +954,12 @@ Status plan_device_init(Plan* p, std::string* err) {
     // The quad path reads the expansion entries packed in 32 bits (orbit | phase << 21).
     if ((st = alloc(&p->d_expand, expand.size() * (p->reps_quad ? 4 : sizeof(int2)), "expansion table")) != Status::kOk)
       return st;
-    const size_t chunk4 = (chunk + 3) / 4 * 4;  // quads of fields
+    // Wide groups (16 FP32 / 8 FP64 fields per line) once a chunk fills one group; the
+    // fused cluster kernels read the quad layout, so CFFT_CLUSTER keeps quads.
+    const size_t gw = 128 / cs;
+    const char* wide_env = std::getenv("CFFT_WIDE");
+    p->reps_wide = p->reps_quad && chunk >= gw && !(wide_env && wide_env[0] == '0') && !std::getenv("CFFT_CLUSTER");
+    const size_t chunk4 = p->reps_wide ? (chunk + gw - 1) / gw * gw : (chunk + 3) / 4 * 4;  // whole groups of fields
     p->g0r_lane_bytes = (((p->reps_quad ? chunk4 : chunk + 1) * T.orbit_rep.size() * cs + 255) / 256) * 256;
     if ((st = alloc(&p->d_g0r, p->lanes * p->g0r_lane_bytes, "representative workspace")) != Status::kOk) return st;
     if (p->reps_quad) {
@@ -1047,6 +1059,16 @@ Status plan_device_init(Plan* p, std::string* err) {
     }
   }
   if (p->cluster) p->zrecon = false;  // the cluster forward writes the z-fastest workspace for stage 2
+  {
+    void* hs = nullptr;
+    CFFT_CUDA(cudaHostAlloc(&hs, sizeof(int), cudaHostAllocMapped), "status word");
+    p->h_status = static_cast<int*>(hs);
+    *p->h_status = 0;
+    void* ds = nullptr;
+    CFFT_CUDA(cudaHostGetDevicePointer(&ds, hs, 0), "status word device address");
+    p->d_status = static_cast<int*>(ds);
+    if (const char* e = std::getenv("CFFT_WAIT_TIMEOUT_NS")) p->timeout_ns = std::strtoull(e, nullptr, 10);
+  }
   cudaStream_t s;
   CFFT_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "create stream");
   p->own_stream = s;
@@ -1107,6 +1129,7 @@ void plan_device_free(Plan* p) {
                    &p->d_qt, &p->d_gt, &p->d_work_Q, &p->d_zr_units, &p->d_zr_pts};
   for (void** b : bufs)
     if (*b) { cudaFree(*b); *b = nullptr; }
+  if (p->h_status) { cudaFreeHost(p->h_status); p->h_status = nullptr; p->d_status = nullptr; }
   for (auto& gph : p->step_graphs) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(gph.exec));
   p->step_graphs.clear();
   if (p->own_stream) { cudaStreamDestroy(static_cast<cudaStream_t>(p->own_stream)); p->own_stream = nullptr; }
@@ -1120,6 +1143,20 @@ void plan_device_free(Plan* p) {
   for (int i = 0; i < Plan::kHostPieces; ++i)
     for (void** ep : {&p->ev_in[i], &p->ev_done[i]})
       if (*ep) { cudaEventDestroy(static_cast<cudaEvent_t>(*ep)); *ep = nullptr; }
+}
+
+Status plan_device_status(Plan* p, bool clear, std::string* err) {
+  if (!p->h_status) { *err = "host-only plan: no device state"; return Status::kInvalid; }
+  volatile int* hs = p->h_status;
+  const int v = *hs;
+  if (clear) *hs = 0;
+  if (v != 0) { *err = "a bounded device wait gave up"; return Status::kTimeout; }
+  return Status::kOk;
+}
+
+Status plan_wait_selftest(Plan* p, unsigned long long timeout_ns, void* stream, std::string* err) {
+  if (!p->d_status) { *err = "host-only plan: no device state"; return Status::kInvalid; }
+  return fast_wait_selftest(timeout_ns, p->d_status, stream, err);
 }
 
 Status exec_forward(Plan* p, const void* f0, void* F, int B, void* stream, std::string* err) {

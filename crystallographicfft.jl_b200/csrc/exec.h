@@ -59,6 +59,7 @@ struct Plan {
   bool rep_perm = false;        // representative ops are signed permutations
   bool rep_diag8 = false;       // representative ops are the 8 diagonal sign matrices
   bool reps_quad = false;       // packed alias rows; fields gathered and expanded in quads
+  bool reps_wide = false;       // the same in groups of 128 / sizeof(complex) fields (one line per point)
   bool zrecon = false;          // forward z FFT fused with the diagonal-sign gather (stage 6)
   int zr_units = 0;             // units of the fused kernel (channel + mirrored row pair)
   bool cluster = false;         // fused cluster kernels: fold+xyz FFT and expand+xyz IFFT+unfold
@@ -82,6 +83,11 @@ struct Plan {
   void* d_gt = nullptr;         // d x n_ch x H^3 int32 workspace index (-1: extinct class)
   void* d_work_Q = nullptr;     // lanes x channel workspace (Q-multiply output)
   int cluster_ctas = 8;         // CTAs per cluster
+  // Status word of the bounded device waits (mapped pinned host memory, so the host
+  // reads it without a synchronisation): 0, or CFFT_ERR_TIMEOUT once a wait ran out.
+  int* h_status = nullptr;
+  int* d_status = nullptr;
+  unsigned long long timeout_ns = 1000000000ull;  // limit of one device wait (CFFT_WAIT_TIMEOUT_NS)
   size_t smem_xy = 0, smem_z = 0;
 };
 
@@ -114,6 +120,11 @@ Status exec_profile_roundtrip(Plan* p, const void* f0, void* F, void* f0_out, in
                               int* n, std::string* err);
 
 Status exec_forward_noalloc(const Plan* p, const void* f0, void* F, int B, void* stream, std::string* err);
+// Status of the plan's bounded device waits (after the caller synchronised): kOk or
+// kTimeout; `clear` resets it.
+Status plan_device_status(Plan* p, bool clear, std::string* err);
+// Bounded-wait self-test on the plan's status word (see k_wait_selftest).
+Status plan_wait_selftest(Plan* p, unsigned long long timeout_ns, void* stream, std::string* err);
 
 int64_t launch_count(bool reset);
 

@@ -32,6 +32,7 @@ struct FastArgs {
   int stage = 0, nb = 0, H = 0, n_ch = 1, centered = 0, cent_type = 0, d = 1;
   int n_spec = 0, n_orbits = 0;
   bool use_K = false, rep_diag8 = false, rep_perm = false, reps_quad = false;
+  bool reps_wide = false;  // backward gather in groups of 128 / sizeof(complex) fields
   // Stage 6 (fused z FFT + diagonal-sign gather): unit table and spectral points.
   const void* zr_units = nullptr;
   const void* zr_pts = nullptr;
@@ -44,6 +45,10 @@ struct FastArgs {
   const void* GT = nullptr;   // d x n_ch x H^3 int32 workspace indices (-1: extinct)
   void* W2 = nullptr;
   void* stream = nullptr;
+  // bounded device waits of the persistent bulk-copy kernels: limit, and the plan's
+  // status word that a wait which runs out sets to CFFT_ERR_TIMEOUT
+  unsigned long long timeout_ns = 1000000000ull;
+  int* status = nullptr;
 };
 
 // Stages 0 and 5 (plane kernels) and stages 1-4 (z FFTs, gathers).
@@ -55,6 +60,12 @@ Status fast_other_f64(const FastArgs& a, std::string* err);
 // backward kernels for channel edge H and centring type ct (0 if they cannot run).
 Status fast_cluster_probe_f32(int H, int ct, int kc, int* max_clusters, std::string* err);
 Status fast_cluster_probe_f64(int H, int ct, int kc, int* max_clusters, std::string* err);
+// Whether the persistent bulk-copy plane kernels serve channel edge H and centring
+// type ct (forward without / with interaction factors, backward).
+void fast_tma_planes_f32(int H, int ct, bool* fwd, bool* fwd_e, bool* bwd);
+void fast_tma_planes_f64(int H, int ct, bool* fwd, bool* fwd_e, bool* bwd);
+// Launches the bounded-wait self-test kernel (k_wait_selftest) on `stream`.
+Status fast_wait_selftest(unsigned long long timeout_ns, int* status, void* stream, std::string* err);
 // Per-device set-up of each unit: constant-memory twiddles and shared-memory limits.
 Status fast_init_planes_f32(std::string* err);
 Status fast_init_planes_f64(std::string* err);

@@ -37,6 +37,13 @@ __device__ __forceinline__ void pdl_enter() {
   asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
 }
 
+// Drop one 128-byte L2 line without writing it back (its contents become undefined).
+// Used on channel-workspace lines that have been read for the last time, so the dirty
+// intermediate never travels to HBM.
+__device__ __forceinline__ void discard_l2_line(const void* p) {
+  asm volatile("discard.global.L2 [%0], 128;\n" ::"l"(p) : "memory");
+}
+
 constexpr int kTwOff4 = 0, kTwOff6 = 4, kTwOff8 = 10, kTwOff12 = 18, kTwOff16 = 30, kTwOff24 = 46,
               kTwOff32 = 70, kTwOff48 = 102, kTwTotal = 150;
 __constant__ float2 c_tw_f[kTwTotal];
@@ -473,6 +480,8 @@ __global__ void k_plane_bwd_h(const DevGeom* __restrict__ g, const typename Cx<T
   const T* Ea = USE_E ? E + static_cast<size_t>(fa) * mvol : nullptr;
   unfold_plane<T, H, CT, VEC>(g, tables, buf, dsta, dsta + mvol, Ea, USE_E ? Ea + mvol : nullptr, has_b, USE_E, iz, tid, nth);
 }
+
+#include "tma_planes.cuh"
 
 // ---------------------------------------------------------------- cluster kernels
 // One thread-block cluster of KC CTAs holds the whole channel volume of one workspace
@@ -921,6 +930,18 @@ __global__ void k_fft_z_recon_diag8(const DevGeom* __restrict__ g, const typenam
     }
   }
   __syncthreads();
+  // Every workspace row (slot, c, z, y) of this unit is read by this CTA alone and never
+  // again: drop its lines from L2 (rows that fill whole 128-byte lines only).
+  if constexpr ((H * sizeof(C)) % 128 == 0) {
+    constexpr int LPR = static_cast<int>(H * sizeof(C) / 128);
+    for (int i = tid; i < SL * 2 * H * LPR; i += nth) {
+      const int li = i % LPR, z = (i / LPR) % H, r = (i / (LPR * H)) & 1, k = i / (LPR * H * 2);
+      const int slot = slot0 + k, y = r ? yb : ya;
+      if (slot < nslots && y >= 0)
+        discard_l2_line(reinterpret_cast<const char*>(W + (static_cast<size_t>(slot) * nch + c) * HV +
+                                                      static_cast<size_t>(z) * H * H + y * H) + li * 128);
+    }
+  }
   const bool cen = g->centered;
   const int M = cen ? 2 * H : H;
   const int ls = cen ? 1 : 0;
@@ -1205,6 +1226,125 @@ __global__ void k_expand4_ifft_z_h(const DevGeom* __restrict__ g, const typename
   for (int z = 0; z < H; ++z) dst[z * H * H] = v[z];
 }
 
+// ---------------------------------------------------------------- wide backward gather
+// Field groups of GW = 128 / sizeof(complex) fields (16 in FP32, 8 in FP64): the
+// spectrum of a group keeps the GW values of one spectral point in one 128-byte line,
+// FT[g][s][k] = F[GW g + k][s], and the orbit representatives of a group keep their
+// GW / 2 workspace-slot inputs in one line, G0P[g][o][j] = X of slot GW/2 g + j.  Each
+// random gather of a warp then fetches whole lines that serve GW fields, a quarter of
+// the L1 wavefronts per useful byte of the quad layout.
+template <typename C> constexpr int wide_fields() { return static_cast<int>(128 / sizeof(C)); }
+constexpr int kWideTile = 128;  // spectral points per CTA of the regroup
+
+// Regroup of the spectra of nb fields into groups of GW: a CTA moves a tile of
+// kWideTile spectral points x GW fields through shared memory (row stride GW + 1, so
+// both phases are free of bank conflicts); reads are coalesced along each field's
+// row, writes are whole lines.  Fields past nb are zero.
+template <typename T>
+__global__ void __launch_bounds__(256) k_group_spectra_w(const typename Cx<T>::type* __restrict__ F,
+                                                         typename Cx<T>::type* __restrict__ FT, int ns, int nb) {
+  pdl_enter();
+  using C = typename Cx<T>::type;
+  constexpr int GW = wide_fields<C>(), SP = kWideTile, RS = GW + 1;
+  __shared__ C tile[SP * RS];
+  const int s0 = blockIdx.x * SP, gq = blockIdx.y;
+  const int np = min(SP, ns - s0);
+  const C z = mk<C>(static_cast<T>(0), static_cast<T>(0));
+  for (int e = threadIdx.x; e < SP * GW; e += blockDim.x) {
+    const int f = e / SP, i = e % SP;
+    const int field = gq * GW + f;
+    tile[i * RS + f] = (i < np && field < nb) ? __ldg(F + static_cast<size_t>(field) * ns + s0 + i) : z;
+  }
+  __syncthreads();
+  C* out = FT + (static_cast<size_t>(gq) * ns + s0) * GW;
+  for (int e = threadIdx.x; e < np * GW; e += blockDim.x) out[e] = tile[(e / GW) * RS + (e % GW)];
+}
+
+// Backward inverse reconstruction for a group of GW fields: as k_inv_recon_quad, with
+// GW / 2 lanes per orbit; lane j reads fields GW g + 2j and GW g + 2j + 1 (two
+// consecutive complex of the spectral point's line), so the lanes of an orbit read
+// each tap's line whole, and stores the slot input X = G_a + i G_b as G0P[g][o][j].
+template <typename T, int D>
+__global__ void __launch_bounds__(256)
+k_inv_recon_w(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+              const uint32_t* __restrict__ inv_pk, const typename Cx<T>::type* __restrict__ FT,
+              typename Cx<T>::type* __restrict__ G0P) {
+  pdl_enter();
+  using C = typename Cx<T>::type;
+  constexpr int GW = wide_fields<C>(), L = GW / 2;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int no = g->n_orbits;
+  const int o = t / L, j = t % L;
+  if (o >= no) return;
+  const int gq = blockIdx.y;
+  const C* ft = FT + static_cast<size_t>(gq) * g->n_spec * GW + 2 * j;
+  const C* ph = tables + g->ph_off;
+  uint32_t e[D];
+  load_alias_row<D>(inv_pk, o, e);
+  C v[D][2];
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    const uint32_t sp = e[a] & 0xFFFFFu;
+    const C* src = ft + static_cast<size_t>(sp ? sp - 1 : 0) * GW;
+    if constexpr (sizeof(C) == 8) {
+      const float4 u = __ldg(reinterpret_cast<const float4*>(src));
+      v[a][0] = mk<C>(u.x, u.y);
+      v[a][1] = mk<C>(u.z, u.w);
+    } else {
+      v[a][0] = __ldg(src);
+      v[a][1] = __ldg(src + 1);
+    }
+  }
+  const T zero = static_cast<T>(0);
+  T re[2] = {zero, zero}, im[2] = {zero, zero};
+#pragma unroll
+  for (int a = 0; a < D; ++a) {
+    C w = ph[e[a] >> 21];
+    if ((e[a] & 0xFFFFFu) == 0) w = mk<C>(zero, zero);
+    const T sg = ((e[a] >> 20) & 1u) ? static_cast<T>(-1) : static_cast<T>(1);
+    const T cA = w.x, cB = sg * w.y, cC = sg * w.x, cD = -w.y;
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+      re[f] = fma(v[a][f].x, cA, fma(v[a][f].y, cB, re[f]));
+      im[f] = fma(v[a][f].y, cC, fma(v[a][f].x, cD, im[f]));
+    }
+  }
+  const T inv_d = static_cast<T>(1.0 / static_cast<double>(D));
+  G0P[(static_cast<size_t>(gq) * no + o) * L + j] = mk<C>(inv_d * (re[0] - im[1]), inv_d * (im[0] + re[1]));
+}
+
+// Backward orbit expansion + inverse z FFT for a group of GW fields (GW / 2 slots): a
+// CTA takes one (y, c, group); thread (x, j) builds the z line of slot GW/2 g + j at
+// (y, x) from the packed expansion entries and G0P[g][orbit][j] (the GW / 2 lanes of
+// one x read one orbit's line), transforms it in registers and stores it to
+// W[slot][c][z][y][x].  Launched with GW / 2 * H threads.
+template <typename T, int H>
+__global__ void __launch_bounds__(wide_fields<typename Cx<T>::type>() / 2 * H)
+k_expand_w_ifft_z_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ tables,
+                    const uint32_t* __restrict__ ETP, const typename Cx<T>::type* __restrict__ G0P,
+                    typename Cx<T>::type* __restrict__ W, int nfields) {
+  pdl_enter();
+  using C = typename Cx<T>::type;
+  constexpr int GW = wide_fields<C>(), L = GW / 2, HV = H * H * H;
+  const int y = blockIdx.x, c = blockIdx.y, gq = blockIdx.z;
+  const int j = threadIdx.x % L, x = threadIdx.x / L;
+  const int slot = gq * L + j;
+  if (2 * slot >= nfields) return;
+  const uint32_t* et = ETP + static_cast<size_t>(c) * HV + y * H + x;
+  const C* rp = G0P + static_cast<size_t>(gq) * g->n_orbits * L + j;
+  const C* ph = tables + g->ph_off;
+  C v[H];
+#pragma unroll
+  for (int z = 0; z < H; ++z) {
+    const uint32_t t = __ldg(et + z * H * H);
+    v[z] = cmulc(__ldg(rp + static_cast<size_t>(L) * (t & 0x1FFFFFu)), ph[t >> 21]);
+  }
+  reg_fft<C, true, H>(v);
+  C* dst = W + (static_cast<size_t>(slot) * g->n_ch + c) * HV + y * H + x;
+#pragma unroll
+  for (int z = 0; z < H; ++z) dst[z * H * H] = v[z];
+}
+
 // Q-matrix diffusion step (execute_m2_q! / execute_m7_scft!, src/q_fused_krfft.jl:553-667,
 // 870-895): for every channel point (c, x, y, z) of a slot, q its subgrid position,
 //   Y'(q) = sum_b Q_b(q) G0(R_b^T q mod M)
@@ -1282,6 +1422,42 @@ inline void launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cu
   } else {
     k<<<grid, block, smem, st>>>(std::forward<Args>(args)...);
   }
+}
+
+// Persistent bulk-copy plane kernels (tma_planes.cuh): on unless CFFT_TMA=0.  They
+// serve centred plans with H >= 16 whose per-group stage and buffer fit at least two
+// groups into one CTA's shared memory.
+inline bool tma_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("CFFT_TMA");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+template <typename T, int H, int CT, bool USE_E>
+constexpr bool fwd_tma_fits() {
+  if constexpr (CT == 0 || H < 16 || H % (16 / static_cast<int>(sizeof(T))) != 0) return false;
+  else return tma_groups<FwdTmaShape<T, H, CT, USE_E>>() >= 2;
+}
+template <typename T, int H, int CT>
+constexpr bool bwd_tma_fits() {
+  if constexpr (CT == 0 || H < 16 || H % (16 / static_cast<int>(sizeof(T))) != 0) return false;
+  else return tma_groups<BwdTmaShape<T, H, CT>>() >= 2;
+}
+// Persistent grid of a bulk-copy plane kernel: every SM's resident CTAs, or fewer when
+// the tasks run out (occupancy looked up once per kernel instantiation).
+template <typename K>
+int tma_grid(K kernel, int threads, size_t smem, int ntasks, int ng) {
+  static int per_sm = -1, sms = 0;
+  if (per_sm < 0) {
+    int dev = 0, occ = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem) != cudaSuccess) occ = 1;
+    per_sm = occ < 1 ? 1 : occ;
+  }
+  const int need = (ntasks + ng - 1) / ng;
+  return std::max(1, std::min(need, per_sm * sms));
 }
 
 // Workspace slots per CTA of the fused z FFT + gather: 4, or 2 with CFFT_ZR_SLOTS=2
@@ -1427,6 +1603,30 @@ Status fast_unit_init(std::string* err) {
           CFFT_FOR_CT(ct, {
             cudaFuncSetAttribute(k_plane_fwd_h<T, HH, CTT>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
             cudaFuncSetAttribute(k_plane_bwd_h<T, HH, CTT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kMaxDynSmemFast);
+            // The bulk-copy kernels also hold a little static shared memory, so their
+            // dynamic limit is their exact need; a refusal is reported.
+            cudaError_t te = cudaSuccess;
+            if constexpr (fwd_tma_fits<T, HH, CTT, false>()) {
+              using SH = FwdTmaShape<T, HH, CTT, false>;
+              constexpr int NG = tma_groups<SH>();
+              te = cudaFuncSetAttribute(k_plane_fwd_tma<T, HH, CTT, NG, false>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(NG * SH::group));
+            }
+            if constexpr (fwd_tma_fits<T, HH, CTT, true>()) {
+              using SH = FwdTmaShape<T, HH, CTT, true>;
+              constexpr int NG = tma_groups<SH>();
+              if (te == cudaSuccess)
+                te = cudaFuncSetAttribute(k_plane_fwd_tma<T, HH, CTT, NG, true>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(NG * SH::group));
+            }
+            if constexpr (bwd_tma_fits<T, HH, CTT>()) {
+              using SH = BwdTmaShape<T, HH, CTT>;
+              constexpr int NG = tma_groups<SH>();
+              if (te == cudaSuccess)
+                te = cudaFuncSetAttribute(k_plane_bwd_tma<T, HH, CTT, NG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          static_cast<int>(NG * SH::group));
+            }
+            if (te != cudaSuccess) return fast_cuda(te, "bulk-copy plane kernel shared-memory attribute", err);
             cluster_attrs<T, HH, CTT, 8>();
             cluster_attrs<T, HH, CTT, 16>();
           });
@@ -1473,6 +1673,19 @@ Status fast_unit_cluster_probe(int H, int ct, int kc, int* max_clusters, std::st
   return Status::kOk;
 }
 
+template <typename T>
+void fast_unit_tma_planes(int H, int ct, bool* fwd, bool* fwd_e, bool* bwd) {
+  *fwd = *fwd_e = *bwd = false;
+  if (!tma_enabled() || !fast_size_ok(H, sizeof(T))) return;
+  CFFT_FOR_H(H, {
+    CFFT_FOR_CT(ct, {
+      *fwd = fwd_tma_fits<T, HH, CTT, false>();
+      *fwd_e = fwd_tma_fits<T, HH, CTT, true>();
+      *bwd = bwd_tma_fits<T, HH, CTT>();
+    });
+  });
+}
+
 // One fast-path stage for `a.nb` fields (two per workspace slot).
 template <typename T, int GROUP>
 Status fast_unit_launch(const FastArgs& a, std::string* err) {
@@ -1514,16 +1727,55 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
     }
     const int thr_plane = std::max(128, ((nch * H + 31) / 32) * 32);
     const size_t smem_plane = static_cast<size_t>(nch) * H * (H + 1) * cs;
+    const int ntasks = nslots * H;
+    auto al16 = [](const void* p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+    const bool tma = tma_enabled() && al16(f0) && al16(E) && al16(f0_out) && al16(W);
     if (a.stage == 0) {
       CFFT_FOR_H(H, {
         CFFT_FOR_CT(a.cent_type, {
-          launch_k(k_plane_fwd_h<T, HH, CTT>, dim3(H, nslots), thr_plane, smem_plane, st, g, tab, f0, E, W, nb);
+          bool done = false;
+          if (tma && E == nullptr) {
+            if constexpr (fwd_tma_fits<T, HH, CTT, false>()) {
+              using SH = FwdTmaShape<T, HH, CTT, false>;
+              constexpr int NG = tma_groups<SH>();
+              auto* k = k_plane_fwd_tma<T, HH, CTT, NG, false>;
+              const int grid = tma_grid(k, NG * SH::threads, NG * SH::group, ntasks, NG);
+              launch_k(k, dim3(grid), NG * SH::threads, NG * SH::group, st, g, tab, f0, E, W, nb, ntasks,
+                       static_cast<uint64_t>(a.timeout_ns), a.status);
+              done = true;
+            }
+          } else if (tma) {
+            if constexpr (fwd_tma_fits<T, HH, CTT, true>()) {
+              using SH = FwdTmaShape<T, HH, CTT, true>;
+              constexpr int NG = tma_groups<SH>();
+              auto* k = k_plane_fwd_tma<T, HH, CTT, NG, true>;
+              const int grid = tma_grid(k, NG * SH::threads, NG * SH::group, ntasks, NG);
+              launch_k(k, dim3(grid), NG * SH::threads, NG * SH::group, st, g, tab, f0, E, W, nb, ntasks,
+                       static_cast<uint64_t>(a.timeout_ns), a.status);
+              done = true;
+            }
+          }
+          if (!done)
+            launch_k(k_plane_fwd_h<T, HH, CTT>, dim3(H, nslots), thr_plane, smem_plane, st, g, tab, f0, E, W, nb);
         });
       });
     } else {
       CFFT_FOR_H(H, {
         CFFT_FOR_CT(a.cent_type, {
-          launch_k(k_plane_bwd_h<T, HH, CTT, true>, dim3(H, nslots), thr_plane, smem_plane, st, g, tab, W, E, f0_out, nb);
+          bool done = false;
+          if (tma) {
+            if constexpr (bwd_tma_fits<T, HH, CTT>()) {
+              using SH = BwdTmaShape<T, HH, CTT>;
+              constexpr int NG = tma_groups<SH>();
+              auto* k = k_plane_bwd_tma<T, HH, CTT, NG>;
+              const int grid = tma_grid(k, NG * SH::threads, NG * SH::group, ntasks, NG);
+              launch_k(k, dim3(grid), NG * SH::threads, NG * SH::group, st, g, tab, static_cast<const C*>(W), E, f0_out,
+                       nb, ntasks, static_cast<uint64_t>(a.timeout_ns), a.status);
+              done = true;
+            }
+          }
+          if (!done)
+            launch_k(k_plane_bwd_h<T, HH, CTT, true>, dim3(H, nslots), thr_plane, smem_plane, st, g, tab, W, E, f0_out, nb);
         });
       });
     }
@@ -1591,6 +1843,22 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
       }
       case 3: {
         const int no = a.n_orbits;
+        if (a.reps_wide) {
+          constexpr int GW = wide_fields<C>();
+          const int ng = (nb + GW - 1) / GW;
+          C* FT = static_cast<C*>(a.FT);
+          launch_k(k_group_spectra_w<T>, dim3((a.n_spec + kWideTile - 1) / kWideTile, ng), 256, 0, st, Fin, FT,
+                   a.n_spec, nb);
+          const dim3 gw((GW / 2 * no + 255) / 256, ng);
+          const uint32_t* pk = static_cast<const uint32_t*>(a.inv_pk);
+          switch (a.d) {
+            case 1: launch_k(k_inv_recon_w<T, 1>, gw, 256, 0, st, g, tab, pk, FT, G0R); break;
+            case 2: launch_k(k_inv_recon_w<T, 2>, gw, 256, 0, st, g, tab, pk, FT, G0R); break;
+            case 4: launch_k(k_inv_recon_w<T, 4>, gw, 256, 0, st, g, tab, pk, FT, G0R); break;
+            default: launch_k(k_inv_recon_w<T, 8>, gw, 256, 0, st, g, tab, pk, FT, G0R); break;
+          }
+          break;
+        }
         if (a.reps_quad) {
           const int nq = (nb + 3) / 4;
           C* FT = static_cast<C*>(a.FT);
@@ -1619,7 +1887,11 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
           break;
         }
         CFFT_FOR_H(H, {
-          if (a.reps_quad) {
+          if (a.reps_wide) {
+            constexpr int GW = wide_fields<C>();
+            launch_k(k_expand_w_ifft_z_h<T, HH>, dim3(HH, nch, (nb + GW - 1) / GW), GW / 2 * HH, 0, st, g, tab,
+                     static_cast<const uint32_t*>(a.expand), G0R, W, nb);
+          } else if (a.reps_quad) {
             // two y values per CTA (128 threads at H = 32): 5 CTAs per SM at this kernel's registers
             constexpr int half = ((2 * HH + 31) / 32) * 32;
             launch_k(k_expand4_ifft_z_h<T, HH, 2>, dim3((HH + 1) / 2, nch, (nb + 3) / 4), 2 * half, 0, st, 

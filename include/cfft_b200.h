@@ -94,7 +94,9 @@ typedef struct cfft_info {
   int P;                 /* lcm(N): phase denominator */
   int64_t workspace_bytes;
   int exec_path;         /* bit 0: compile-time sized kernels; bit 1: packed quad backward gather;
-                            bit 2: fused 8-CTA cluster kernels (0 for host-only plans) */
+                            bit 2: fused 8-CTA cluster kernels; bit 3 / bit 4: persistent bulk-copy
+                            (TMA) forward / backward plane kernels; bit 5: backward gather in
+                            groups of 16 (FP32) / 8 (FP64) fields (0 for host-only plans) */
   int chunk;             /* fields per workspace chunk */
   int lanes;             /* concurrent chunk lanes */
 } cfft_info;
@@ -238,6 +240,17 @@ cfft_status cfft_forward_noalloc(cfft_plan plan, const void* f0, void* F, int ba
 cfft_status cfft_forward_host(cfft_plan plan, const void* f0_host, void* F_host, int batch);
 cfft_status cfft_backward_host(cfft_plan plan, const void* F_host, void* f0_host, int batch);
 cfft_status cfft_scft_step_host(cfft_plan plan, void* f0_host, int batch);
+
+/* Status of the plan's bounded device waits.  No reference counterpart: the
+ * persistent bulk-copy kernels bound every wait on a copy (CFFT_WAIT_TIMEOUT_NS,
+ * default one second); a wait that runs out records CFFT_ERR_TIMEOUT here, and every
+ * later execute call on the plan returns CFFT_ERR_TIMEOUT until it is cleared.  Call
+ * after synchronising the stream; clear != 0 resets the status. */
+cfft_status cfft_plan_device_status(cfft_plan plan, int clear);
+/* Self-test of that mechanism: launches one kernel on `stream` whose bounded wait
+ * waits for bytes that never arrive, so after timeout_ns it records CFFT_ERR_TIMEOUT
+ * in the plan's status and returns (the GPU context stays usable). */
+cfft_status cfft_wait_selftest(cfft_plan plan, unsigned long long timeout_ns, void* stream);
 
 /* ---------------- diagnostics ---------------- */
 /* Forward then backward of one batch with a CUDA event between every launch;
