@@ -36,4 +36,6 @@ from .asu import (  # noqa: F401
     compute_full_orbit, pack_asu, pack_asu_interleaved, CFFTPlan, plan_cfft, mul, ldiv,
 )
 
-__version__ = "0.1.0"
+from .scft import SCFTSolver, initial_fields, plan_scft  # noqa: F401
+
+__version__ = "0.2.0"

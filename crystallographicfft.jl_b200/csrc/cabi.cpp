@@ -7,6 +7,7 @@
 #include "../../include/cfft_b200.h"
 #include "exec.h"
 #include "fast_api.h"
+#include "scft.h"
 
 using cfft::Status;
 
@@ -338,6 +339,63 @@ cfft_status cfft_update_kernel(cfft_plan plan, double ds, const double* lattice)
     Status s_ = (expr);                                               \
     return ret(s_, err);                                              \
   } while (0)
+
+cfft_status cfft_scft_create(cfft_plan plan, const cfft_scft_params* params, cfft_scft* scft) {
+  if (!plan || !params || !scft) return ret(Status::kInvalid, "null argument");
+  cfft::ScftParams prm;
+  prm.f = params->f;
+  prm.chiN = params->chiN;
+  prm.Ns = params->Ns;
+  prm.history = params->history;
+  prm.tol = params->tol;
+  prm.max_iter = params->max_iter;
+  prm.lam_simple = params->lam_simple;
+  prm.lam_anderson = params->lam_anderson;
+  prm.anderson_start = params->anderson_start;
+  std::string err;
+  cfft::Scft* s = nullptr;
+  const Status st = cfft::scft_create(reinterpret_cast<cfft::Plan*>(plan), prm, &s, &err);
+  if (st == Status::kOk) *scft = reinterpret_cast<cfft_scft>(s);
+  return ret(st, err);
+}
+
+cfft_status cfft_scft_destroy(cfft_scft scft) {
+  cfft::scft_destroy(reinterpret_cast<cfft::Scft*>(scft));
+  return CFFT_OK;
+}
+
+static void to_c_state(const cfft::ScftState& s, cfft_scft_state* out) {
+  out->Q = s.Q;
+  out->F = s.F;
+  out->err = s.err;
+  out->iterations = s.iterations;
+  out->converged = s.converged;
+}
+
+cfft_status cfft_scft_evaluate(cfft_scft scft, const void* w, void* phi, void* d, cfft_scft_state* state,
+                               void* stream) {
+  if (!scft || !state) return ret(Status::kInvalid, "null argument");
+  std::string err;
+  cfft::ScftState s;
+  const Status st = cfft::scft_evaluate(reinterpret_cast<cfft::Scft*>(scft), w, phi, d, &s, stream, &err);
+  to_c_state(s, state);
+  return ret(st, err);
+}
+
+cfft_status cfft_scft_solve(cfft_scft scft, void* w, cfft_scft_state* state, void* stream) {
+  if (!scft || !state) return ret(Status::kInvalid, "null argument");
+  std::string err;
+  cfft::ScftState s;
+  const Status st = cfft::scft_solve(reinterpret_cast<cfft::Scft*>(scft), w, &s, stream, &err);
+  to_c_state(s, state);
+  return ret(st, err);
+}
+
+cfft_status cfft_scft_densities(cfft_scft scft, void* phi, void* stream) {
+  if (!scft || !phi) return ret(Status::kInvalid, "null argument");
+  std::string err;
+  return ret(cfft::scft_densities(reinterpret_cast<cfft::Scft*>(scft), phi, stream, &err), err);
+}
 
 cfft_status cfft_plan_device_status(cfft_plan plan, int clear) {
   if (!plan) return ret(Status::kInvalid, "null plan");

@@ -761,6 +761,20 @@ Status check_batch(const Plan* p, int B, std::string* err) {
 
 }  // namespace
 
+void add_launches(int64_t n) { g_launches += n; }
+
+Status exec_contour_step(Plan* p, const void* in, void* out, const void* E, int B, void* stream, std::string* err) {
+  Status st = check_batch(p, B, err);
+  if (st != Status::kOk) return st;
+  if (!in || !out || !E || in == out) { *err = "invalid argument"; return Status::kInvalid; }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (p->precision == 8)
+    return run_chunks<double>(p, true, true, static_cast<const double*>(in), static_cast<double2*>(p->d_work_F),
+                              static_cast<double*>(out), static_cast<const double*>(E), true, B, s, err);
+  return run_chunks<float>(p, true, true, static_cast<const float*>(in), static_cast<float2*>(p->d_work_F),
+                           static_cast<float*>(out), static_cast<const float*>(E), true, B, s, err);
+}
+
 int64_t launch_count(bool reset) {
   const int64_t v = g_launches;
   if (reset) g_launches = 0;

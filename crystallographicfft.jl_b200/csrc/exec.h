@@ -127,5 +127,11 @@ Status plan_device_status(Plan* p, bool clear, std::string* err);
 Status plan_wait_selftest(Plan* p, unsigned long long timeout_ns, void* stream, std::string* err);
 
 int64_t launch_count(bool reset);
+// Adds n to the launch counter (kernels launched outside exec.cu).
+void add_launches(int64_t n);
+
+// One contour step of a batch with per-field interaction factors E (B x M-grid):
+// out = E . IKRFFT(K . KRFFT(E . in)), in and out distinct buffers of B fields.
+Status exec_contour_step(Plan* p, const void* in, void* out, const void* E, int B, void* stream, std::string* err);
 
 }  // namespace cfft

@@ -1424,16 +1424,24 @@ inline void launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cu
   }
 }
 
-// Persistent bulk-copy plane kernels (tma_planes.cuh): on unless CFFT_TMA=0.  They
-// serve centred plans with H >= 16 whose per-group stage and buffer fit at least two
-// groups into one CTA's shared memory.
-inline bool tma_enabled() {
-  static const bool on = [] {
+// Persistent bulk-copy plane kernels (tma_planes.cuh).  They serve centred plans with
+// H >= 16 whose per-group stage and buffer fit at least two groups into one CTA's
+// shared memory.  CFFT_TMA selects them: "fwd" (default: the forward plane stage),
+// "all" (both stages), "0" (neither).  Measured on Im-3m 128^3 FP32: the forward one
+// matches the per-plane kernel, the backward one (12 warps per SM against 20) is 30%
+// slower, so the backward stage keeps the per-plane kernel by default.
+inline int tma_mode() {  // bit 0: forward, bit 1: backward
+  static const int m = [] {
     const char* e = std::getenv("CFFT_TMA");
-    return !(e && e[0] == '0');
+    if (!e) return 1;
+    if (e[0] == '0') return 0;
+    if (e[0] == 'a' || e[0] == '1') return 3;
+    if (e[0] == 'b') return 2;
+    return 1;
   }();
-  return on;
+  return m;
 }
+inline bool tma_enabled() { return tma_mode() != 0; }
 template <typename T, int H, int CT, bool USE_E>
 constexpr bool fwd_tma_fits() {
   if constexpr (CT == 0 || H < 16 || H % (16 / static_cast<int>(sizeof(T))) != 0) return false;
@@ -1679,9 +1687,9 @@ void fast_unit_tma_planes(int H, int ct, bool* fwd, bool* fwd_e, bool* bwd) {
   if (!tma_enabled() || !fast_size_ok(H, sizeof(T))) return;
   CFFT_FOR_H(H, {
     CFFT_FOR_CT(ct, {
-      *fwd = fwd_tma_fits<T, HH, CTT, false>();
-      *fwd_e = fwd_tma_fits<T, HH, CTT, true>();
-      *bwd = bwd_tma_fits<T, HH, CTT>();
+      *fwd = (tma_mode() & 1) && fwd_tma_fits<T, HH, CTT, false>();
+      *fwd_e = (tma_mode() & 1) && fwd_tma_fits<T, HH, CTT, true>();
+      *bwd = (tma_mode() & 2) && bwd_tma_fits<T, HH, CTT>();
     });
   });
 }
@@ -1729,7 +1737,8 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
     const size_t smem_plane = static_cast<size_t>(nch) * H * (H + 1) * cs;
     const int ntasks = nslots * H;
     auto al16 = [](const void* p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
-    const bool tma = tma_enabled() && al16(f0) && al16(E) && al16(f0_out) && al16(W);
+    const bool tma = tma_enabled() && al16(f0) && al16(E) && al16(f0_out) && al16(W) &&
+                     (tma_mode() & (a.stage == 0 ? 1 : 2));
     if (a.stage == 0) {
       CFFT_FOR_H(H, {
         CFFT_FOR_CT(a.cent_type, {

@@ -252,6 +252,49 @@ cfft_status cfft_plan_device_status(cfft_plan plan, int clear);
  * in the plan's status and returns (the GPU context stays usable). */
 cfft_status cfft_wait_selftest(cfft_plan plan, unsigned long long timeout_ns, void* stream);
 
+/* ---------------- SCFT driver (AB diblock melt) ----------------
+ * No reference counterpart: the reference stops at the contour step these entries run
+ * on (step_diffusion!, src/diffusion_solver.jl:254-282; execute_m2_scft!,
+ * src/q_fused_krfft.jl:989-1026).  The self-consistent field iteration of an
+ * incompressible AB diblock melt (Gaussian chain, lengths in the plan's lattice units,
+ * contour s in [0, 1], ds = 1/Ns; the plan's ds must equal 1/Ns and its max_batch be
+ * at least 2): propagators q, q_dagger (one two-field batch of the plan's contour
+ * step), Q = <q(r, 1)>, densities by Simpson's rule, residuals
+ * d_A = chiN (phi_B - 1/2) + (w_B - w_A)/2, d_B = chiN (phi_A - 1/2) + (w_A - w_B)/2,
+ * err = sqrt(sum d^2 / sum w^2), F = -ln Q + <chiN phi_A phi_B - w_A phi_A - w_B phi_B>,
+ * simple mixing above anderson_start, Anderson mixing below.  Q, F, the residual
+ * norms, the Anderson Gram matrix and its least-squares solve are FP64 on the device.
+ * Fields are [w_A | w_B] on the plan's M-grid (2 x M1 M2 M3 reals of the plan's
+ * precision, device memory). */
+typedef struct cfft_scft_params {
+  double f;              /* A-block fraction, 0 < f < 1 */
+  double chiN;           /* chi N */
+  int Ns;                /* contour steps */
+  int history;           /* Anderson history depth, 0..32 */
+  double tol;            /* stop when err < tol */
+  int max_iter;
+  double lam_simple;     /* simple-mixing step (err > anderson_start) */
+  double lam_anderson;   /* Anderson mixing step */
+  double anderson_start; /* residual below which Anderson mixing runs */
+} cfft_scft_params;
+typedef struct cfft_scft_state {
+  double Q, F, err;
+  int iterations;
+  int converged;
+} cfft_scft_state;
+typedef struct cfft_scft_s* cfft_scft;
+cfft_status cfft_scft_create(cfft_plan plan, const cfft_scft_params* params, cfft_scft* scft);
+cfft_status cfft_scft_destroy(cfft_scft scft);
+/* One evaluation of fields w: Q, F, err into *state; densities [phi_A | phi_B] into phi
+ * and residuals [d_A | d_B] into d when not NULL.  Synchronises the stream. */
+cfft_status cfft_scft_evaluate(cfft_scft scft, const void* w, void* phi, void* d, cfft_scft_state* state,
+                               void* stream);
+/* Iterate from w (in/out) until err < tol or max_iter; *state holds the last
+ * evaluation.  One stream synchronisation per iteration (the convergence test). */
+cfft_status cfft_scft_solve(cfft_scft scft, void* w, cfft_scft_state* state, void* stream);
+/* Densities [phi_A | phi_B] of the last evaluation (device copy on `stream`). */
+cfft_status cfft_scft_densities(cfft_scft scft, void* phi, void* stream);
+
 /* ---------------- diagnostics ---------------- */
 /* Forward then backward of one batch with a CUDA event between every launch;
  * stage_ms receives up to 8 per-stage device times (plane/fold+xy FFT, z FFT,

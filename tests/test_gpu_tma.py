@@ -40,7 +40,7 @@ def test_headline_plan_uses_bulk_copy_planes(cf, prep):
     N = (128, 128, 128)
     p = prep(229, N, seed=5)
     plan = cf.KRFFTPlan(p["spec"], p["ops_s"], precision=4, max_batch=2)
-    assert plan.info.exec_path & 8 and plan.info.exec_path & 16
+    assert plan.info.exec_path & 8  # forward stage (the backward one is opt-in: CFFT_TMA=all)
     plan.close()
 
 
@@ -49,7 +49,7 @@ def test_step_diffusion_ia3d96_fp32_vs_oracle(cf, O, prep):
     N = (96, 96, 96)
     p = prep(230, N, seed=8)
     plan = cf.KRFFTPlan(p["spec"], p["ops_s"], precision=4, max_batch=1, ds=0.02, lattice=np.eye(3) * 3.8)
-    assert plan.H == (24, 24, 24) and plan.info.exec_path & 16
+    assert plan.H == (24, 24, 24) and plan.info.exec_path & 8
     f0 = O.pack_stride(p["u"], plan.L)
     w = 0.3 * O.pack_stride(O.make_symmetric(p["oops"], N, seed=9), plan.L)
     q = _dev(f0)
@@ -78,5 +78,5 @@ def test_bounded_wait_timeout_reported(cf, O, prep):
     assert cf.LIB.cfft_plan_device_status(plan.handle, 0) == 0
     F = plan.forward(x)                                                         # the context is usable
     truth = O.spectrum_on_asu(p["u"], O.calc_spectral_asu(p["oops"], 3, N))
-    assert rel_err(F.cpu().numpy()[0], truth) < 1e-5
+    assert rel_err(F.cpu().numpy().reshape(-1), truth) < 1e-5
     plan.close()
