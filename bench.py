@@ -2,13 +2,13 @@
 FP32 with the centring fold, batched fields resident in HBM.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl ours|reference]
-                    [--workload im3m128|pmmm64|ia3d96-step|mixed]
+                    [--workload im3m128|scft-ia3d96|pmmm64|ia3d96-step|mixed]
 
 One step = one forward + backward KRFFT over B fields (f0 -> spectral ASU -> f0).
 The default workload is the headline line; --workload selects a secondary single-GPU
-measurement (Pmmm 64^3 FP64 forward + backward; the Ia-3d 96^3 FP32 diffusion contour
-step; 64 fields over four cubic groups and four grid edges, forward + backward and a
-50-step diffusion solve each).
+measurement (the SCFT time-to-tolerance of an AB diblock in Ia-3d at 96^3; Pmmm 64^3
+FP64 forward + backward; the Ia-3d 96^3 FP32 diffusion contour step; 64 fields over four
+cubic groups and four grid edges, forward + backward and a 50-step diffusion solve each).
 Prints ONE JSON line on rank 0.  Under torchrun each rank runs its own batch
 (fields are independent: replicas / weak scaling); the step time is the max over
 ranks.  `--impl reference` times the FP64 CPU restatement of the reference's
@@ -46,6 +46,20 @@ def load_package():
     sys.modules[name] = mod
     spec.loader.exec_module(mod)
     return mod
+
+
+def kernel_source_sha():
+    """Hash of the native sources; a DRAM-traffic figure measured by ncu applies to the
+    build it was measured on only."""
+    import hashlib
+
+    h = hashlib.sha256()
+    csrc = os.path.join(PKG_DIR, "csrc")
+    for name in sorted(os.listdir(csrc)):
+        if name.endswith((".cu", ".cuh", ".h", ".cpp")):
+            h.update(name.encode())
+            h.update(open(os.path.join(csrc, name), "rb").read())
+    return h.hexdigest()[:16]
 
 
 def algorithmic_bytes_per_field(M, n_spec, real_bytes=4):
@@ -446,12 +460,18 @@ def run_ours(args):
             line["cpu_baseline"] = cpu_reference_sample(budget_s=12.0)
         except Exception as exc:  # the baseline is reported, never required
             line["cpu_baseline"] = {"error": repr(exc)}
+    # DRAM traffic per step from the ncu capture of this very build (matched by the hash
+    # of the native sources); null when the sources changed since the capture.
     traffic_file = os.path.join(ROOT, "profiles", "traffic_im3m128.json")
+    line["roofline"]["kernel_source_sha"] = kernel_source_sha()
     if os.path.exists(traffic_file):
         try:
             tr = json.load(open(traffic_file))
-            line["roofline"]["traffic"] = tr.get("bytes_per_field", 0) * B
-            line["roofline"]["traffic_note"] = tr.get("note")
+            if tr.get("kernel_source_sha") == line["roofline"]["kernel_source_sha"]:
+                line["roofline"]["traffic"] = tr.get("bytes_per_field", 0) * B
+                line["roofline"]["traffic_note"] = tr.get("note")
+            else:
+                line["roofline"]["traffic_note"] = "no ncu capture of this build's sources"
         except (OSError, ValueError):
             pass
     plan.close()
@@ -473,6 +493,89 @@ WORKLOADS = {
                        "FP32: forward+backward and a 50-step diffusion solve each (one plan and stream per "
                        "group and edge; the 50-step loop replays a CUDA graph)"),
 }
+
+
+SCFT_CONFIG = dict(sg=230, n=96, f=0.4, chiN=20.0, Ns=100, history=20, tol=1e-6, switch=1e-4, sigma=2.0,
+                   amplitude=1.0, cell=3.8 * np.sqrt(6.0))
+
+
+def run_scft(args):
+    """SCFT time-to-tolerance, AB diblock in Ia-3d (No. 230) on 96^3: f = 0.4, chiN = 20,
+    Ns = 100, Anderson history 20, residual 1e-6.  One step = one solve from the seeded
+    start (Gaussian-filtered noise, sigma = 2 grid points, amplitude 1.0, symmetrised):
+    FP32 fields and propagators until the residual is below 1e-4, then the same fields
+    in FP64 to 1e-6 (FP32 rounding leaves a residual floor near 2e-6 at 96^3).  Q, F and
+    the mixing solve are FP64 on the device throughout."""
+    import torch
+
+    cf = load_package()
+    C = SCFT_CONFIG
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(0)
+    N = (C["n"],) * 3
+    _, ops_s = cf.find_optimal_shift(cf.get_ops(C["sg"], 3, N), N)
+    kw = dict(f=C["f"], chiN=C["chiN"], Ns=C["Ns"], history=C["history"], max_iter=1000)
+    p32, s32 = cf.plan_scft(C["sg"], N, C["cell"], precision=4, ops=ops_s, tol=C["switch"], **kw)
+    p64, s64 = cf.plan_scft(C["sg"], N, C["cell"], precision=8, ops=ops_s, tol=C["tol"], **kw)
+    w0 = cf.initial_fields(ops_s, N, p32.L, C["f"], C["chiN"], seed=0, sigma=C["sigma"], amplitude=C["amplitude"])
+    w0_32 = torch.tensor(w0, dtype=torch.float32, device=dev).contiguous()
+    s32.evaluate(w0_32)  # captures the propagator graphs
+    s64.evaluate(w0_32.double())
+
+    def solve():
+        w = w0_32.clone()
+        a = s32.solve(w)
+        w64 = w.double()
+        b = s64.solve(w64)
+        return a, b
+
+    for _ in range(args.warmup):
+        solve()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(0.3)
+    cf.LIB.cfft_launch_count(1)
+    times, res = [], None
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = solve()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / 1000.0)
+    launches = int(cf.LIB.cfft_launch_count(1))
+    clk = clocks.stop()
+    a, b = res
+    # per-iteration evaluation time of each precision (the solves synchronise every iteration)
+    ev = {}
+    for name, sol, w in (("fp32", s32, w0_32), ("fp64", s64, w0_32.double())):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(5):
+            sol.evaluate(w)
+        e1.record()
+        torch.cuda.synchronize()
+        ev[name] = e0.elapsed_time(e1) / 5
+    mean_s = float(np.mean(times))
+    line = {"metric": "SCFT time-to-tol, s per solve (AB diblock, Ia-3d 96^3, f=0.4, chiN=20, Ns=100, "
+                      "Anderson 20, residual 1e-6; plain seeded start)",
+            "value": mean_s, "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": mean_s * 1000.0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": "scft-ia3d96", "group": C["sg"], "N": C["n"], "f": C["f"], "chiN": C["chiN"],
+                       "Ns": C["Ns"], "anderson_history": C["history"], "tol": C["tol"],
+                       "cell": "3.8 b sqrt(N) = %.4f Rg" % C["cell"],
+                       "start": "seeded Gaussian-filtered noise, sigma 2 grid points, amplitude 1.0, symmetrised",
+                       "phases": "FP32 to residual %.0e, then FP64 to %.0e" % (C["switch"], C["tol"])},
+            "result": {"F": b["F"], "Q": b["Q"], "residual": b["err"], "converged": b["converged"],
+                       "iterations_fp32": a["iterations"], "iterations_fp64": b["iterations"],
+                       "disordered_F": C["chiN"] * C["f"] * (1 - C["f"]),
+                       "solve_s": [round(t, 4) for t in times]},
+            "evaluate_ms": ev, "gpu_launches": launches, "clocks": clk, "e2e": None, "roofline": None}
+    for o in (s32, s64, p32, p64):
+        o.close()
+    print(json.dumps(line), flush=True)
 
 
 def _field_bytes(plan, rs):
@@ -588,12 +691,14 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing (profiling runs)")
-    ap.add_argument("--workload", default="im3m128", choices=["im3m128"] + sorted(WORKLOADS),
+    ap.add_argument("--workload", default="im3m128", choices=["im3m128", "scft-ia3d96"] + sorted(WORKLOADS),
                     help="im3m128 is the headline line; the others are secondary single-GPU measurements")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "scft-ia3d96":
+        run_scft(args)
     elif args.workload != "im3m128":
         run_workload(args)
     else:

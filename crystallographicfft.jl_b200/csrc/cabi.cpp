@@ -208,7 +208,7 @@ cfft_status cfft_plan_info(cfft_plan plan, cfft_info* info) {
     tma = (fw ? 8 : 0) | (bw ? 16 : 0);
   }
   info->exec_path = (p->fast_h > 0 ? 1 : 0) | (p->reps_quad ? 2 : 0) | (p->cluster ? 4 : 0) | tma |
-                    (p->reps_wide && !p->cluster ? 32 : 0);
+                    (p->reps_wide && !p->cluster ? 32 : 0) | (p->qsep ? 64 : 0);
   info->chunk = p->chunk;
   info->lanes = p->lanes;
   return CFFT_OK;

@@ -50,6 +50,25 @@ template <typename C> __device__ __forceinline__ C cscale(C a, decltype(C::x) s)
 // multiply by -i (forward) or +i (inverse)
 template <typename C, bool INV> __device__ __forceinline__ C mul_mi(C a) { return INV ? mk<C>(-a.y, a.x) : mk<C>(a.y, -a.x); }
 
+// FP32 complex arithmetic on sm_100's packed two-lane instructions (FADD2 / FMUL2 /
+// FFMA2 through __fadd2_rn, __fmul2_rn, __ffma2_rn): a complex add or subtract is one
+// instruction instead of two.  Each lane rounds like the scalar operation it replaces
+// (round to nearest), so results are unchanged except where the scalar code would
+// have fused a multiply-add differently.  Off with -DCFFT_NO_PACKED_F32.
+#ifndef CFFT_NO_PACKED_F32
+template <> __device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b) { return __fadd2_rn(a, b); }
+template <> __device__ __forceinline__ float2 csub<float2>(float2 a, float2 b) {
+  return __ffma2_rn(b, make_float2(-1.f, -1.f), a);
+}
+template <> __device__ __forceinline__ float2 cmul<float2>(float2 a, float2 b) {
+  return __ffma2_rn(make_float2(a.x, a.x), b, __fmul2_rn(make_float2(a.y, a.y), make_float2(-b.y, b.x)));
+}
+template <> __device__ __forceinline__ float2 cmulc<float2>(float2 a, float2 b) {  // a * conj(b)
+  return __ffma2_rn(make_float2(a.x, a.x), make_float2(b.x, -b.y), __fmul2_rn(make_float2(a.y, a.y), make_float2(b.y, b.x)));
+}
+template <> __device__ __forceinline__ float2 cscale<float2>(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
+#endif
+
 // ---------------------------------------------------------------- small DFTs
 template <typename C, bool INV> __device__ __forceinline__ void dft2(C* v) {
   C a = v[0], b = v[1];
@@ -158,6 +177,15 @@ __device__ C* fft_lines(C* a, C* b, int n, int nf, const int* radix, int nlines,
     Ns *= R;
   }
   return a;
+}
+
+// Walsh-Hadamard transform of 8 complex values (two real transforms in the lanes).
+template <typename C> __device__ __forceinline__ void wht8c(C* v) {
+#pragma unroll
+  for (int s = 1; s < 8; s <<= 1)
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      if (!(i & s)) { const C a = v[i], b = v[i + s]; v[i] = cadd(a, b); v[i + s] = csub(a, b); }
 }
 
 // Walsh-Hadamard transform of 8 values indexed e0 + 2 e1 + 4 e2 (three butterfly stages).

@@ -612,6 +612,8 @@ Status launch_stage(Plan* p, int stage, const T* f0, typename Cx<T>::type* F, co
       a.q_step = true;
       a.QT = p->d_qt;
       a.GT = p->d_gt;
+      a.qsep = p->qsep;
+      a.QS = p->d_qsep;
       C* WQ = reinterpret_cast<C*>(static_cast<char*>(p->d_work_Q) + lane * p->w_lane_bytes);
       if (stage == 4) a.W2 = WQ;
       else if (stage == 5) a.W = WQ;
@@ -988,9 +990,33 @@ Status plan_device_init(Plan* p, std::string* err) {
       return Status::kUnsupported;
     }
     const size_t np = static_cast<size_t>(T.n_ch) * hvol;
-    if ((st = alloc(&p->d_qt, T.d * np * cs, "Q coefficients")) != Status::kOk) return st;
-    if ((st = alloc(&p->d_gt, T.d * np * 4, "Q gather")) != Status::kOk) return st;
     if ((st = alloc(&p->d_work_Q, p->lanes * p->w_lane_bytes, "Q workspace")) != Status::kOk) return st;
+    // Separable Q-multiply (_is_pmmm_like, src/q_fused_krfft.jl:431-454): M2Q plan, d = 8,
+    // L = (2, 2, 2), diagonal representatives listed in parity-class order with
+    // translations 0 or N - 1, and an orthogonal cell (K factorises per axis).
+    {
+      bool sep = p->qmode == 3 && !T.centered && T.n_ch == 1 && T.d == 8 && p->fast_h == T.M[0] &&
+                 T.M[0] == T.M[1] && T.M[1] == T.M[2] && T.L[0] == 2 && T.L[1] == 2 && T.L[2] == 2;
+      for (int i = 0; i < 3 && sep; ++i)
+        for (int j = 0; j < 3; ++j)
+          if (i != j && std::fabs(p->lattice[3 * j + i]) > 1e-12 * std::fabs(p->lattice[4 * i])) sep = false;
+      for (int a = 0; a < 8 && sep; ++a)
+        for (int d = 0; d < 3 && sep; ++d) {
+          for (int e = 0; e < 3; ++e)
+            if (e != d && T.rep_ops[a].R[d][e] != 0) sep = false;
+          const long tm = floor_mod(T.rep_ops[a].t[d], T.N[d]);
+          if (tm != 0 && tm != T.N[d] - 1) sep = false;
+          if ((tm != 0) != (((a >> d) & 1) != 0)) sep = false;
+        }
+      const char* qe = std::getenv("CFFT_QSEP");
+      p->qsep = sep && !(qe && qe[0] == '0');
+    }
+    if (p->qsep) {
+      if ((st = alloc(&p->d_qsep, static_cast<size_t>(9) * T.M[0] * cs, "separable Q factors")) != Status::kOk) return st;
+    } else {
+      if ((st = alloc(&p->d_qt, T.d * np * cs, "Q coefficients")) != Status::kOk) return st;
+      if ((st = alloc(&p->d_gt, T.d * np * 4, "Q gather")) != Status::kOk) return st;
+    }
     // Gather targets as indices into the z-fastest forward workspace WT[c][x][y][z].
     const int H = T.H[0];
     const long Mvol = static_cast<long>(T.M[0]) * T.M[1] * T.M[2];
@@ -1011,7 +1037,7 @@ Status plan_device_init(Plan* p, std::string* err) {
               }
               gt[b * np + pos] = cc < 0 ? -1 : static_cast<int32_t>(cc * hvol + (static_cast<size_t>(k[0]) * H + k[1]) * H + k[2]);
             }
-    CFFT_CUDA(cudaMemcpy(p->d_gt, gt.data(), gt.size() * 4, cudaMemcpyHostToDevice), "upload Q gather");
+    if (p->d_gt) CFFT_CUDA(cudaMemcpy(p->d_gt, gt.data(), gt.size() * 4, cudaMemcpyHostToDevice), "upload Q gather");
   }
   CFFT_CUDA(cudaMemcpy(p->d_geom, &g, sizeof(g), cudaMemcpyHostToDevice), "upload geometry");
   CFFT_CUDA(cudaMemcpy(p->d_tables, tab.data(), tab.size(), cudaMemcpyHostToDevice), "upload tables");
@@ -1109,6 +1135,31 @@ Status plan_upload_kernel(Plan* p, std::string* err) {
     std::vector<float> k(p->T.K.begin(), p->T.K.end());
     CFFT_CUDA(cudaMemcpy(p->d_K, k.data(), k.size() * 4, cudaMemcpyHostToDevice), "upload K");
   }
+  if (p->qsep && p->d_qsep) {
+    // 1-D twiddles e^{2 pi i q / N_d} (q < M) and kernel factors exp(-ds (2 pi h_c / a_d)^2)
+    // (h < N_d, h_c = h - N_d for h >= N_d / 2) of the separable Q-multiply.
+    const PlanTables& T = p->T;
+    const int Mq = T.M[0];
+    std::vector<double> qs(static_cast<size_t>(9) * Mq * 2, 0.0);
+    for (int d = 0; d < 3; ++d) {
+      for (int q = 0; q < Mq; ++q) {
+        qs[(d * Mq + q) * 2] = std::cos(2.0 * M_PI * q / T.N[d]);
+        qs[(d * Mq + q) * 2 + 1] = std::sin(2.0 * M_PI * q / T.N[d]);
+      }
+      const double ad = p->lattice[4 * d];
+      for (int h = 0; h < T.N[d]; ++h) {
+        const int hc = h >= T.N[d] / 2 ? h - T.N[d] : h;
+        const double kk = 2.0 * M_PI * hc / ad;
+        qs[(3 * Mq + d * T.N[d] + h) * 2] = std::exp(-p->ds * kk * kk);
+      }
+    }
+    if (p->precision == 8) {
+      CFFT_CUDA(cudaMemcpy(p->d_qsep, qs.data(), qs.size() * 8, cudaMemcpyHostToDevice), "upload separable Q");
+    } else {
+      std::vector<float> qf(qs.begin(), qs.end());
+      CFFT_CUDA(cudaMemcpy(p->d_qsep, qf.data(), qf.size() * 4, cudaMemcpyHostToDevice), "upload separable Q");
+    }
+  }
   if (p->qmode && p->d_qt) {
     // Q first row in the order the Q-multiply kernel walks the channel points: [b][c][z][y][x].
     const PlanTables& T = p->T;
@@ -1140,7 +1191,7 @@ void plan_device_free(Plan* p) {
   void** bufs[] = {&p->d_geom, &p->d_tables, &p->d_spec_h, &p->d_K, &p->d_orbit_rep, &p->d_inv_spec,
                    &p->d_inv_phase, &p->d_img_mask, &p->d_fill_map, &p->d_work_T, &p->d_work_F,
                    &p->d_work_E, &p->d_stage_in, &p->d_stage_out, &p->d_expand, &p->d_g0r, &p->d_inv_pk, &p->d_ft,
-                   &p->d_qt, &p->d_gt, &p->d_work_Q, &p->d_zr_units, &p->d_zr_pts};
+                   &p->d_qt, &p->d_gt, &p->d_work_Q, &p->d_zr_units, &p->d_zr_pts, &p->d_qsep};
   for (void** b : bufs)
     if (*b) { cudaFree(*b); *b = nullptr; }
   if (p->h_status) { cudaFreeHost(p->h_status); p->h_status = nullptr; p->d_status = nullptr; }

@@ -82,6 +82,8 @@ struct Plan {
   void* d_qt = nullptr;         // d x n_ch x H^3 complex coefficients
   void* d_gt = nullptr;         // d x n_ch x H^3 int32 workspace index (-1: extinct class)
   void* d_work_Q = nullptr;     // lanes x channel workspace (Q-multiply output)
+  bool qsep = false;            // separable Q-multiply (Pmmm-like M2Q plans, CFFT_QSEP=0 turns it off)
+  void* d_qsep = nullptr;       // its 1-D twiddles (3 x H) and kernel factors (3 x 2H), complex
   int cluster_ctas = 8;         // CTAs per cluster
   // Status word of the bounded device waits (mapped pinned host memory, so the host
   // reads it without a synchronisation): 0, or CFFT_ERR_TIMEOUT once a wait ran out.

@@ -44,6 +44,8 @@ struct FastArgs {
   const void* QT = nullptr;   // d x n_ch x H^3 coefficients
   const void* GT = nullptr;   // d x n_ch x H^3 int32 workspace indices (-1: extinct)
   void* W2 = nullptr;
+  bool qsep = false;          // separable Q-multiply (Pmmm-like plans)
+  const void* QS = nullptr;   // its 1-D twiddles and kernel factors
   void* stream = nullptr;
   // bounded device waits of the persistent bulk-copy kernels: limit, and the plan's
   // status word that a wait which runs out sets to CFFT_ERR_TIMEOUT

@@ -174,11 +174,10 @@ __device__ __forceinline__ void fold_emit(const T (&va)[8][VW], const T (&vb)[8]
   const C ty = ftx[iy];
 #pragma unroll
   for (int l = 0; l < VW; ++l) {
-    T a8[8], b8[8];
+    C p8[8];  // field a in the real lane, field b in the imaginary lane
 #pragma unroll
-    for (int k = 0; k < 8; ++k) { a8[k] = va[k][l]; b8[k] = vb[k][l]; }
-    wht8(a8);
-    wht8(b8);
+    for (int k = 0; k < 8; ++k) p8[k] = mk<C>(va[k][l], vb[k][l]);
+    wht8c(p8);
     const int ix = ix0 + l;
     const C tx = ftx[ix];
 #pragma unroll
@@ -188,7 +187,7 @@ __device__ __forceinline__ void fold_emit(const T (&va)[8][VW], const T (&vb)[8]
       if (o & 1) w = tx;
       if (o & 2) w = cmul(w, ty);
       if (o & 4) w = cmul(w, ftz);
-      buf[c * PL + iy * S + ix] = cmul(mk<C>(a8[o], b8[o]), w);
+      buf[c * PL + iy * S + ix] = o ? cmul(p8[o], w) : p8[o];
     }
   }
 }
@@ -1387,6 +1386,70 @@ __global__ void k_qmul_ifft_z_h(const DevGeom* __restrict__ g, const typename Cx
   for (int z = 0; z < H; ++z) dst[z * H * H] = v[z];
 }
 
+// Separable Q-multiply of the M2Q step for Pmmm-like plans (_q_multiply_separable!,
+// src/q_fused_krfft.jl:606-667; detection _is_pmmm_like, :431-454): d = 8, L = (2, 2, 2),
+// the representatives diag(s) with translations 0 or -1, and an orthogonal cell.  Then
+// B = WHT8 diag(tw^alpha) and the first row of Q = B^-1 diag(K) B gives
+//   Y'(q) = (1/8) sum_m K(q + M alpha_m) [WHT8 (tw^alpha_a(q) Y(s_a q mod M))]_m,
+// tw_d(q) = e^{2 pi i q_d / N_d}, K(h) = prod_d exp(-ds (2 pi h_c,d / a_d)^2).  Nothing is
+// tabulated per point: QS holds the 1-D twiddles (3 x H complex) and the 1-D kernel
+// factors (3 x 2H, real parts).  Same line structure as k_qmul_ifft_z_h (plain path,
+// one channel, H = M): the z line of (y, x) is assembled, inverse z FFT, stored to W2.
+template <typename T, int H>
+__global__ void k_qsep_ifft_z_h(const DevGeom* __restrict__ g, const typename Cx<T>::type* __restrict__ QS,
+                                const typename Cx<T>::type* __restrict__ WT, typename Cx<T>::type* __restrict__ W2) {
+  pdl_enter();
+  using C = typename Cx<T>::type;
+  constexpr int HV = H * H * H;
+  const int y0 = blockIdx.x * kZB, slot = blockIdx.z;
+  const int ny = min(kZB, H - y0);
+  const int yy = threadIdx.x / H, x = threadIdx.x % H;
+  if (yy >= ny) return;
+  const int y = y0 + yy;
+  const C* wt = WT + static_cast<size_t>(slot) * HV;
+  const C* tw = QS;              // tw[d * H + q]
+  const C* kf = QS + 3 * H;      // kf[d * 2H + h].x
+  int neg[8];                    // bit d: axis d negated by representative a
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+    neg[a] = (g->rep_R[a][0] < 0 ? 1 : 0) | (g->rep_R[a][4] < 0 ? 2 : 0) | (g->rep_R[a][8] < 0 ? 4 : 0);
+  const int xm = x ? H - x : 0, ym = y ? H - y : 0;
+  const C twx = tw[x], twy = tw[H + y];
+  const T kx0 = kf[x].x, kx1 = kf[x + H].x, ky0 = kf[2 * H + y].x, ky1 = kf[2 * H + y + H].x;
+  const C txy = cmul(twx, twy);
+  C v[H];
+#pragma unroll
+  for (int z = 0; z < H; ++z) {
+    const int zm = z ? H - z : 0;
+    const C twz = tw[2 * H + z];
+    C p[8];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const int gx = (neg[a] & 1) ? xm : x, gy = (neg[a] & 2) ? ym : y, gz = (neg[a] & 4) ? zm : z;
+      p[a] = wt[(gx * H + gy) * H + gz];
+    }
+    p[1] = cmul(p[1], twx);
+    p[2] = cmul(p[2], twy);
+    p[3] = cmul(p[3], txy);
+    p[4] = cmul(p[4], twz);
+    p[5] = cmul(p[5], cmul(twx, twz));
+    p[6] = cmul(p[6], cmul(twy, twz));
+    p[7] = cmul(p[7], cmul(txy, twz));
+    wht8c(p);
+    const T kz0 = kf[4 * H + z].x, kz1 = kf[4 * H + z + H].x;
+    const T k00 = kx0 * ky0, k10 = kx1 * ky0, k01 = kx0 * ky1, k11 = kx1 * ky1;
+    const T km[8] = {k00 * kz0, k10 * kz0, k01 * kz0, k11 * kz0, k00 * kz1, k10 * kz1, k01 * kz1, k11 * kz1};
+    C acc = cscale(p[0], km[0]);
+#pragma unroll
+    for (int m = 1; m < 8; ++m) acc = cadd(acc, cscale(p[m], km[m]));
+    v[z] = cscale(acc, static_cast<T>(0.125));
+  }
+  reg_fft<C, true, H>(v);
+  C* dst = W2 + static_cast<size_t>(slot) * HV + y * H + x;
+#pragma unroll
+  for (int z = 0; z < H; ++z) dst[z * H * H] = v[z];
+}
+
 constexpr int kMaxDynSmemFast = 227 * 1024;
 
 // Programmatic dependent launch of the fast-path kernels (off with CFFT_PDL=0): each
@@ -1426,14 +1489,15 @@ inline void launch_k(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cu
 
 // Persistent bulk-copy plane kernels (tma_planes.cuh).  They serve centred plans with
 // H >= 16 whose per-group stage and buffer fit at least two groups into one CTA's
-// shared memory.  CFFT_TMA selects them: "fwd" (default: the forward plane stage),
-// "all" (both stages), "0" (neither).  Measured on Im-3m 128^3 FP32: the forward one
-// matches the per-plane kernel, the backward one (12 warps per SM against 20) is 30%
-// slower, so the backward stage keeps the per-plane kernel by default.
+// shared memory.  CFFT_TMA selects them: "fwd" (the forward plane stage), "all" (both
+// stages), unset or "0" (neither).  Measured on Im-3m 128^3 FP32 (B200): the forward
+// one is 2-5% slower than the per-plane kernel and the backward one 30% slower -- with
+// one 195 KB CTA per SM they run 8 and 12 warps per SM against the per-plane kernels'
+// 20, and the FFT phases, not the loads, bound the stage -- so both are opt-in.
 inline int tma_mode() {  // bit 0: forward, bit 1: backward
   static const int m = [] {
     const char* e = std::getenv("CFFT_TMA");
-    if (!e) return 1;
+    if (!e) return 0;
     if (e[0] == '0') return 0;
     if (e[0] == 'a' || e[0] == '1') return 3;
     if (e[0] == 'b') return 2;
@@ -1887,6 +1951,13 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
         break;
       }
       default:
+        if (a.q_step && a.qsep) {
+          CFFT_FOR_H(H, {
+            launch_k(k_qsep_ifft_z_h<T, HH>, gz, thr_z, 0, st, g, static_cast<const C*>(a.QS), W,
+                     static_cast<C*>(a.W2));
+          });
+          break;
+        }
         if (a.q_step) {
           CFFT_FOR_H(H, {
             launch_k(k_qmul_ifft_z_h<T, HH>, gz, thr_z, 0, st, g, static_cast<const C*>(a.QT),

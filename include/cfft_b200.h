@@ -96,7 +96,8 @@ typedef struct cfft_info {
   int exec_path;         /* bit 0: compile-time sized kernels; bit 1: packed quad backward gather;
                             bit 2: fused 8-CTA cluster kernels; bit 3 / bit 4: persistent bulk-copy
                             (TMA) forward / backward plane kernels; bit 5: backward gather in
-                            groups of 16 (FP32) / 8 (FP64) fields (0 for host-only plans) */
+                            groups of 16 (FP32) / 8 (FP64) fields; bit 6: separable Q-multiply
+                            (Pmmm-like M2Q plans) (0 for host-only plans) */
   int chunk;             /* fields per workspace chunk */
   int lanes;             /* concurrent chunk lanes */
 } cfft_info;
