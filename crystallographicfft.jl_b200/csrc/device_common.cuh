@@ -218,6 +218,32 @@ template <> __device__ __forceinline__ void vstore<double>(double* p, const doub
   *reinterpret_cast<double2*>(p) = make_double2(in[0], in[1]);
 }
 
+// Streaming (evict-first) 16-byte loads and stores for data touched once per pass (the
+// caller's f0 in the fold and the unfold), so they do not push the channel workspace out
+// of L2 between the kernels that produce and consume it.  -DCFFT_NO_CACHE_HINTS turns
+// them into plain accesses.
+template <typename T> __device__ __forceinline__ void vload_stream(T* out, const T* p) {
+#ifdef CFFT_NO_CACHE_HINTS
+  vload<T>(out, p);
+#else
+  if constexpr (sizeof(T) == 4) {
+    const float4 v = __ldcs(reinterpret_cast<const float4*>(p));
+    out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = v.w;
+  } else {
+    const double2 v = __ldcs(reinterpret_cast<const double2*>(p));
+    out[0] = v.x; out[1] = v.y;
+  }
+#endif
+}
+template <typename T> __device__ __forceinline__ void vstore_stream(T* p, const T* in) {
+#ifdef CFFT_NO_CACHE_HINTS
+  vstore<T>(p, in);
+#else
+  if constexpr (sizeof(T) == 4) __stcs(reinterpret_cast<float4*>(p), make_float4(in[0], in[1], in[2], in[3]));
+  else __stcs(reinterpret_cast<double2*>(p), make_double2(in[0], in[1]));
+#endif
+}
+
 template <int M> __device__ __forceinline__ int mod_m(int v) {
   if constexpr ((M & (M - 1)) == 0) {
     return v & (M - 1);

@@ -229,8 +229,8 @@ __device__ __forceinline__ void fold_plane(const DevGeom* __restrict__ g, const 
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
           const int idx = ((iz + ((k >> 2) & 1) * H) * M + iy + ((k >> 1) & 1) * H) * M + ix0 + (k & 1) * H;
-          vload<T>(va[k], srca + idx);
-          if (has_b) vload<T>(vb[k], srcb + idx);
+          vload_stream<T>(va[k], srca + idx);
+          if (has_b) vload_stream<T>(vb[k], srcb + idx);
           else {
 #pragma unroll
             for (int l = 0; l < VW; ++l) vb[k][l] = zero;
@@ -353,8 +353,8 @@ __device__ __forceinline__ void unfold_plane(const DevGeom* __restrict__ g, cons
               for (int l = 0; l < VW; ++l) ob[k][l] *= ea[l];
             }
           }
-          vstore<T>(dsta + idx, oa[k]);
-          if (has_b) vstore<T>(dstb + idx, ob[k]);
+          vstore_stream<T>(dsta + idx, oa[k]);
+          if (has_b) vstore_stream<T>(dstb + idx, ob[k]);
         }
       }
     } else {
@@ -472,6 +472,12 @@ __global__ void k_plane_bwd_h(const DevGeom* __restrict__ g, const typename Cx<T
     for (int i = 0; i < H; ++i) p[i * S] = v[i];
   }
   __syncthreads();
+  // Last read of these workspace planes: drop their lines from L2 without a write-back.
+  if constexpr ((H * H * sizeof(C)) % 128 == 0) {
+    constexpr int LPP = static_cast<int>(H * H * sizeof(C) / 128);
+    for (int i = tid; i < nch * LPP; i += nth)
+      discard_l2_line(reinterpret_cast<const char*>(src0 + static_cast<size_t>(i / LPP) * HV) + (i % LPP) * 128);
+  }
   group_rows<C, true, H>(buf, nch * H, tid, nth);
   __syncthreads();
   const size_t mvol = static_cast<size_t>(g->M[0]) * g->M[1] * g->M[2];

@@ -6,7 +6,7 @@ It must agree with the generic Q path (CFFT_QSEP=0, read at plan creation) and w
 FP64 oracle's Q-matrix step and the full-grid truth (test/runtests.jl:317-402 bars:
 1e-10 against the full grid, 1e-12 against the oracle), and it must not be taken by
 groups whose representatives carry fractional (glide/screw) translations
-(src/q_fused_krfft.jl:426-429)."""
+(src/q_fused_krfft.jl:426-429).  Groups: Pmmm, Pm-3m, P4/mmm, Pm-3 and Im-3m."""
 import os
 
 import numpy as np
@@ -41,7 +41,7 @@ def _generic(cf, p, precision, **kw):
         del os.environ["CFFT_QSEP"]
 
 
-@pytest.mark.parametrize("sg", [47, 221, 123, 200])
+@pytest.mark.parametrize("sg", [47, 221, 123, 200, 229])
 def test_separable_matches_generic_oracle_and_fullgrid(cf, O, prep, sg):
     N = (32, 32, 32)
     p = prep(sg, N)
@@ -75,10 +75,11 @@ def test_separable_fp32_batched_pmmm64(cf, O, prep):
     plan.close()
 
 
-@pytest.mark.parametrize("sg", [70, 230, 229])
-def test_nonsymmorphic_or_centred_use_generic(cf, prep, sg):
-    # Fddd, Ia-3d: fractional translations in the representatives; Im-3m: centring
-    # translations N/2 -- none of them is Pmmm-like
+@pytest.mark.parametrize("sg", [70, 230])
+def test_nonsymmorphic_use_generic(cf, prep, sg):
+    # Fddd, Ia-3d: fractional (glide / screw) translations in the representatives.  (Im-3m's
+    # representatives are the eight diagonal operations with translations 0 or -1, so it
+    # is Pmmm-like and takes the separable path, as _is_pmmm_like decides.)
     p = prep(sg, (32, 32, 32))
     plan = q_plan(cf, p, cf.PATH_M2Q, DS, np.eye(3), precision=8)
     assert not plan.info.exec_path & 64
