@@ -490,8 +490,8 @@ WORKLOADS = {
                         desc="Ia-3d (No. 230) diffusion contour step exp(-w ds/2) IFFT(K FFT(exp(-w ds/2) q)), 96^3 FP32"),
     "mixed": dict(op="mixed", precision=4, batch=64,
                   desc="64 fields drawn from Pm-3m, Im-3m, Fd-3m (origin 2), Ia-3d with edges {32,48,64,96}^3, "
-                       "FP32: forward+backward and a 50-step diffusion solve each (one plan and stream per "
-                       "group and edge; the 50-step loop replays a CUDA graph)"),
+                       "FP32: forward+backward and a 50-step diffusion solve each (one autotuned plan and one "
+                       "stream per group and edge, the whole step replayed as one CUDA graph)"),
 }
 
 
@@ -603,11 +603,16 @@ def run_workload(args):
                 if count:
                     jobs.append((int(sg), int(n), count))
         built = []
+        tunings = []
         for sg, n, count in jobs:
             N = (n,) * 3
             _, ops_s = cf.find_optimal_shift(cf.get_ops(sg, 3, N), N)
             spec = cf.calc_spectral_asu(ops_s, 3, N)
-            plan = cf.KRFFTPlan(spec, ops_s, precision=rs, max_batch=count, ds=0.01)
+            # execution choices per (group, edge, batch) from the autotuner (cached)
+            tu, tms = cf.autotune_plan(spec, ops_s, N=N, precision=rs, batch=count, op="mixed", n_steps=50,
+                                       ds=0.01, cache_path=args.tune_cache)
+            tunings.append({"group": sg, "N": n, "fields": count, "tuning": tu, "tuned_ms": round(tms, 4)})
+            plan = cf.KRFFTPlan(spec, ops_s, precision=rs, max_batch=count, ds=0.01, tuning=tu)
             q = symmetric_fields(cf, torch, ops_s, N, plan.L, count, seed=sg * 1000 + n, device=dev).to(rdt).contiguous()
             w = 0.1 * symmetric_fields(cf, torch, ops_s, N, plan.L, count, seed=sg + n, device=dev).to(rdt).contiguous()
             F = torch.empty((count, plan.n_spec), dtype=torch.complex64 if rs == 4 else torch.complex128, device=dev)
@@ -628,23 +633,26 @@ def run_workload(args):
     fields = sum(j[4] for j in jobs)
     qs = [j[1].clone() for j in jobs]
     main = torch.cuda.current_stream()
-    # independent plans run on their own streams (each plan owns its workspaces)
-    streams = [torch.cuda.Stream() for _ in jobs] if len(jobs) > 1 else [main]
 
-    def step():
-        for st in streams:
-            st.wait_stream(main)
-        for (plan, q, w, F, count, _), qc, st in zip(jobs, qs, streams):
-            with torch.cuda.stream(st):
-                if W["op"] == "step":
-                    plan.step_diffusion(qc, w, 0.01, 1)
-                else:
-                    plan.forward(q, out=F)
-                    plan.backward(F, out=qc)
-                    if W["op"] == "mixed":
-                        plan.step_diffusion(qc, w, 0.01, 50)
-        for st in streams:
-            main.wait_stream(st)
+    def job(plan, q, w, F, qc):
+        def run():
+            if W["op"] == "step":
+                plan.step_diffusion(qc, w, 0.01, 1)
+            else:
+                plan.forward(q, out=F)
+                plan.backward(F, out=qc)
+                if W["op"] == "mixed":
+                    plan.step_diffusion(qc, w, 0.01, 50)
+        return run
+
+    runs = [job(plan, q, w, F, qc) for (plan, q, w, F, count, _), qc in zip(jobs, qs)]
+    if W["op"] == "mixed":
+        # every plan's work (its own stream each) replayed as one CUDA graph per step
+        step = cf.MultiPlanStep(runs)
+    else:
+        def step():
+            for r in runs:
+                r()
 
     for _ in range(args.warmup):
         step()
@@ -660,6 +668,8 @@ def run_workload(args):
     e1.record()
     torch.cuda.synchronize()
     launches = int(cf.LIB.cfft_launch_count(1))
+    if W["op"] == "mixed":
+        launches = int(step.kernels_per_run) * args.steps  # replayed graph: the kernels it holds
     ms_step = e0.elapsed_time(e1) / args.steps
     clk = clocks.stop()
     peaks = {}
@@ -679,6 +689,9 @@ def run_workload(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_source": "measured" if "hbm_gbs" in peaks else "fallback", "traffic": None},
             "gpu_launches": launches, "clocks": clk, "e2e": None}
+    if W["op"] == "mixed":
+        line["config"]["tuning"] = tunings
+        line["config"]["launch"] = "one CUDA graph per step (MultiPlanStep) over one stream per plan"
     print(json.dumps(line), flush=True)
 
 
@@ -691,6 +704,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing (profiling runs)")
+    ap.add_argument("--tune-cache", default=None, help="autotuner cache file (default ~/.cache/cfft_b200/tuning.json)")
     ap.add_argument("--workload", default="im3m128", choices=["im3m128", "scft-ia3d96"] + sorted(WORKLOADS),
                     help="im3m128 is the headline line; the others are secondary single-GPU measurements")
     args = ap.parse_args()

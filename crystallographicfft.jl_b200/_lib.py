@@ -43,6 +43,11 @@ class CFFTInfo(ctypes.Structure):
     ]
 
 
+class CFFTTuning(ctypes.Structure):
+    _fields_ = [("chunk_bytes", ctypes.c_int64), ("lanes", c_int), ("zr_slots", c_int), ("wide", c_int),
+                ("tma", c_int), ("cluster", c_int)]
+
+
 STATUS = {
     0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "not commensurate", 4: "unsupported",
     5: "timeout", 6: "allocation failed", 7: "parity class not reachable",
@@ -71,6 +76,8 @@ def _load():
         "cfft_spectral_asu": (c_int, [c_int, c_int_p, c_int, c_int32_p, c_int32_p, c_int, c_int_p, c_int32_p, c_int32_p]),
         "cfft_plan_create": (c_int, [ctypes.POINTER(CFFTDesc), ctypes.POINTER(c_void_p)]),
         "cfft_plan_create_host": (c_int, [ctypes.POINTER(CFFTDesc), ctypes.POINTER(c_void_p)]),
+        "cfft_plan_create_tuned": (c_int, [ctypes.POINTER(CFFTDesc), ctypes.POINTER(CFFTTuning),
+                                           ctypes.POINTER(c_void_p)]),
         "cfft_plan_destroy": (c_int, [c_void_p]),
         "cfft_plan_info": (c_int, [c_void_p, ctypes.POINTER(CFFTInfo)]),
         "cfft_plan_spectral_asu": (c_int, [c_void_p, c_int32_p, c_int32_p]),

@@ -131,7 +131,8 @@ cfft_status cfft_spectral_asu(int dim, const int* N, int n_ops, const int32_t* R
   return CFFT_OK;
 }
 
-static cfft_status plan_create_impl(const cfft_desc* desc, cfft_plan* plan, bool device) {
+static cfft_status plan_create_impl(const cfft_desc* desc, cfft_plan* plan, bool device,
+                                    const cfft_tuning* tuning = nullptr) {
   if (!desc || !plan) return ret(Status::kInvalid, "null argument");
   *plan = nullptr;
   std::string err;
@@ -146,6 +147,14 @@ static cfft_status plan_create_impl(const cfft_desc* desc, cfft_plan* plan, bool
   if (!p) return ret(Status::kAlloc, "host allocation failed");
   p->precision = desc->precision;
   p->max_batch = desc->max_batch;
+  if (tuning) {
+    p->tune.chunk_bytes = tuning->chunk_bytes;
+    p->tune.lanes = tuning->lanes;
+    p->tune.zr_slots = tuning->zr_slots;
+    p->tune.wide = tuning->wide;
+    p->tune.tma = tuning->tma;
+    p->tune.cluster = tuning->cluster;
+  }
   p->ds = desc->ds;
   std::memcpy(p->lattice, desc->lattice, sizeof(p->lattice));
   const bool plain = desc->path == CFFT_PATH_M2 || desc->path == CFFT_PATH_M2Q;
@@ -173,6 +182,14 @@ static cfft_status plan_create_impl(const cfft_desc* desc, cfft_plan* plan, bool
 }
 
 cfft_status cfft_plan_create(const cfft_desc* desc, cfft_plan* plan) { return plan_create_impl(desc, plan, true); }
+cfft_status cfft_plan_create_tuned(const cfft_desc* desc, const cfft_tuning* tuning, cfft_plan* plan) {
+  if (tuning && (tuning->lanes < 0 || tuning->lanes > 4 || (tuning->zr_slots && tuning->zr_slots != 2 &&
+                 tuning->zr_slots != 4) || tuning->wide < -1 || tuning->wide > 1 || tuning->tma < -1 ||
+                 tuning->tma > 3 || (tuning->cluster > 0 && tuning->cluster != 8 && tuning->cluster != 16) ||
+                 tuning->cluster < -1 || tuning->chunk_bytes < 0))
+    return ret(Status::kInvalid, "invalid tuning value");
+  return plan_create_impl(desc, plan, true, tuning);
+}
 cfft_status cfft_plan_create_host(const cfft_desc* desc, cfft_plan* plan) { return plan_create_impl(desc, plan, false); }
 
 cfft_status cfft_plan_destroy(cfft_plan plan) {
@@ -203,8 +220,8 @@ cfft_status cfft_plan_info(cfft_plan plan, cfft_info* info) {
   int tma = 0;
   if (p->fast_h > 0 && !p->cluster && p->d_geom) {
     bool fw = false, fwe = false, bw = false;
-    if (p->precision == 8) cfft::fast_tma_planes_f64(p->fast_h, p->cent_type, &fw, &fwe, &bw);
-    else cfft::fast_tma_planes_f32(p->fast_h, p->cent_type, &fw, &fwe, &bw);
+    if (p->precision == 8) cfft::fast_tma_planes_f64(p->fast_h, p->cent_type, p->tune.tma, &fw, &fwe, &bw);
+    else cfft::fast_tma_planes_f32(p->fast_h, p->cent_type, p->tune.tma, &fw, &fwe, &bw);
     tma = (fw ? 8 : 0) | (bw ? 16 : 0);
   }
   info->exec_path = (p->fast_h > 0 ? 1 : 0) | (p->reps_quad ? 2 : 0) | (p->cluster ? 4 : 0) | tma |

@@ -608,6 +608,8 @@ Status launch_stage(Plan* p, int stage, const T* f0, typename Cx<T>::type* F, co
     a.cluster_ctas = p->cluster_ctas;
     a.status = p->d_status;
     a.timeout_ns = p->timeout_ns;
+    a.zr_slots = p->tune.zr_slots;
+    a.tma = p->tune.tma;
     if (q_step) {  // stage 4: Q-multiply + inverse z FFT into the Q workspace; stage 5 reads it
       a.q_step = true;
       a.QT = p->d_qt;
@@ -916,11 +918,13 @@ Status plan_device_init(Plan* p, std::string* err) {
   // On the fast path two fields share one workspace slot, and chunks hold whole pairs.
   size_t budget = static_cast<size_t>(64) << 20;
   if (const char* cb = std::getenv("CFFT_CHUNK_BYTES")) budget = std::strtoull(cb, nullptr, 10);
+  if (p->tune.chunk_bytes > 0) budget = static_cast<size_t>(p->tune.chunk_bytes);
   const size_t per_field = T.n_ch * hvol * cs / (p->fast_h ? 2 : 1);
   size_t ch = std::max<size_t>(1, std::min<size_t>(B, budget / std::max<size_t>(per_field, 1)));
   // Batches of at least 8 fields on the fast path run as two concurrent lanes.
   p->lanes = 1;
-  if (const char* ln = std::getenv("CFFT_LANES")) p->lanes = std::max(1, std::min(Plan::kMaxLanes, std::atoi(ln)));
+  if (p->tune.lanes > 0) p->lanes = std::min(Plan::kMaxLanes, p->tune.lanes);
+  else if (const char* ln = std::getenv("CFFT_LANES")) p->lanes = std::max(1, std::min(Plan::kMaxLanes, std::atoi(ln)));
   else if (p->fast_h && B >= 8) p->lanes = 2;
   if (p->lanes > 1) ch = std::min(ch, (B + p->lanes - 1) / p->lanes);
   if (p->fast_h && ch < B && ch > 1) ch &= ~static_cast<size_t>(1);
@@ -974,7 +978,10 @@ Status plan_device_init(Plan* p, std::string* err) {
     // fused cluster kernels read the quad layout, so CFFT_CLUSTER keeps quads.
     const size_t gw = 128 / cs;
     const char* wide_env = std::getenv("CFFT_WIDE");
-    p->reps_wide = p->reps_quad && chunk >= gw && !(wide_env && wide_env[0] == '0') && !std::getenv("CFFT_CLUSTER");
+    const char* cl_env = std::getenv("CFFT_CLUSTER");
+    const bool cluster_wanted = p->tune.cluster >= 0 ? p->tune.cluster > 0 : (cl_env && std::atoi(cl_env) > 0);
+    const bool wide_wanted = p->tune.wide >= 0 ? p->tune.wide > 0 : !(wide_env && wide_env[0] == '0');
+    p->reps_wide = p->reps_quad && chunk >= gw && wide_wanted && !cluster_wanted;
     const size_t chunk4 = p->reps_wide ? (chunk + gw - 1) / gw * gw : (chunk + 3) / 4 * 4;  // whole groups of fields
     p->g0r_lane_bytes = (((p->reps_quad ? chunk4 : chunk + 1) * T.orbit_rep.size() * cs + 255) / 256) * 256;
     if ((st = alloc(&p->d_g0r, p->lanes * p->g0r_lane_bytes, "representative workspace")) != Status::kOk) return st;
@@ -1081,7 +1088,7 @@ Status plan_device_init(Plan* p, std::string* err) {
     // faster (1.66 vs 1.90 / 2.07 us per Im-3m 128^3 field), because one slot per SM
     // group serialises the load, transform and exchange phases.
     const char* ce = std::getenv("CFFT_CLUSTER");
-    const int want = ce ? std::atoi(ce) : 0;
+    const int want = p->tune.cluster >= 0 ? p->tune.cluster : (ce ? std::atoi(ce) : 0);
     p->cluster_ctas = want == 16 ? 16 : 8;
     p->cluster = want != 0 && !p->qmode && p->reps_quad && fast_cluster_fits(p->fast_h, T.n_ch, p->precision);
     if (p->cluster) {

@@ -7,8 +7,20 @@
 
 namespace cfft {
 
+// Per-plan execution choices (cfft_plan_create_tuned); unset fields (0 / -1) fall back
+// to the process defaults (environment switches, then built-in defaults).
+struct Tuning {
+  int64_t chunk_bytes = 0;  // channel workspace per chunk
+  int lanes = 0;            // concurrent chunk lanes
+  int zr_slots = 0;         // slots per CTA of the fused z FFT + gather (2 or 4)
+  int wide = -1;            // backward gather in 128-byte field groups
+  int tma = -1;             // bulk-copy plane kernels: bit 0 forward, bit 1 backward
+  int cluster = -1;         // fused cluster kernels: 0, 8 or 16 CTAs
+};
+
 struct Plan {
   PlanTables T;
+  Tuning tune;
   int precision = 4;   // 4 = float, 8 = double
   int max_batch = 1;
   double lattice[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};

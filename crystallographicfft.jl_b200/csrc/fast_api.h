@@ -51,6 +51,9 @@ struct FastArgs {
   // status word that a wait which runs out sets to CFFT_ERR_TIMEOUT
   unsigned long long timeout_ns = 1000000000ull;
   int* status = nullptr;
+  // per-plan choices (0 / -1: the process default)
+  int zr_slots = 0;
+  int tma = -1;
 };
 
 // Stages 0 and 5 (plane kernels) and stages 1-4 (z FFTs, gathers).
@@ -64,8 +67,8 @@ Status fast_cluster_probe_f32(int H, int ct, int kc, int* max_clusters, std::str
 Status fast_cluster_probe_f64(int H, int ct, int kc, int* max_clusters, std::string* err);
 // Whether the persistent bulk-copy plane kernels serve channel edge H and centring
 // type ct (forward without / with interaction factors, backward).
-void fast_tma_planes_f32(int H, int ct, bool* fwd, bool* fwd_e, bool* bwd);
-void fast_tma_planes_f64(int H, int ct, bool* fwd, bool* fwd_e, bool* bwd);
+void fast_tma_planes_f32(int H, int ct, int tma, bool* fwd, bool* fwd_e, bool* bwd);
+void fast_tma_planes_f64(int H, int ct, int tma, bool* fwd, bool* fwd_e, bool* bwd);
 // Launches the bounded-wait self-test kernel (k_wait_selftest) on `stream`.
 Status fast_wait_selftest(unsigned long long timeout_ns, int* status, void* stream, std::string* err);
 // Per-device set-up of each unit: constant-memory twiddles and shared-memory limits.

@@ -1752,14 +1752,15 @@ Status fast_unit_cluster_probe(int H, int ct, int kc, int* max_clusters, std::st
 }
 
 template <typename T>
-void fast_unit_tma_planes(int H, int ct, bool* fwd, bool* fwd_e, bool* bwd) {
+void fast_unit_tma_planes(int H, int ct, int tma, bool* fwd, bool* fwd_e, bool* bwd) {
   *fwd = *fwd_e = *bwd = false;
-  if (!tma_enabled() || !fast_size_ok(H, sizeof(T))) return;
+  const int mode = tma >= 0 ? tma : tma_mode();
+  if (!mode || !fast_size_ok(H, sizeof(T))) return;
   CFFT_FOR_H(H, {
     CFFT_FOR_CT(ct, {
-      *fwd = (tma_mode() & 1) && fwd_tma_fits<T, HH, CTT, false>();
-      *fwd_e = (tma_mode() & 1) && fwd_tma_fits<T, HH, CTT, true>();
-      *bwd = (tma_mode() & 2) && bwd_tma_fits<T, HH, CTT>();
+      *fwd = (mode & 1) && fwd_tma_fits<T, HH, CTT, false>();
+      *fwd_e = (mode & 1) && fwd_tma_fits<T, HH, CTT, true>();
+      *bwd = (mode & 2) && bwd_tma_fits<T, HH, CTT>();
     });
   });
 }
@@ -1807,8 +1808,8 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
     const size_t smem_plane = static_cast<size_t>(nch) * H * (H + 1) * cs;
     const int ntasks = nslots * H;
     auto al16 = [](const void* p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
-    const bool tma = tma_enabled() && al16(f0) && al16(E) && al16(f0_out) && al16(W) &&
-                     (tma_mode() & (a.stage == 0 ? 1 : 2));
+    const int tmode = a.tma >= 0 ? a.tma : tma_mode();
+    const bool tma = al16(f0) && al16(E) && al16(f0_out) && al16(W) && (tmode & (a.stage == 0 ? 1 : 2));
     if (a.stage == 0) {
       CFFT_FOR_H(H, {
         CFFT_FOR_CT(a.cent_type, {
@@ -1901,7 +1902,7 @@ Status fast_unit_launch(const FastArgs& a, std::string* err) {
       }
       case 6: {
         // fused z FFT + diagonal-sign gather, ZR_SLOTS workspace slots per CTA
-        const int sl = zr_slots();
+        const int sl = a.zr_slots == 2 || a.zr_slots == 4 ? a.zr_slots : zr_slots();
         const T* K = static_cast<const T*>(a.K);
         const uint32_t* sh = static_cast<const uint32_t*>(a.spec_h);
         const uint4* un = static_cast<const uint4*>(a.zr_units);

@@ -22,7 +22,7 @@ import ctypes
 import numpy as np
 
 from . import symmetry as sym
-from ._lib import LIB, CFFTDesc, CFFTError, CFFTInfo, check
+from ._lib import LIB, CFFTDesc, CFFTError, CFFTInfo, CFFTTuning, check
 
 PATH_AUTO, PATH_M2, PATH_CENTERED, PATH_M2Q, PATH_M7, PATH_FULLGRID = 0, 1, 2, 3, 4, 5
 _REAL = {4: np.float32, 8: np.float64}
@@ -44,8 +44,10 @@ class KRFFTPlan:
     the SCFT diffusion step share it.  Mirrors GeneralCFFTPlan / CenteredKRFFTPlan /
     M2BackwardPlan / CenteredKRFFTBackwardPlan / CenteredSCFTPlan / M2SCFTPlan."""
 
+    TUNING_DEFAULTS = dict(chunk_bytes=0, lanes=0, zr_slots=0, wide=-1, tma=-1, cluster=-1)
+
     def __init__(self, spec, ops_shifted, *, N=None, ds=0.0, lattice=None, precision=8, max_batch=1,
-                 path=PATH_AUTO, device=True):
+                 path=PATH_AUTO, device=True, tuning=None):
         N = tuple(spec.N if N is None else N)
         dim = len(N)
         self.spec = spec
@@ -77,8 +79,13 @@ class KRFFTPlan:
         d.max_batch = self.max_batch
         d.path = int(path)
         h = ctypes.c_void_p()
-        create = LIB.cfft_plan_create if device else LIB.cfft_plan_create_host
-        check(create(ctypes.byref(d), ctypes.byref(h)))
+        self.tuning = dict(self.TUNING_DEFAULTS, **(tuning or {}))
+        if tuning and device:
+            tu = CFFTTuning(**self.tuning)
+            check(LIB.cfft_plan_create_tuned(ctypes.byref(d), ctypes.byref(tu), ctypes.byref(h)))
+        else:
+            create = LIB.cfft_plan_create if device else LIB.cfft_plan_create_host
+            check(create(ctypes.byref(d), ctypes.byref(h)))
         self._h = h
         info = CFFTInfo()
         check(LIB.cfft_plan_info(h, ctypes.byref(info)))

@@ -166,6 +166,19 @@ cfft_status cfft_spectral_asu(int dim, const int* N, int n_ops, const int32_t* R
  * (src/centering_fold.jl:328,630,868; src/krfft.jl:301,1101; src/q_fused_krfft.jl:948):
  * one plan holds the forward, backward and diffusion-step state for a batch. */
 cfft_status cfft_plan_create(const cfft_desc* desc, cfft_plan* plan);
+/* Execution choices of one plan (no reference counterpart: the autotuner's knobs).
+ * Zero / -1 fields keep the default (the environment switch of the same name, then the
+ * built-in default measured best on Im-3m 128^3). */
+typedef struct cfft_tuning {
+  int64_t chunk_bytes;   /* channel workspace per chunk (CFFT_CHUNK_BYTES; 64 MiB) */
+  int lanes;             /* concurrent chunk lanes 1..4 (CFFT_LANES; 2 for batches >= 8) */
+  int zr_slots;          /* workspace slots per CTA of the fused z FFT + gather, 2 or 4 (CFFT_ZR_SLOTS; 4) */
+  int wide;              /* backward gather in 128-byte field groups: 0, 1 (CFFT_WIDE; 1) */
+  int tma;               /* bulk-copy plane kernels: 0, 1 forward, 2 backward, 3 both (CFFT_TMA; 0) */
+  int cluster;           /* fused cluster kernels: 0, 8 or 16 CTAs (CFFT_CLUSTER; 0) */
+} cfft_tuning;
+/* cfft_plan_create with explicit execution choices (tuning may be NULL). */
+cfft_status cfft_plan_create_tuned(const cfft_desc* desc, const cfft_tuning* tuning, cfft_plan* plan);
 /* Same plan-time tables without any device state (no GPU needed); execute calls on
  * such a plan return CFFT_ERR_INVALID.  For table inspection and host tooling. */
 cfft_status cfft_plan_create_host(const cfft_desc* desc, cfft_plan* plan);
