@@ -495,85 +495,84 @@ WORKLOADS = {
 }
 
 
-SCFT_CONFIG = dict(sg=230, n=96, f=0.4, chiN=20.0, Ns=100, history=20, tol=1e-6, switch=1e-4, sigma=2.0,
-                   amplitude=1.0, cell=3.8 * np.sqrt(6.0))
+SCFT_CONFIG = dict(sg=230, n=96, f=0.4, chiN=20.0, Ns=100, history=20, tol=1e-6, switch=1e-5, sigma=2.0,
+                   amplitude=1.0)
+SNO_WEIGHTS = os.path.join(ROOT, "crystallographicfft.jl_b200", "data", "sno_warmstart.npy")
 
 
 def run_scft(args):
     """SCFT time-to-tolerance, AB diblock in Ia-3d (No. 230) on 96^3: f = 0.4, chiN = 20,
-    Ns = 100, Anderson history 20, residual 1e-6.  One step = one solve from the seeded
-    start (Gaussian-filtered noise, sigma = 2 grid points, amplitude 1.0, symmetrised):
-    FP32 fields and propagators until the residual is below 1e-4, then the same fields
-    in FP64 to 1e-6 (FP32 rounding leaves a residual floor near 2e-6 at 96^3).  Q, F and
-    the mixing solve are FP64 on the device throughout."""
+    Ns = 100, Anderson history 20, residual 1e-6, cell 3.8 b sqrt(N), learned warm start
+    against the plain start.  One step = one solve from each start: FP32 fields and
+    propagators to a residual of 1e-5, then the same fields in FP64 to 1e-6 (FP32 rounding
+    leaves a residual floor near 2e-6 at 96^3); Q, F and the mixing solve are FP64 on the
+    device throughout.
+    - plain: the seeded start (Gaussian-filtered noise, sigma 2 grid points, amplitude
+      1.0, symmetrised), simple mixing for 100 iterations (the gyroid grows out of the
+      unstable modes; Anderson mixing from this near-uniform start converges to the
+      disordered state), then Anderson mixing;
+    - learned: the spectral neural operator's prediction on the 96^3 grid (trained at
+      64^3 on the driver's own converged fields; its inference is inside the timed
+      region), Anderson mixing from the first iteration."""
     import torch
 
     cf = load_package()
-    C = SCFT_CONFIG
-    dev = torch.device("cuda", 0)
-    torch.cuda.set_device(0)
-    N = (C["n"],) * 3
-    _, ops_s = cf.find_optimal_shift(cf.get_ops(C["sg"], 3, N), N)
-    kw = dict(f=C["f"], chiN=C["chiN"], Ns=C["Ns"], history=C["history"], max_iter=1000)
-    p32, s32 = cf.plan_scft(C["sg"], N, C["cell"], precision=4, ops=ops_s, tol=C["switch"], **kw)
-    p64, s64 = cf.plan_scft(C["sg"], N, C["cell"], precision=8, ops=ops_s, tol=C["tol"], **kw)
-    w0 = cf.initial_fields(ops_s, N, p32.L, C["f"], C["chiN"], seed=0, sigma=C["sigma"], amplitude=C["amplitude"])
-    w0_32 = torch.tensor(w0, dtype=torch.float32, device=dev).contiguous()
-    s32.evaluate(w0_32)  # captures the propagator graphs
-    s64.evaluate(w0_32.double())
+    from crystallographicfft_b200 import warmstart as ws
 
-    def solve():
-        w = w0_32.clone()
-        a = s32.solve(w)
-        w64 = w.double()
-        b = s64.solve(w64)
+    C = SCFT_CONFIG
+    torch.cuda.set_device(0)
+    gg = ws.GroupGrid(C["sg"], C["n"], Ns=C["Ns"])
+    plan = cf.KRFFTPlan(gg.spec, gg.ops, N=gg.N, precision=4, max_batch=32)
+    model = cf.SpectralNeuralOperator()
+    model.load(SNO_WEIGHTS)
+    ctx = model.bind(plan, C["sg"], gg.shift, 1)
+    plain0 = torch.tensor(gg.plain_start(C["f"], C["chiN"], plan.L), dtype=torch.float32, device="cuda")
+
+    def predict():
+        return ctx.predict([(C["chiN"], C["f"])])[0]
+
+    def once():
+        a = ws.time_to_tol(gg, C["chiN"], C["f"], plain0, warm=False, tol=C["tol"], switch=C["switch"])
+        b = ws.time_to_tol(gg, C["chiN"], C["f"], None, warm=True, tol=C["tol"], switch=C["switch"], predict=predict)
         return a, b
 
     for _ in range(args.warmup):
-        solve()
+        once()
     torch.cuda.synchronize()
     clocks = ClockSampler(0)
     clocks.start()
     time.sleep(0.3)
     cf.LIB.cfft_launch_count(1)
-    times, res = [], None
-    for _ in range(args.steps):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        res = solve()
-        e1.record()
-        torch.cuda.synchronize()
-        times.append(e0.elapsed_time(e1) / 1000.0)
+    runs = [once() for _ in range(args.steps)]
     launches = int(cf.LIB.cfft_launch_count(1))
     clk = clocks.stop()
-    a, b = res
-    # per-iteration evaluation time of each precision (the solves synchronise every iteration)
-    ev = {}
-    for name, sol, w in (("fp32", s32, w0_32), ("fp64", s64, w0_32.double())):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(5):
-            sol.evaluate(w)
-        e1.record()
-        torch.cuda.synchronize()
-        ev[name] = e0.elapsed_time(e1) / 5
-    mean_s = float(np.mean(times))
-    line = {"metric": "SCFT time-to-tol, s per solve (AB diblock, Ia-3d 96^3, f=0.4, chiN=20, Ns=100, "
-                      "Anderson 20, residual 1e-6; plain seeded start)",
-            "value": mean_s, "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": mean_s * 1000.0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32+f64", "data": "synthetic",
+    plain_s = [a["seconds"] for a, _ in runs]
+    learned_s = [b["seconds"] for _, b in runs]
+    a, b = runs[-1]
+    mean_l, mean_p = float(np.mean(learned_s)), float(np.mean(plain_s))
+    line = {"metric": "SCFT time-to-tol, s per solve, learned warm start vs plain (AB diblock, Ia-3d 96^3, f=0.4, "
+                      "chiN=20, Ns=100, Anderson 20, residual 1e-6)",
+            "value": mean_l, "unit": "s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": (mean_l + mean_p) * 1000.0, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64 (network bf16 weights, f32 accumulate)", "data": "synthetic",
             "config": {"workload": "scft-ia3d96", "group": C["sg"], "N": C["n"], "f": C["f"], "chiN": C["chiN"],
                        "Ns": C["Ns"], "anderson_history": C["history"], "tol": C["tol"],
-                       "cell": "3.8 b sqrt(N) = %.4f Rg" % C["cell"],
-                       "start": "seeded Gaussian-filtered noise, sigma 2 grid points, amplitude 1.0, symmetrised",
+                       "cell": "3.8 b sqrt(N) = %.4f Rg" % ws.CELL,
+                       "plain_start": "seeded Gaussian-filtered noise, sigma 2 grid points, amplitude 1.0, "
+                                      "symmetrised; %d simple-mixing iterations, then Anderson" % ws.PLAIN["min_simple"],
+                       "learned_start": "spectral neural operator prediction (weights %s), Anderson from the start"
+                                        % os.path.relpath(SNO_WEIGHTS, ROOT),
                        "phases": "FP32 to residual %.0e, then FP64 to %.0e" % (C["switch"], C["tol"])},
-            "result": {"F": b["F"], "Q": b["Q"], "residual": b["err"], "converged": b["converged"],
-                       "iterations_fp32": a["iterations"], "iterations_fp64": b["iterations"],
+            "result": {"plain_seconds": mean_p, "learned_seconds": mean_l, "speedup": mean_p / mean_l,
+                       "F_plain": a["F"], "F_learned": b["F"], "dF": abs(a["F"] - b["F"]),
+                       "residual_plain": a["err"], "residual_learned": b["err"],
+                       "converged": bool(a["converged"] and b["converged"]),
+                       "iterations_plain": [a["iterations_fp32"], a["iterations_fp64"]],
+                       "iterations_learned": [b["iterations_fp32"], b["iterations_fp64"]],
                        "disordered_F": C["chiN"] * C["f"] * (1 - C["f"]),
-                       "solve_s": [round(t, 4) for t in times]},
-            "evaluate_ms": ev, "gpu_launches": launches, "clocks": clk, "e2e": None, "roofline": None}
-    for o in (s32, s64, p32, p64):
+                       "plain_s": [round(t, 4) for t in plain_s], "learned_s": [round(t, 4) for t in learned_s]},
+            "gpu_launches": launches, "clocks": clk, "e2e": None, "roofline": None}
+    for o in (ctx, model, plan):
         o.close()
     print(json.dumps(line), flush=True)
 

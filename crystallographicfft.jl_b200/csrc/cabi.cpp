@@ -8,6 +8,7 @@
 #include "exec.h"
 #include "fast_api.h"
 #include "scft.h"
+#include "sno.h"
 
 using cfft::Status;
 
@@ -369,11 +370,83 @@ cfft_status cfft_scft_create(cfft_plan plan, const cfft_scft_params* params, cff
   prm.lam_simple = params->lam_simple;
   prm.lam_anderson = params->lam_anderson;
   prm.anderson_start = params->anderson_start;
+  prm.min_simple = params->min_simple;
   std::string err;
   cfft::Scft* s = nullptr;
   const Status st = cfft::scft_create(reinterpret_cast<cfft::Plan*>(plan), prm, &s, &err);
   if (st == Status::kOk) *scft = reinterpret_cast<cfft_scft>(s);
   return ret(st, err);
+}
+
+int64_t cfft_sno_param_count(void) { return cfft::SnoLayout::total; }
+
+cfft_status cfft_sno_create(const cfft_sno_config* cfg, cfft_sno* model) {
+  if (!model) return ret(Status::kInvalid, "null argument");
+  cfft::SnoConfig c;
+  if (cfg) {
+    c.lr = cfg->lr;
+    c.beta1 = cfg->beta1;
+    c.beta2 = cfg->beta2;
+    c.eps = cfg->eps;
+    c.weight_decay = cfg->weight_decay;
+  }
+  std::string err;
+  cfft::SnoModel* m = nullptr;
+  const Status st = cfft::sno_model_create(c, &m, &err);
+  if (st == Status::kOk) *model = reinterpret_cast<cfft_sno>(m);
+  return ret(st, err);
+}
+
+cfft_status cfft_sno_destroy(cfft_sno model) {
+  cfft::sno_model_destroy(reinterpret_cast<cfft::SnoModel*>(model));
+  return CFFT_OK;
+}
+
+cfft_status cfft_sno_set_params(cfft_sno model, const float* host) {
+  if (!model || !host) return ret(Status::kInvalid, "null argument");
+  std::string err;
+  return ret(cfft::sno_set_params(reinterpret_cast<cfft::SnoModel*>(model), host, &err), err);
+}
+
+cfft_status cfft_sno_get_params(cfft_sno model, float* host) {
+  if (!model || !host) return ret(Status::kInvalid, "null argument");
+  std::string err;
+  return ret(cfft::sno_get_params(reinterpret_cast<cfft::SnoModel*>(model), host, &err), err);
+}
+
+cfft_status cfft_sno_get_grads(cfft_sno model, float* host) {
+  if (!model || !host) return ret(Status::kInvalid, "null argument");
+  std::string err;
+  return ret(cfft::sno_get_grads(reinterpret_cast<cfft::SnoModel*>(model), host, &err), err);
+}
+
+cfft_status cfft_sno_bind(cfft_sno model, cfft_plan plan, int group_slot, const double* shift, int max_samples,
+                          cfft_sno_ctx* ctx) {
+  if (!model || !plan || !shift || !ctx) return ret(Status::kInvalid, "null argument");
+  std::string err;
+  cfft::SnoCtx* c = nullptr;
+  const Status st = cfft::sno_bind(reinterpret_cast<cfft::SnoModel*>(model), reinterpret_cast<cfft::Plan*>(plan),
+                                   group_slot, shift, max_samples, &c, &err);
+  if (st == Status::kOk) *ctx = reinterpret_cast<cfft_sno_ctx>(c);
+  return ret(st, err);
+}
+
+cfft_status cfft_sno_unbind(cfft_sno_ctx ctx) {
+  cfft::sno_unbind(reinterpret_cast<cfft::SnoCtx*>(ctx));
+  return CFFT_OK;
+}
+
+cfft_status cfft_sno_predict(cfft_sno_ctx ctx, const double* params, int n_samples, void* w_out, void* stream) {
+  std::string err;
+  return ret(cfft::sno_predict(reinterpret_cast<cfft::SnoCtx*>(ctx), params, n_samples, w_out, stream, &err), err);
+}
+
+cfft_status cfft_sno_train(cfft_sno_ctx ctx, const double* params, int n_samples, const void* w_target, double lr,
+                           int step, double* loss, void* stream) {
+  std::string err;
+  return ret(cfft::sno_train(reinterpret_cast<cfft::SnoCtx*>(ctx), params, n_samples, w_target, lr, step, loss, stream,
+                             &err),
+             err);
 }
 
 cfft_status cfft_scft_destroy(cfft_scft scft) {

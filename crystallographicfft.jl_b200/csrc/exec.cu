@@ -1345,7 +1345,11 @@ Status exec_step_diffusion(Plan* p, void* q, const void* w, double dt, int n_ste
   const size_t n = static_cast<size_t>(B) * p->T.M[0] * p->T.M[1] * p->T.M[2];
   const int grid = static_cast<int>(std::min<size_t>((n + 255) / 256, 148 * 16));
   const char* ge = std::getenv("CFFT_STEP_GRAPH");
-  const bool graph = n_steps >= kGraphMinSteps && !(ge && ge[0] == '0');
+  // Inside the caller's own stream capture the steps are recorded as plain launches:
+  // a graph cannot be launched into (or captured beside) a capturing stream.
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cap) != cudaSuccess) cudaGetLastError();
+  const bool graph = n_steps >= kGraphMinSteps && !(ge && ge[0] == '0') && cap == cudaStreamCaptureStatusNone;
   bool done = false;
   if (p->precision == 8) {
     k_interaction<double><<<grid, 256, 0, s>>>(static_cast<const double*>(w), static_cast<double*>(p->d_work_E), dt / 2, n);

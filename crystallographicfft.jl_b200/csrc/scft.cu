@@ -9,7 +9,8 @@
 //   phi_B over [f, 1] (Simpson's rule, trapezoid for an odd block);
 //   d_A = chiN (phi_B - 1/2) + (w_B - w_A)/2, d_B = chiN (phi_A - 1/2) + (w_A - w_B)/2;
 //   err = sqrt(sum d^2 / sum w^2), F = -ln Q + <chiN phi_A phi_B - w_A phi_A - w_B phi_B>;
-//   simple mixing (w += lam_s d) while err > anderson_start, then Anderson mixing over
+//   simple mixing (w += lam_s d) for the first min_simple iterations and while
+//   err > anderson_start, then Anderson mixing over
 //   the last `history` iterates (U c = V from the Gram matrix of the residuals).
 //
 // Fields live on the plan's stride-L subgrid (M-grid): for fields symmetric under the
@@ -382,7 +383,7 @@ Status solve_t(Scft* S, T* w, ScftState* out, cudaStream_t st, std::string* err)
     rs.slot[0] = k;
     T* wnext = Wr + static_cast<size_t>((it + 1) % R) * n2;
     double lam;
-    if (out->err > S->prm.anderson_start) {
+    if (out->err > S->prm.anderson_start || it < S->prm.min_simple) {
       hist = 0;
       start = it + 1;
       rs.m = 0;
@@ -418,8 +419,8 @@ Status scft_create(Plan* p, const ScftParams& prm, Scft** out, std::string* err)
   if (!p->d_geom) { *err = "the SCFT driver needs a device plan"; return Status::kInvalid; }
   if (p->max_batch < 2) { *err = "the SCFT driver needs a plan with max_batch >= 2 (q and q_dagger)"; return Status::kInvalid; }
   if (prm.Ns < 2 || prm.f <= 0.0 || prm.f >= 1.0 || prm.history < 0 || prm.history > kScftMaxHistory ||
-      prm.max_iter < 0 || !(prm.tol > 0.0)) {
-    *err = "invalid SCFT parameters (Ns >= 2, 0 < f < 1, 0 <= history <= 32, tol > 0)";
+      prm.max_iter < 0 || !(prm.tol > 0.0) || prm.min_simple < 0) {
+    *err = "invalid SCFT parameters (Ns >= 2, 0 < f < 1, 0 <= history <= 32, tol > 0, min_simple >= 0)";
     return Status::kInvalid;
   }
   const int NA = static_cast<int>(std::lround(prm.f * prm.Ns));

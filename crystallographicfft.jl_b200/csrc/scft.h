@@ -19,6 +19,7 @@ struct ScftParams {
   double lam_simple = 0.1;    // simple-mixing step while err > anderson_start
   double lam_anderson = 1.0;  // Anderson mixing step
   double anderson_start = 0.2;
+  int min_simple = 0;         // simple-mixing iterations before Anderson mixing may start
 };
 
 struct ScftState {

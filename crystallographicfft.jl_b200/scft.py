@@ -20,7 +20,7 @@ from .plans import KRFFTPlan, _torch
 class _Params(ctypes.Structure):
     _fields_ = [("f", ctypes.c_double), ("chiN", ctypes.c_double), ("Ns", ctypes.c_int), ("history", ctypes.c_int),
                 ("tol", ctypes.c_double), ("max_iter", ctypes.c_int), ("lam_simple", ctypes.c_double),
-                ("lam_anderson", ctypes.c_double), ("anderson_start", ctypes.c_double)]
+                ("lam_anderson", ctypes.c_double), ("anderson_start", ctypes.c_double), ("min_simple", ctypes.c_int)]
 
 
 class _State(ctypes.Structure):
@@ -48,13 +48,15 @@ def _state(s):
 class SCFTSolver:
     """Self-consistent field iteration of an incompressible AB diblock melt on `plan`
     (whose ds must be 1/Ns and max_batch at least 2): A-block fraction f, chiN, Ns
-    contour steps, Anderson mixing over `history` iterates below `anderson_start`."""
+    contour steps, Anderson mixing over `history` iterates below `anderson_start` once
+    `min_simple` simple-mixing iterations have run."""
 
     def __init__(self, plan, f, chiN, Ns, *, history=20, tol=1e-6, max_iter=1000, lam_simple=0.1,
-                 lam_anderson=1.0, anderson_start=0.2):
+                 lam_anderson=1.0, anderson_start=0.2, min_simple=0):
         self.plan = plan
         self.params = dict(f=f, chiN=chiN, Ns=Ns, history=history, tol=tol, max_iter=max_iter,
-                           lam_simple=lam_simple, lam_anderson=lam_anderson, anderson_start=anderson_start)
+                           lam_simple=lam_simple, lam_anderson=lam_anderson, anderson_start=anderson_start,
+                           min_simple=min_simple)
         p = _Params(**self.params)
         h = ctypes.c_void_p()
         check(LIB.cfft_scft_create(plan.handle, ctypes.byref(p), ctypes.byref(h)))

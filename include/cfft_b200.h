@@ -276,7 +276,8 @@ cfft_status cfft_wait_selftest(cfft_plan plan, unsigned long long timeout_ns, vo
  * step), Q = <q(r, 1)>, densities by Simpson's rule, residuals
  * d_A = chiN (phi_B - 1/2) + (w_B - w_A)/2, d_B = chiN (phi_A - 1/2) + (w_A - w_B)/2,
  * err = sqrt(sum d^2 / sum w^2), F = -ln Q + <chiN phi_A phi_B - w_A phi_A - w_B phi_B>,
- * simple mixing above anderson_start, Anderson mixing below.  Q, F, the residual
+ * simple mixing for the first min_simple iterations and above anderson_start, Anderson
+ * mixing after.  Q, F, the residual
  * norms, the Anderson Gram matrix and its least-squares solve are FP64 on the device.
  * Fields are [w_A | w_B] on the plan's M-grid (2 x M1 M2 M3 reals of the plan's
  * precision, device memory). */
@@ -290,6 +291,9 @@ typedef struct cfft_scft_params {
   double lam_simple;     /* simple-mixing step (err > anderson_start) */
   double lam_anderson;   /* Anderson mixing step */
   double anderson_start; /* residual below which Anderson mixing runs */
+  int min_simple;        /* simple-mixing iterations before Anderson mixing may start: from a
+                            near-uniform start the ordered structure must first grow out of the
+                            unstable modes, or Anderson mixing converges to the disordered state */
 } cfft_scft_params;
 typedef struct cfft_scft_state {
   double Q, F, err;
@@ -308,6 +312,49 @@ cfft_status cfft_scft_evaluate(cfft_scft scft, const void* w, void* phi, void* d
 cfft_status cfft_scft_solve(cfft_scft scft, void* w, cfft_scft_state* state, void* stream);
 /* Densities [phi_A | phi_B] of the last evaluation (device copy on `stream`). */
 cfft_status cfft_scft_densities(cfft_scft scft, void* phi, void* stream);
+
+/* ---------------- learned warm start (spectral neural operator) ----------------
+ * No reference counterpart: a network that predicts SCFT fields [w_A | w_B] of an AB
+ * diblock melt from (chiN, f) and the space group (one-hot slot 0 Im-3m, 1 Ia-3d,
+ * 2 Pm-3m), trained on converged fields of the SCFT driver above, used as its starting
+ * point.  Lift of 21 input channels (chiN, f, the group one-hot and the symmetrised
+ * plane waves of 8 reflections) to 32 channels, 4 Fourier layers (a 1 x 1 channel map
+ * plus a spectral convolution with one real 32 x 32 matrix per mode class, 12 retained
+ * modes per axis, gelu), a 32 -> 64 -> 2 projection.  The spectral convolution runs on
+ * the plan's own KRFFT (the 32 channels of every sample as one batch); the channel maps
+ * run on the tensor cores with BF16 weights and FP32 accumulation.  Fields live on the
+ * plan's M-grid: FP32 plans of a cubic group on a cubic grid with M1 M2 M3 a multiple of
+ * 128, max_batch >= 32 * max_samples, max_samples <= 32.  A model's weights are shared
+ * by all its bound contexts (one per plan), so one model trains on several groups and
+ * grids; parameters are cfft_sno_param_count() floats in the library's fixed order. */
+typedef struct cfft_sno_config {
+  double lr, beta1, beta2, eps, weight_decay; /* Adam (decoupled weight decay) */
+} cfft_sno_config;
+typedef struct cfft_sno_s* cfft_sno;
+typedef struct cfft_sno_ctx_s* cfft_sno_ctx;
+int64_t cfft_sno_param_count(void);
+/* A model with seeded initial weights (cfg may be NULL for the defaults 1e-3, 0.9,
+ * 0.999, 1e-8, 0). */
+cfft_status cfft_sno_create(const cfft_sno_config* cfg, cfft_sno* model);
+cfft_status cfft_sno_destroy(cfft_sno model);
+cfft_status cfft_sno_set_params(cfft_sno model, const float* host);
+cfft_status cfft_sno_get_params(cfft_sno model, float* host);
+/* Gradients of the last cfft_sno_train call (host copy, parameter order). */
+cfft_status cfft_sno_get_grads(cfft_sno model, float* host);
+/* Binds the model to a plan: shift is the fractional origin shift of the plan's
+ * operations (find_optimal_shift), so the input features are the same functions of
+ * position on every grid. */
+cfft_status cfft_sno_bind(cfft_sno model, cfft_plan plan, int group_slot, const double* shift, int max_samples,
+                          cfft_sno_ctx* ctx);
+cfft_status cfft_sno_unbind(cfft_sno_ctx ctx);
+/* params = n_samples pairs (chiN, f) on the host; w_out = n_samples x [w_A | w_B]
+ * (n_samples x 2 x M-grid floats, device).  Synchronises the stream. */
+cfft_status cfft_sno_predict(cfft_sno_ctx ctx, const double* params, int n_samples, void* w_out, void* stream);
+/* Loss (mean square of (w - w_target) / chiN over samples, both fields and grid
+ * points) and gradients for targets w_target (device, the layout of w_out); step != 0
+ * then applies one Adam step with learning rate lr.  Synchronises the stream. */
+cfft_status cfft_sno_train(cfft_sno_ctx ctx, const double* params, int n_samples, const void* w_target, double lr,
+                           int step, double* loss, void* stream);
 
 /* ---------------- diagnostics ---------------- */
 /* Forward then backward of one batch with a CUDA event between every launch;

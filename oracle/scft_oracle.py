@@ -18,7 +18,8 @@ the library's device driver (cfft_scft_*) can be checked against it:
   d_A = chiN (phi_B - 1/2) + (w_B - w_A)/2,  d_B = chiN (phi_A - 1/2) + (w_A - w_B)/2;
   error = sqrt(sum(d_A^2 + d_B^2) / sum(w_A^2 + w_B^2)).
 - Free energy per chain: F = -ln Q + <chiN phi_A phi_B - w_A phi_A - w_B phi_B>.
-- Mixing: simple mixing w += lam_s d while the error is above `anderson_start`, then
+- Mixing: simple mixing w += lam_s d for the first `min_simple` iterations and while the
+  error is above `anderson_start`, then
   Anderson mixing (D. G. Anderson, J. ACM 12, 547 (1965); as used for SCFT by
   R. B. Thompson et al., J. Chem. Phys. 120, 31 (2004) and M. W. Matsen, Eur. Phys. J.
   E 30, 361 (2009)) over the last `history` iterations:
@@ -47,12 +48,13 @@ def simpson_weights(n):
 
 class SCFTOracle:
     def __init__(self, ops_shifted, N, f, chiN, Ns, lattice, history=20, lam_simple=0.1, lam_anderson=1.0,
-                 anderson_start=0.2):
+                 anderson_start=0.2, min_simple=0):
         self.N, self.f, self.chiN, self.Ns = tuple(N), float(f), float(chiN), int(Ns)
         self.NA = int(round(self.f * self.Ns))
         self.ds = 1.0 / self.Ns
         self.plan = O.plan_m2_scft_ops(ops_shifted, self.N, self.ds, lattice)
         self.history, self.lam_s, self.lam_a, self.a_start = history, lam_simple, lam_anderson, anderson_start
+        self.min_simple = int(min_simple)
 
     def _step(self, q, w):
         return O.step_diffusion(lambda x: O.execute_m2_scft(self.plan, x), q, w, self.ds)
@@ -94,7 +96,7 @@ class SCFTOracle:
             if ev["err"] < tol:
                 return w[:n].reshape(shape), w[n:].reshape(shape), ev, it
             d = np.concatenate([ev["dA"].ravel(), ev["dB"].ravel()])
-            if ev["err"] > self.a_start:
+            if ev["err"] > self.a_start or it < self.min_simple:
                 W.clear()
                 D.clear()
                 w = w + self.lam_s * d

@@ -1,0 +1,117 @@
+"""The warm-start network on the device (cfft_sno_*) against its FP64 oracle
+(oracle/sno_oracle.py, full-grid numpy FFTs; BF16 rounding emulated where the device
+rounds: the weights and the inputs of the tensor-core channel products).
+
+- forward: predicted fields [w_A | w_B] on the plan's subgrid, three groups (centred
+  Im-3m and Ia-3d, primitive Pm-3m), relative error <= 2e-4;
+- gradients of every parameter tensor, relative (to the tensor's largest entry)
+  error <= 2e-3;
+- a few Adam steps on fixed targets reduce the loss;
+- weights survive a save / load round trip at BF16 precision.
+"""
+import numpy as np
+import pytest
+
+from conftest import oracle_group
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from oracle import sno_oracle as S  # noqa: E402
+
+PARAMS = [(20.0, 0.4), (14.0, 0.33)]
+
+
+def _case(cf, O, sg, N, nsamp=2):
+    ops = O.get_ops(sg, 3, N)
+    shift, oops = O.find_optimal_shift(ops, N)
+    ops_s = [cf.SymOp(op.R, op.t) for op in oops]
+    spec = cf.calc_spectral_asu(ops_s, 3, N)
+    plan = cf.KRFFTPlan(spec, ops_s, precision=4, max_batch=32 * nsamp)
+    a = np.stack([S.features(sg, N, c, f, ops, shift) for c, f in PARAMS[:nsamp]])
+    return plan, shift, oops, a
+
+
+def _to_sub(x, L):
+    """(S, C, N1, N2, N3) full grid [x, y, z] -> (S, C, M3, M2, M1) memory order."""
+    sub = x[:, :, ::L[0], ::L[1], ::L[2]]
+    return np.ascontiguousarray(sub.transpose(0, 1, 4, 3, 2))
+
+
+def _targets(O, oops, N, nsamp):
+    t = np.stack([np.stack([O.make_symmetric(oops, N, seed=10 * s + c) for c in range(2)]) for s in range(nsamp)])
+    return 0.1 * t
+
+
+@pytest.mark.parametrize("sg", [229, 230, 221])
+def test_sno_forward_matches_oracle(cf, O, sg):
+    N = (16, 16, 16)
+    plan, shift, oops, a = _case(cf, O, sg, N)
+    model = cf.SpectralNeuralOperator()
+    p = S.unflatten(model.get_params().astype(np.float64))
+    ctx = model.bind(plan, sg, shift, 2)
+    w = ctx.predict(PARAMS).cpu().numpy().astype(np.float64)
+    out, _ = S.SNO(p, bf16_mode=True).forward(a)
+    want = np.stack([np.stack(S.w_from_output(out[s], c, f)) for s, (c, f) in enumerate(PARAMS)])
+    want = _to_sub(want, plan.L)
+    dev = w - np.array([[c * (1 - f), c * f] for c, f in PARAMS])[:, :, None, None, None]
+    ref = want - np.array([[c * (1 - f), c * f] for c, f in PARAMS])[:, :, None, None, None]
+    err = np.max(np.abs(dev - ref)) / np.max(np.abs(ref))
+    assert err <= 2e-4, err
+    ctx.close()
+    model.close()
+    plan.close()
+
+
+@pytest.mark.parametrize("sg", [229, 221])
+def test_sno_gradients_match_oracle(cf, O, sg):
+    N = (16, 16, 16)
+    plan, shift, oops, a = _case(cf, O, sg, N)
+    model = cf.SpectralNeuralOperator()
+    p = S.unflatten(model.get_params().astype(np.float64))
+    t = _targets(O, oops, N, 2)
+    w_t = np.stack([np.stack(S.w_from_output(t[s], c, f)) for s, (c, f) in enumerate(PARAMS)])
+    ctx = model.bind(plan, sg, shift, 2)
+    wt_dev = torch.tensor(_to_sub(w_t, plan.L), dtype=torch.float32, device="cuda")
+    loss = ctx.train_step(PARAMS, wt_dev, step=False)
+    g_dev = S.unflatten(model.grads().astype(np.float64))
+    net = S.SNO(p, bf16_mode=True)
+    out, c = net.forward(a)
+    assert abs(loss - net.loss(out, t)) <= 1e-4 * net.loss(out, t)
+    g = net.backward(out, t, c)
+    for k in S.PARAM_ORDER:
+        scale = np.max(np.abs(g[k]))
+        if scale == 0.0:
+            assert np.max(np.abs(g_dev[k])) < 1e-12, k
+            continue
+        err = np.max(np.abs(g_dev[k] - g[k])) / scale
+        assert err <= 2e-3, (k, err)
+    ctx.close()
+    model.close()
+    plan.close()
+
+
+def test_sno_training_reduces_loss_and_save_load(cf, O, tmp_path):
+    N = (16, 16, 16)
+    plan, shift, oops, a = _case(cf, O, 230, N)
+    model = cf.SpectralNeuralOperator(lr=2e-3)
+    ctx = model.bind(plan, 230, shift, 2)
+    t = _targets(O, oops, N, 2)
+    w_t = np.stack([np.stack(S.w_from_output(t[s], c, f)) for s, (c, f) in enumerate(PARAMS)])
+    wt_dev = torch.tensor(_to_sub(w_t, plan.L), dtype=torch.float32, device="cuda")
+    losses = [ctx.train_step(PARAMS, wt_dev) for _ in range(30)]
+    assert losses[-1] < 0.5 * losses[0], losses
+    path = tmp_path / "w.npy"
+    model.save(str(path))
+    before = ctx.predict(PARAMS).cpu().numpy()
+    m2 = cf.SpectralNeuralOperator()
+    m2.load(str(path))
+    ctx2 = m2.bind(plan, 230, shift, 2)
+    after = ctx2.predict(PARAMS).cpu().numpy()
+    # the working copy is BF16 already, so only the FP32 biases move (by BF16 rounding)
+    assert np.max(np.abs(after - before)) <= 2e-2 * np.max(np.abs(before))
+    for o in (ctx, ctx2, model, m2, plan):
+        o.close()
