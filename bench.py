@@ -2,13 +2,15 @@
 FP32 with the centring fold, batched fields resident in HBM.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--batch B] [--impl ours|reference]
-                    [--workload im3m128|scft-ia3d96|pmmm64|ia3d96-step|mixed]
+                    [--workload im3m128|scft-ia3d96|sno-train|pmmm64|ia3d96-step|mixed]
 
 One step = one forward + backward KRFFT over B fields (f0 -> spectral ASU -> f0).
 The default workload is the headline line; --workload selects a secondary single-GPU
-measurement (the SCFT time-to-tolerance of an AB diblock in Ia-3d at 96^3; Pmmm 64^3
-FP64 forward + backward; the Ia-3d 96^3 FP32 diffusion contour step; 64 fields over four
-cubic groups and four grid edges, forward + backward and a 50-step diffusion solve each).
+measurement (the SCFT time-to-tolerance of an AB diblock in Ia-3d at 96^3 from the
+learned warm start and from the plain start; one training step of the warm-start
+network; Pmmm 64^3 FP64 forward + backward; the Ia-3d 96^3 FP32 diffusion contour step;
+64 fields over four cubic groups and four grid edges, forward + backward and a 50-step
+diffusion solve each).
 Prints ONE JSON line on rank 0.  Under torchrun each rank runs its own batch
 (fields are independent: replicas / weak scaling); the step time is the max over
 ranks.  `--impl reference` times the FP64 CPU restatement of the reference's
@@ -48,17 +50,23 @@ def load_package():
     return mod
 
 
+# Sources of the transform path (plan tables, scheduling, kernels); the SCFT driver, the
+# warm-start network, the space-group table and the C ABI wrappers do not change its traffic.
+TRANSFORM_SOURCES = ("cfft_internal.h", "device_common.cuh", "exec.cu", "exec.h", "fast_api.h", "fast_kernels.cuh",
+                     "fast_other_f32.cu", "fast_other_f64.cu", "fast_planes_f32.cu", "fast_planes_f64.cu",
+                     "planner.cpp", "tma_planes.cuh")
+
+
 def kernel_source_sha():
-    """Hash of the native sources; a DRAM-traffic figure measured by ncu applies to the
-    build it was measured on only."""
+    """Hash of the transform path's native sources; a DRAM-traffic figure measured by ncu
+    applies to the build it was measured on only."""
     import hashlib
 
     h = hashlib.sha256()
     csrc = os.path.join(PKG_DIR, "csrc")
-    for name in sorted(os.listdir(csrc)):
-        if name.endswith((".cu", ".cuh", ".h", ".cpp")):
-            h.update(name.encode())
-            h.update(open(os.path.join(csrc, name), "rb").read())
+    for name in TRANSFORM_SOURCES:
+        h.update(name.encode())
+        h.update(open(os.path.join(csrc, name), "rb").read())
     return h.hexdigest()[:16]
 
 
@@ -577,6 +585,53 @@ def run_scft(args):
     print(json.dumps(line), flush=True)
 
 
+def run_sno_train(args):
+    """Training step of the warm-start network (secondary line): Ia-3d 64^3, 16 samples
+    per step (the training configuration), targets = seeded plain-start fields.  One step =
+    forward (4 Fourier layers: 8 batched KRFFTs of 512 fields, tensor-core channel
+    products) + loss + backward + Adam update; device time by CUDA events."""
+    import torch
+
+    cf = load_package()
+    from crystallographicfft_b200 import warmstart as ws
+
+    torch.cuda.set_device(0)
+    S = 16
+    gg = ws.GroupGrid(230, 64)
+    plan = cf.KRFFTPlan(gg.spec, gg.ops, N=gg.N, precision=4, max_batch=32 * S)
+    model = cf.SpectralNeuralOperator()
+    ctx = model.bind(plan, 230, gg.shift, S)
+    prm = ws.draws(S, seed=5)
+    tgt = torch.tensor(np.stack([gg.plain_start(f, c, plan.L) for c, f in prm]), dtype=torch.float32,
+                       device="cuda").contiguous()
+    for _ in range(args.warmup):
+        ctx.train_step(prm, tgt, lr=1e-4)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(0.3)
+    cf.LIB.cfft_launch_count(1)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        ctx.train_step(prm, tgt, lr=1e-4)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = int(cf.LIB.cfft_launch_count(1))
+    clk = clocks.stop()
+    line = {"metric": "warm-start network training step, ms (Ia-3d 64^3, 16 samples, forward + backward + Adam)",
+            "value": ms, "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16 weights / tensor-core operands, f32 accumulate and fields", "data": "synthetic",
+            "config": {"workload": "sno-train", "group": 230, "N": 64, "samples": S, "width": 32, "modes": 12,
+                       "layers": 4, "params": int(cf.sno.N_PARAMS)},
+            "samples_per_s": S / (ms / 1000.0), "gpu_launches": launches, "clocks": clk, "e2e": None, "roofline": None}
+    for o in (ctx, model, plan):
+        o.close()
+    print(json.dumps(line), flush=True)
+
+
 def _field_bytes(plan, rs):
     return 2 * (rs * int(np.prod(plan.M)) + 2 * rs * plan.n_spec)
 
@@ -704,7 +759,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing (profiling runs)")
     ap.add_argument("--tune-cache", default=None, help="autotuner cache file (default ~/.cache/cfft_b200/tuning.json)")
-    ap.add_argument("--workload", default="im3m128", choices=["im3m128", "scft-ia3d96"] + sorted(WORKLOADS),
+    ap.add_argument("--workload", default="im3m128", choices=["im3m128", "scft-ia3d96", "sno-train"] + sorted(WORKLOADS),
                     help="im3m128 is the headline line; the others are secondary single-GPU measurements")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -712,6 +767,8 @@ def main():
         run_reference(args)
     elif args.workload == "scft-ia3d96":
         run_scft(args)
+    elif args.workload == "sno-train":
+        run_sno_train(args)
     elif args.workload != "im3m128":
         run_workload(args)
     else:

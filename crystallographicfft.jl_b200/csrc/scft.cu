@@ -8,7 +8,13 @@
 //   w = w_A on s < f, w_B after; Q = <q(r, 1)>; phi_A = (1/Q) int_0^f q q_dagger ds,
 //   phi_B over [f, 1] (Simpson's rule, trapezoid for an odd block);
 //   d_A = chiN (phi_B - 1/2) + (w_B - w_A)/2, d_B = chiN (phi_A - 1/2) + (w_A - w_B)/2;
-//   err = sqrt(sum d^2 / sum w^2), F = -ln Q + <chiN phi_A phi_B - w_A phi_A - w_B phi_B>;
+//   err = sqrt(sum d^2 / sum w^2);
+//   F = -ln Q + <w_-^2 / chiN - w_+> + chiN / 4 with w_+- = (w_B +- w_A) / 2, the
+//   field-theoretic Hamiltonian: at the saddle point it equals the mean-field free energy
+//   -ln Q + <chiN phi_A phi_B - w_A phi_A - w_B phi_B>, and it is stationary there
+//   (dF/dw_+ = phi_A + phi_B - 1, dF/dw_- = phi_B - phi_A + 2 w_- / chiN), so its error
+//   is second order in the residual and two solves converged to the same tolerance
+//   agree on F far below that tolerance;
 //   simple mixing (w += lam_s d) for the first min_simple iterations and while
 //   err > anderson_start, then Anderson mixing over
 //   the last `history` iterates (U c = V from the Gram matrix of the residuals).
@@ -141,7 +147,8 @@ __global__ void __launch_bounds__(kRedThreads) k_scft_residual(const T* __restri
     d[n + r] = db;
     sd += static_cast<double>(da) * da + static_cast<double>(db) * db;
     sw += static_cast<double>(wa) * wa + static_cast<double>(wb) * wb;
-    sf += chiN * static_cast<double>(pa) * pb - static_cast<double>(wa) * pa - static_cast<double>(wb) * pb;
+    const double wm = 0.5 * (static_cast<double>(wb) - static_cast<double>(wa));
+    sf += wm * wm / chiN - 0.5 * (static_cast<double>(wa) + static_cast<double>(wb));
   }
   double t = block_sum(sd, sh);
   if (threadIdx.x == 0) part[blockIdx.x * 3 + 0] = t;
@@ -349,7 +356,7 @@ void fill_state(const Scft* S, ScftState* out) {
   const double* h = S->h_red;
   out->Q = h[0];
   out->err = std::sqrt(h[1] / std::max(h[2], 1e-300));
-  out->F = -std::log(h[0]) + h[3] / static_cast<double>(S->n);
+  out->F = -std::log(h[0]) + h[3] / static_cast<double>(S->n) + 0.25 * S->prm.chiN;
 }
 
 template <typename T>

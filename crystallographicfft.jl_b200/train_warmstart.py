@@ -52,6 +52,12 @@ def main():
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--threads", type=int, default=8)
     ap.add_argument("--time-test", type=int, default=200, help="held-out draws timed (plain vs learned)")
+    ap.add_argument("--train-seconds", type=float, default=900.0, help="training time limit")
+    ap.add_argument("--max-iter", default="230:1000,229:1000,221:700", help="group:iteration cap of the data solves")
+    ap.add_argument("--weights", default=None, help="evaluate these weights: no training set, no training")
+    ap.add_argument("--plain", default="data", choices=["data", "timed"],
+                    help="schedule of the timed plain start on held-out draws: that of the training data "
+                         "(200 simple-mixing iterations) or the shorter one of the 96^3 gyroid (100)")
     a = ap.parse_args()
 
     import torch
@@ -71,19 +77,20 @@ def main():
         return [(int(g), int(c)) for g, c in (x.split(":") for x in spec.split(","))]
 
     train_spec, test_spec = parse(a.train), parse(a.test)
+    caps = dict(parse(a.max_iter))
     groups = sorted({g for g, _ in train_spec + test_spec}, key=lambda g: [x for x, _ in train_spec].index(g))
     grids = {g: ws.GroupGrid(g, a.grid) for g in groups}
     data = {}
-    for k, (g, cnt) in enumerate(train_spec):
+    for k, (g, cnt) in enumerate(train_spec if a.weights is None else []):
         d = ws.draws(cnt, seed=1000 + k)
-        fld, st, tm = ws.generate(grids[g], d, threads=a.threads, log=log)
+        fld, st, tm = ws.generate(grids[g], d, threads=a.threads, log=log, max_iter=caps.get(g, 1000))
         ok = np.array([s["err"] < 1e-3 for s in st])
         data[g] = dict(params=d[ok], fields=fld[torch.as_tensor(np.nonzero(ok)[0], device="cuda")].contiguous(),
                        F=np.array([s["F"] for s in st])[ok], seconds=float(np.sum(tm)), dropped=int((~ok).sum()))
     tests = {}
     for k, (g, cnt) in enumerate(test_spec):
         d = ws.draws(cnt, seed=2000 + k)
-        fld, st, tm = ws.generate(grids[g], d, threads=a.threads, log=log)
+        fld, st, tm = ws.generate(grids[g], d, threads=a.threads, log=log, max_iter=caps.get(g, 1000))
         tests[g] = dict(params=d, fields=fld, states=st)
     gen_s = time.time() - t_start
     log(f"data generated in {gen_s:.1f} s")
@@ -97,14 +104,18 @@ def main():
         if g in data:
             sets.append((ctxs[g], data[g]["params"], data[g]["fields"]))
     t0 = time.time()
-    hist = ws.train(model, sets, a.epochs, batch=a.batch, lr=a.lr, log=log)
+    if a.weights is None:
+        hist = ws.train(model, sets, a.epochs, batch=a.batch, lr=a.lr, log=log, max_seconds=a.train_seconds)
+        log(f"trained {a.epochs} epochs in {time.time() - t0:.1f} s, final loss {hist[-1]:.3e}")
+        os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
+        model.save(a.out)
+    else:
+        model.load(a.weights)
+        hist = [float("nan")]
     train_s = time.time() - t0
-    log(f"trained {a.epochs} epochs in {train_s:.1f} s, final loss {hist[-1]:.3e}")
-    os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
-    model.save(a.out)
 
     # held-out: field error of the prediction
-    report = dict(grid=a.grid, train={str(g): dict(n=int(len(v["params"])), dropped=v["dropped"],
+    report = dict(grid=a.grid, weights=a.weights or a.out, train={str(g): dict(n=int(len(v["params"])), dropped=v["dropped"],
                                                    solve_seconds=v["seconds"]) for g, v in data.items()},
                   epochs=a.epochs, batch=a.batch, lr=a.lr, loss_history=[float(x) for x in hist[::5]] + [float(hist[-1])],
                   generate_seconds=gen_s, train_seconds=train_s, params=int(cf.sno.N_PARAMS))
@@ -125,11 +136,18 @@ def main():
     for j in order[:a.time_test]:
         h = held[j]
         gg, ctx = grids[h["group"]], ctxs[h["group"]]
-        r_plain = ws.time_to_tol(gg, h["chiN"], h["f"],
-                                 torch.tensor(gg.plain_start(h["f"], h["chiN"], plans[h["group"]].L),
-                                              dtype=torch.float32, device="cuda"), warm=False)
-        r_warm = ws.time_to_tol(gg, h["chiN"], h["f"], None, warm=True,
-                                predict=lambda: ctx.predict([(h["chiN"], h["f"])])[0])
+        which = "plain"
+        try:
+            r_plain = ws.time_to_tol(gg, h["chiN"], h["f"],
+                                     torch.tensor(gg.plain_start(h["f"], h["chiN"], plans[h["group"]].L),
+                                                  dtype=torch.float32, device="cuda"), warm=False,
+                                     plain=ws.PLAIN_DATA if a.plain == "data" else ws.PLAIN)
+            which = "learned"
+            r_warm = ws.time_to_tol(gg, h["chiN"], h["f"], None, warm=True,
+                                    predict=lambda: ctx.predict([(h["chiN"], h["f"])])[0])
+        except cf.CFFTError as e:
+            h.update(error=str(e), failed_start=which)
+            continue
         h.update(plain=r_plain, learned=r_warm, speedup=r_plain["seconds"] / r_warm["seconds"],
                  dF=abs(r_plain["F"] - r_warm["F"]))
         timed += 1
@@ -138,10 +156,14 @@ def main():
         sp = np.array([h["speedup"] for h in tm])
         dF = np.array([h["dF"] for h in tm])
         match = dF <= 1e-7
-        report["held_out"] = dict(n=len(tm), speedup_median=float(np.median(sp)),
+        report["held_out"] = dict(n=len(tm), failed=len([h for h in held if "error" in h]),
+                                  speedup_median=float(np.median(sp)),
                                   speedup_median_matching=float(np.median(sp[match])) if match.any() else None,
                                   speedup_mean_matching=float(np.mean(sp[match])) if match.any() else None,
-                                  matching_F=int(match.sum()),
+                                  matching_F=int(match.sum()), matching_F_1e6=int((dF <= 1e-6).sum()),
+                                  plain_schedule=a.plain,
+                                  failed_plain=len([h for h in held if h.get("failed_start") == "plain"]),
+                                  failed_learned=len([h for h in held if h.get("failed_start") == "learned"]),
                                   plain_seconds_mean=float(np.mean([h["plain"]["seconds"] for h in tm])),
                                   learned_seconds_mean=float(np.mean([h["learned"]["seconds"] for h in tm])),
                                   field_rel_err_median=float(np.median([h["field_rel_err"] for h in held])))

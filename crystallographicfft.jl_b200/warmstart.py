@@ -20,6 +20,7 @@ import time
 import numpy as np
 
 from . import symmetry as sym
+from ._lib import CFFTError
 from .plans import _torch
 from .scft import initial_fields, plan_scft
 from .sno import GROUP_SLOTS, SpectralNeuralOperator
@@ -30,7 +31,7 @@ CELL = 3.8 * np.sqrt(6.0)  # cubic cell edge in units of Rg (3.8 b sqrt(N))
 # disordered state); a prediction starts with Anderson mixing.
 PLAIN = dict(min_simple=100, lam_simple=0.1, anderson_start=0.2)       # timed plain start
 PLAIN_DATA = dict(min_simple=200, lam_simple=0.1, anderson_start=0.2)  # training-data solves
-WARM = dict(min_simple=0, lam_simple=0.1, anderson_start=1e9)          # from a prediction
+WARM = dict(min_simple=0, lam_simple=0.1, anderson_start=0.3)          # from a prediction
 
 
 class GroupGrid:
@@ -86,7 +87,11 @@ def generate(gg, draws, tol=1e-4, schedule=None, max_iter=1000, threads=8, log=N
                     plan, sol = gg.solver(f, chiN, 4, tol, schedule, max_iter=max_iter)
                     w = torch.tensor(gg.plain_start(f, chiN, L), dtype=torch.float32, device="cuda").contiguous()
                     t0 = time.time()
-                    states[i] = sol.solve(w)
+                    try:
+                        states[i] = sol.solve(w)
+                    except CFFTError as e:  # a diverged solve is reported, not fatal
+                        states[i] = dict(Q=float("nan"), F=float("nan"), err=float("inf"), iterations=-1,
+                                         converged=False, error=str(e))
                     times[i] = time.time() - t0
                     out[i].copy_(w)
                     sol.close()
@@ -116,11 +121,12 @@ def draws(n, seed, chiN_range=(12.0, 30.0), f_range=(0.30, 0.50)):
     return np.stack([rng.uniform(*chiN_range, n), rng.uniform(*f_range, n)], axis=1)
 
 
-def train(model, sets, epochs, batch=16, lr=1e-3, lr_final=1e-5, seed=0, log=None):
+def train(model, sets, epochs, batch=16, lr=1e-3, lr_final=1e-5, seed=0, log=None, max_seconds=None):
     """sets: list of (ctx, params (n, 2), fields tensor (n, 2, M...)).  Cosine learning-rate
     decay from lr to lr_final; one mini-batch of one group per step.  Returns the mean
-    loss of each epoch."""
+    loss of each epoch; stops after the epoch that passes max_seconds."""
     torch = _torch()
+    t0 = time.time()
     rng = np.random.default_rng(seed)
     steps_per_epoch = sum((len(p) + batch - 1) // batch for _, p, _ in sets)
     total = epochs * steps_per_epoch
@@ -141,6 +147,10 @@ def train(model, sets, epochs, batch=16, lr=1e-3, lr_final=1e-5, seed=0, log=Non
         hist.append(acc / len(jobs))
         if log and (ep % 10 == 0 or ep == epochs - 1):
             log(f"epoch {ep}: loss {hist[-1]:.3e}")
+        if max_seconds is not None and time.time() - t0 > max_seconds:
+            if log:
+                log(f"stopped after epoch {ep}: {time.time() - t0:.0f} s")
+            break
     return hist
 
 
@@ -151,7 +161,7 @@ def time_to_tol(gg, chiN, f, start, *, warm, tol=1e-6, switch=1e-5, predict=None
     the schedule of the FP32 phase (WARM, else `plain` or PLAIN)."""
     torch = _torch()
     sch = WARM if warm else (plain or PLAIN)
-    p32, s32 = gg.solver(f, chiN, 4, switch, sch)
+    p32, s32 = gg.solver(f, chiN, 4, switch, sch, max_iter=600)  # FP64 finishes what FP32 rounding leaves
     p64, s64 = gg.solver(f, chiN, 8, tol, WARM)
     probe = (predict() if start is None else start).to(torch.float32).contiguous()
     s32.evaluate(probe.clone())  # captures the propagator graphs outside the timed region

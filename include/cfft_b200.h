@@ -275,7 +275,9 @@ cfft_status cfft_wait_selftest(cfft_plan plan, unsigned long long timeout_ns, vo
  * at least 2): propagators q, q_dagger (one two-field batch of the plan's contour
  * step), Q = <q(r, 1)>, densities by Simpson's rule, residuals
  * d_A = chiN (phi_B - 1/2) + (w_B - w_A)/2, d_B = chiN (phi_A - 1/2) + (w_A - w_B)/2,
- * err = sqrt(sum d^2 / sum w^2), F = -ln Q + <chiN phi_A phi_B - w_A phi_A - w_B phi_B>,
+ * err = sqrt(sum d^2 / sum w^2), F = -ln Q + <(w_B - w_A)^2 / (4 chiN) - (w_A + w_B) / 2> + chiN / 4
+ * (the field-theoretic Hamiltonian: equal to -ln Q + <chiN phi_A phi_B - w_A phi_A - w_B phi_B>
+ * at the saddle point and stationary there, so its error is second order in the residual),
  * simple mixing for the first min_simple iterations and above anderson_start, Anderson
  * mixing after.  Q, F, the residual
  * norms, the Anderson Gram matrix and its least-squares solve are FP64 on the device.

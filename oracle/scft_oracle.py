@@ -17,7 +17,10 @@ the library's device driver (cfft_scft_*) can be checked against it:
   xi = (w_A + w_B - chiN) / 2):
   d_A = chiN (phi_B - 1/2) + (w_B - w_A)/2,  d_B = chiN (phi_A - 1/2) + (w_A - w_B)/2;
   error = sqrt(sum(d_A^2 + d_B^2) / sum(w_A^2 + w_B^2)).
-- Free energy per chain: F = -ln Q + <chiN phi_A phi_B - w_A phi_A - w_B phi_B>.
+- Free energy per chain: the field-theoretic Hamiltonian
+  F = -ln Q + <(w_B - w_A)^2 / (4 chiN) - (w_A + w_B) / 2> + chiN / 4, equal at the saddle
+  point to the mean-field -ln Q + <chiN phi_A phi_B - w_A phi_A - w_B phi_B> and stationary
+  there (error second order in the residual); `F_mf` is the mean-field form.
 - Mixing: simple mixing w += lam_s d for the first `min_simple` iterations and while the
   error is above `anderson_start`, then
   Anderson mixing (D. G. Anderson, J. ACM 12, 547 (1965); as used for SCFT by
@@ -81,8 +84,9 @@ class SCFTOracle:
         dA = chiN * (phiB - 0.5) + 0.5 * (wB - wA)
         dB = chiN * (phiA - 0.5) + 0.5 * (wA - wB)
         err = float(np.sqrt((np.sum(dA ** 2) + np.sum(dB ** 2)) / (np.sum(wA ** 2) + np.sum(wB ** 2))))
-        F = -np.log(Q) + float(np.mean(chiN * phiA * phiB - wA * phiA - wB * phiB))
-        return dict(Q=Q, phiA=phiA, phiB=phiB, dA=dA, dB=dB, err=err, F=F)
+        F_mf = -np.log(Q) + float(np.mean(chiN * phiA * phiB - wA * phiA - wB * phiB))
+        F = -np.log(Q) + float(np.mean((wB - wA) ** 2 / (4.0 * chiN) - 0.5 * (wA + wB))) + 0.25 * chiN
+        return dict(Q=Q, phiA=phiA, phiB=phiB, dA=dA, dB=dB, err=err, F=F, F_mf=F_mf)
 
     def solve(self, wA, wB, tol=1e-6, max_iter=2000, callback=None):
         """Iterate from (wA, wB) until error < tol.  Returns (wA, wB, last evaluation, iterations)."""

@@ -49,4 +49,5 @@ def test_oracle_converges_to_microphase(ia3d):
     assert ev["err"] < 1e-8
     assert np.max(np.abs(ev["phiA"] + ev["phiB"] - 1)) < 1e-6   # incompressible at the saddle point
     assert ev["F"] < chiN * f * (1 - f)                          # below the disordered melt
+    assert abs(ev["F"] - ev["F_mf"]) < 1e-7                      # Hamiltonian = mean-field F at the saddle
     assert np.ptp(ev["phiA"]) > 0.5                              # microphase separated
