@@ -110,15 +110,18 @@ class SCFTSolver:
             pass
 
 
-def plan_scft(sg, N, cell, *, f=0.4, chiN=20.0, Ns=100, precision=4, ops=None, **kw):
+def plan_scft(sg, N, cell, *, f=0.4, chiN=20.0, Ns=100, precision=4, ops=None, path=0, tuning=None, **kw):
     """A plan for group `sg` on grid N with cubic cell edge `cell` (lattice = cell * I)
     and ds = 1/Ns, and its SCFTSolver.  `ops` (shifted operations) defaults to the
-    library's table shifted by find_optimal_shift."""
+    library's table shifted by find_optimal_shift; `path` selects the plan's contour
+    step (cfft_path: the spectral-ASU step by default, or the Q-matrix steps) and `tuning`
+    its execution choices (cfft_tuning fields as a dict)."""
     N = tuple(N)
     if ops is None:
         _, ops = sym.find_optimal_shift(sym.get_ops(sg, len(N), N), N)
     spec = sym.calc_spectral_asu(ops, len(N), N)
-    plan = KRFFTPlan(spec, ops, N=N, ds=1.0 / Ns, lattice=np.eye(3) * cell, precision=precision, max_batch=2)
+    plan = KRFFTPlan(spec, ops, N=N, ds=1.0 / Ns, lattice=np.eye(3) * cell, precision=precision, max_batch=2,
+                     path=path, tuning=tuning)
     return plan, SCFTSolver(plan, f, chiN, Ns, **kw)
 
 
