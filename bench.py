@@ -662,7 +662,9 @@ def run_workload(args):
             N = (n,) * 3
             _, ops_s = cf.find_optimal_shift(cf.get_ops(sg, 3, N), N)
             spec = cf.calc_spectral_asu(ops_s, 3, N)
-            # execution choices per (group, edge, batch) from the autotuner (cached)
+            # execution choices per (group, edge, batch) from the autotuner (cached); choosing the
+            # decomposition per plan as well (autotune_path) timed each plan alone and made the
+            # overlapped one-graph step slower (49.2 against 46.0 us per field), so it is not used
             tu, tms = cf.autotune_plan(spec, ops_s, N=N, precision=rs, batch=count, op="mixed", n_steps=50,
                                        ds=0.01, cache_path=args.tune_cache)
             tunings.append({"group": sg, "N": n, "fields": count, "tuning": tu, "tuned_ms": round(tms, 4)})

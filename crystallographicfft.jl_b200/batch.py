@@ -8,7 +8,8 @@ time on the CPU.  They serve batches of fields of uneven space group and grid si
   fused-z slots per CTA, the wide backward gather, the bulk-copy plane kernels, the
   fused cluster kernels) on the device with CUDA events, by coordinate descent from the
   defaults, and caches the winner in a JSON file keyed by device, operations, grid,
-  precision, batch and operation.
+  precision, batch, operation and path; autotune_path also chooses the decomposition
+  (centring fold, plain stride-L, Q-matrix steps).
 * MultiPlanStep runs one callable per plan, each on its own stream forked from and
   joined to the caller's stream.  Its first call runs them directly and then captures
   the whole set into a single CUDA graph (capturing runs nothing); every later call
@@ -89,7 +90,8 @@ def autotune_plan(spec, ops_shifted, *, N=None, precision=4, batch=1, op="fwdbwd
     N = tuple(spec.N if N is None else N)
     cache_path = cache_path or _default_cache()
     key = "|".join([torch.cuda.get_device_name(), _ops_signature(ops_shifted), "x".join(map(str, N)), str(precision),
-                    str(batch), op, str(n_steps), str(path)])
+                    str(batch), op, str(n_steps), str(path),
+                    hashlib.sha1(repr(tuple((k, tuple(v)) for k, v in knobs)).encode()).hexdigest()[:8]])
     cache = {}
     if os.path.exists(cache_path):
         try:
@@ -128,6 +130,34 @@ def autotune_plan(spec, ops_shifted, *, N=None, precision=4, batch=1, op="fwdbwd
     with open(cache_path, "w") as fh:
         json.dump(cache, fh, indent=1, sort_keys=True)
     return dict(cur), best
+
+
+# Decompositions the autotuner chooses between (cfft_path): the centring fold when the
+# lattice is centred (plan_krfft_centered, src/centering_fold.jl:328), the plain stride-L
+# transform (plan_krfft + plan_m2_backward, src/krfft.jl:301,1101), and the Q-matrix
+# contour steps on either (plan_m2_q, plan_m7_scft, src/q_fused_krfft.jl:83,822).  All
+# take the same subgrid fields and give the same spectra and steps.
+PATHS = (0, 1, 3, 4)
+
+
+def autotune_path(spec, ops_shifted, *, paths=PATHS, knobs=KNOBS, **kw):
+    """The decomposition and execution choices that minimise the device time of `op`:
+    every path in `paths` is timed with the default execution choices, then the
+    fastest is tuned by autotune_plan (both cached).  Returns (path, tuning dict, ms);
+    paths that do not apply to this plan (a Q-matrix step outside its sizes) are
+    skipped."""
+    best = None
+    for p in paths:
+        try:
+            _, ms = autotune_plan(spec, ops_shifted, path=p, knobs=(), **kw)
+        except CFFTError:
+            continue
+        if best is None or ms < best[1]:
+            best = (p, ms)
+    if best is None:
+        raise CFFTError(4, "no decomposition runs for this plan")
+    tu, ms = autotune_plan(spec, ops_shifted, path=best[0], knobs=knobs, **kw)
+    return best[0], tu, ms
 
 
 class MultiPlanStep:

@@ -353,43 +353,84 @@ __global__ void k_unpack_g0(const DevGeom* __restrict__ g, const typename Cx<T>:
   if (2 * slot + 1 < nfields) G0[(2L * slot + 1) * mvol + q] = gb;
 }
 
-// Per-block DFT of the legacy block plan (plan_cfft + mul!/ldiv!, src/cfft_plan.jl,
+// Per-block FFT of the legacy block plan (plan_cfft + mul!/ldiv!, src/cfft_plan.jl,
 // src/execution.jl): blocks are concatenated, each column-major (x fastest) with
-// dims[b] = (n1, n2, n3); one pass transforms one axis of every block, one thread per
-// output element, y(k) = sum_j x(j) e^{-+2 pi i j k / n} along the axis (the angle
-// index j k mod n is exact; the twiddle is sincospi of it).  `scale` multiplies the
-// result (1/(n1 n2 n3) in the last inverse pass).
+// dims[b] = (n1, n2, n3).  One pass transforms one axis of every block; a CTA takes one
+// work item (block b, first line l0, cnt lines along the axis), stages the lines in
+// shared memory, builds the n twiddles e^{-2 pi i m / n} once, and runs the mixed-radix
+// Stockham passes (radices 8, 4, 2, 3, 5) of fft_lines; a length with another prime
+// factor is transformed as a DFT from the same twiddle table (index j k mod n exact).
+// y(k) = sum_j x(j) e^{-+2 pi i j k / n}; the inverse's 1/n is k_block_scale.
 template <typename T>
-__global__ void k_block_dft_axis(const int32_t* __restrict__ dims, const long long* __restrict__ off, int n_blocks,
-                                 const typename Cx<T>::type* __restrict__ src, typename Cx<T>::type* __restrict__ dst,
-                                 int axis, T sign, T scale) {
+__global__ void k_block_fft_axis(const int32_t* __restrict__ dims, const long long* __restrict__ off,
+                                 const int4* __restrict__ items, const typename Cx<T>::type* __restrict__ src,
+                                 typename Cx<T>::type* __restrict__ dst, int axis, int inverse) {
   using C = typename Cx<T>::type;
-  const long long total = off[n_blocks];
-  for (long long e = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; e < total;
-       e += static_cast<long long>(gridDim.x) * blockDim.x) {
-    int lo = 0, hi = n_blocks - 1;  // block of element e: off[b] <= e < off[b + 1]
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) / 2;
-      if (off[mid] <= e) lo = mid; else hi = mid - 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int4 it = items[blockIdx.x];
+  const int b = it.x, l0 = it.y, cnt = it.z;
+  const int n0 = dims[3 * b], n1 = dims[3 * b + 1];
+  const int n = dims[3 * b + axis];
+  C* bufa = reinterpret_cast<C*>(smem_raw);
+  C* bufb = bufa + static_cast<size_t>(cnt) * n;
+  C* tw = bufb + static_cast<size_t>(cnt) * n;
+  const int tid = threadIdx.x, nth = blockDim.x;
+  // line l of the block along `axis`: base offset and element stride
+  auto line_base = [&](int l, long long* stride) -> long long {
+    if (axis == 0) { *stride = 1; return off[b] + static_cast<long long>(l) * n0; }
+    if (axis == 1) {
+      *stride = n0;
+      const int c0 = l % n0, c2 = l / n0;
+      return off[b] + c0 + static_cast<long long>(c2) * n0 * n1;
     }
-    const int b = lo;
-    const int n0 = dims[3 * b], n1 = dims[3 * b + 1], n2 = dims[3 * b + 2];
-    const long long l = e - off[b];
-    const int c[3] = {static_cast<int>(l % n0), static_cast<int>((l / n0) % n1), static_cast<int>(l / (static_cast<long long>(n0) * n1))};
-    const int n = axis == 0 ? n0 : axis == 1 ? n1 : n2;
-    const long long stride = axis == 0 ? 1 : axis == 1 ? n0 : static_cast<long long>(n0) * n1;
-    const long long base = off[b] + l - static_cast<long long>(c[axis]) * stride;
-    const int k = c[axis];
-    C acc = mk<C>(static_cast<T>(0), static_cast<T>(0));
-    for (int j = 0; j < n; ++j) {
-      const int m = static_cast<int>((static_cast<long long>(j) * k) % n);
-      T sv, cv;
-      if constexpr (sizeof(T) == 8) sincospi(2.0 * m / n, &sv, &cv);
-      else sincospif(2.0f * m / n, &sv, &cv);
-      const C x = src[base + j * stride];
-      acc = cadd(acc, cmul(x, mk<C>(cv, sign * sv)));
+    *stride = static_cast<long long>(n0) * n1;
+    return off[b] + l;
+  };
+  for (int m = tid; m < n; m += nth) {
+    T sv, cv;
+    if constexpr (sizeof(T) == 8) sincospi(-2.0 * m / n, &sv, &cv);
+    else sincospif(-2.0f * m / n, &sv, &cv);
+    tw[m] = mk<C>(cv, sv);
+  }
+  for (int e = tid; e < cnt * n; e += nth) {
+    const int l = e / n, j = e % n;
+    long long st;
+    const long long base = line_base(l0 + l, &st);
+    bufa[e] = src[base + j * st];
+  }
+  __syncthreads();
+  int radix[24], nf = 0, r = n;
+  while (r > 1 && nf < 24) {
+    int f = 0;
+    if (r % 8 == 0) f = 8; else if (r % 4 == 0) f = 4; else if (r % 2 == 0) f = 2;
+    else if (r % 3 == 0) f = 3; else if (r % 5 == 0) f = 5;
+    if (!f) break;
+    radix[nf++] = f;
+    r /= f;
+  }
+  const C* res;
+  if (r == 1) {
+    res = inverse ? fft_lines<C, true>(bufa, bufb, n, nf, radix, cnt, cnt, 0, n, 1, tw, tid, nth)
+                  : fft_lines<C, false>(bufa, bufb, n, nf, radix, cnt, cnt, 0, n, 1, tw, tid, nth);
+  } else {
+    for (int e = tid; e < cnt * n; e += nth) {
+      const int l = e / n, k = e % n;
+      const C* x = bufa + static_cast<size_t>(l) * n;
+      C acc = mk<C>(static_cast<T>(0), static_cast<T>(0));
+      for (int j = 0; j < n; ++j) {
+        const C w = tw[static_cast<int>((static_cast<long long>(j) * k) % n)];
+        acc = cadd(acc, inverse ? cmulc(x[j], w) : cmul(x[j], w));
+      }
+      bufb[e] = acc;
     }
-    dst[e] = cscale(acc, scale);
+    __syncthreads();
+    res = bufb;
+  }
+  for (int e = tid; e < cnt * n; e += nth) {
+    const int l = e / n, j = e % n;
+    long long st;
+    const long long base = line_base(l0 + l, &st);
+    dst[base + j * st] = res[e];
   }
 }
 
@@ -1436,11 +1477,35 @@ Status block_plan_create(int n_blocks, const int32_t* dims, int precision, Block
   bp->n_blocks = n_blocks;
   bp->total = off[n_blocks];
   bp->precision = precision;
+  // work items per axis: (block, first line, lines) with lines x length <= kBlockLineElems
+  std::vector<int32_t> items;
+  for (int a = 0; a < 3; ++a) {
+    bp->item_off[a] = static_cast<int>(items.size() / 4);
+    for (int b = 0; b < n_blocks; ++b) {
+      const int n = dims[3 * b + a];
+      if (n > kBlockMaxLen) { *err = "block edge above the supported length"; delete bp; return Status::kUnsupported; }
+      const long long vol = static_cast<long long>(dims[3 * b]) * dims[3 * b + 1] * dims[3 * b + 2];
+      const int lines = static_cast<int>(vol / n);
+      const int per = std::max(1, std::min(lines, kBlockLineElems / n));
+      for (int l = 0; l < lines; l += per) {
+        items.push_back(b);
+        items.push_back(l);
+        items.push_back(std::min(per, lines - l));
+        items.push_back(0);
+      }
+    }
+    bp->n_items[a] = static_cast<int>(items.size() / 4) - bp->item_off[a];
+    for (int b = 0; b < n_blocks; ++b) bp->max_len[a] = std::max(bp->max_len[a], dims[3 * b + a]);
+  }
   cudaError_t e = cudaMalloc(&bp->d_dims, sizeof(int32_t) * 3 * n_blocks);
   if (e == cudaSuccess) e = cudaMalloc(&bp->d_off, sizeof(long long) * (n_blocks + 1));
   if (e == cudaSuccess) e = cudaMalloc(&bp->d_work, static_cast<size_t>(bp->total) * 2 * precision);
+  if (e == cudaSuccess) e = cudaMalloc(&bp->d_items, sizeof(int32_t) * items.size());
   if (e == cudaSuccess) e = cudaMemcpy(bp->d_dims, dims, sizeof(int32_t) * 3 * n_blocks, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(bp->d_off, off.data(), sizeof(long long) * (n_blocks + 1), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(bp->d_items, items.data(), sizeof(int32_t) * items.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_block_fft_axis<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBlockSmemMax);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_block_fft_axis<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBlockSmemMax);
   if (e != cudaSuccess) {
     *err = cuda_msg(e, "block plan");
     block_plan_destroy(bp);
@@ -1452,46 +1517,42 @@ Status block_plan_create(int n_blocks, const int32_t* dims, int precision, Block
 
 void block_plan_destroy(BlockPlan* bp) {
   if (!bp) return;
-  for (void* q : {bp->d_dims, bp->d_off, bp->d_work})
+  for (void* q : {bp->d_dims, bp->d_off, bp->d_work, bp->d_items})
     if (q) cudaFree(q);
   delete bp;
 }
 
 // mul! (forward, unnormalised) / ldiv! (inverse, 1/n) over every block: x -> out -> work -> out.
-Status block_execute(BlockPlan* bp, const void* in, void* out, bool inverse, void* stream, std::string* err) {
-  if (!bp || !in || !out) { *err = "null argument"; return Status::kInvalid; }
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const int grid = static_cast<int>(std::min<long long>((bp->total + 255) / 256, 148 * 16));
+template <typename T>
+Status block_execute_t(BlockPlan* bp, const void* in, void* out, bool inverse, cudaStream_t s, std::string* err) {
+  using C = typename Cx<T>::type;
   const int32_t* dims = static_cast<const int32_t*>(bp->d_dims);
   const long long* off = static_cast<const long long*>(bp->d_off);
-  if (bp->precision == 8) {
-    const double sg = inverse ? 1.0 : -1.0;
-    const double2* src[3] = {static_cast<const double2*>(in), static_cast<const double2*>(out), static_cast<const double2*>(bp->d_work)};
-    double2* dst[3] = {static_cast<double2*>(out), static_cast<double2*>(bp->d_work), static_cast<double2*>(out)};
-    for (int a = 0; a < 3; ++a) {
-      // the inverse's 1/n is applied per axis (1/n_axis of each block) through a second pass below
-      k_block_dft_axis<double><<<grid, 256, 0, s>>>(dims, off, bp->n_blocks, src[a], dst[a], a, sg, 1.0);
-      ++g_launches;
-    }
-    if (inverse) {
-      k_block_scale<double><<<grid, 256, 0, s>>>(dims, off, bp->n_blocks, static_cast<double2*>(out));
-      ++g_launches;
-    }
-  } else {
-    const float sg = inverse ? 1.f : -1.f;
-    const float2* src[3] = {static_cast<const float2*>(in), static_cast<const float2*>(out), static_cast<const float2*>(bp->d_work)};
-    float2* dst[3] = {static_cast<float2*>(out), static_cast<float2*>(bp->d_work), static_cast<float2*>(out)};
-    for (int a = 0; a < 3; ++a) {
-      k_block_dft_axis<float><<<grid, 256, 0, s>>>(dims, off, bp->n_blocks, src[a], dst[a], a, sg, 1.f);
-      ++g_launches;
-    }
-    if (inverse) {
-      k_block_scale<float><<<grid, 256, 0, s>>>(dims, off, bp->n_blocks, static_cast<float2*>(out));
-      ++g_launches;
-    }
+  const int4* items = static_cast<const int4*>(bp->d_items);
+  const C* src[3] = {static_cast<const C*>(in), static_cast<const C*>(out), static_cast<const C*>(bp->d_work)};
+  C* dst[3] = {static_cast<C*>(out), static_cast<C*>(bp->d_work), static_cast<C*>(out)};
+  for (int a = 0; a < 3; ++a) {
+    if (bp->n_items[a] == 0) continue;
+    // shared memory: two line buffers of up to max(kBlockLineElems, n) elements and n twiddles
+    const size_t smem = static_cast<size_t>(2 * std::max(kBlockLineElems, bp->max_len[a]) + bp->max_len[a]) * sizeof(C);
+    k_block_fft_axis<T><<<bp->n_items[a], 128, smem, s>>>(dims, off, items + bp->item_off[a], src[a], dst[a], a,
+                                                         inverse ? 1 : 0);
+    ++g_launches;
+  }
+  if (inverse) {
+    const int grid = static_cast<int>(std::min<long long>((bp->total + 255) / 256, 148 * 16));
+    k_block_scale<T><<<grid, 256, 0, s>>>(dims, off, bp->n_blocks, static_cast<C*>(out));
+    ++g_launches;
   }
   CFFT_CUDA(cudaGetLastError(), "block transform launch");
   return Status::kOk;
+}
+
+Status block_execute(BlockPlan* bp, const void* in, void* out, bool inverse, void* stream, std::string* err) {
+  if (!bp || !in || !out) { *err = "null argument"; return Status::kInvalid; }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  return bp->precision == 8 ? block_execute_t<double>(bp, in, out, inverse, s, err)
+                            : block_execute_t<float>(bp, in, out, inverse, s, err);
 }
 
 // Subgrid spectrum G0 = FFT_M(f0) per field (the F000 of execute_staged!, the Y buffer

@@ -117,6 +117,9 @@ Status exec_step_diffusion(Plan* p, void* q, const void* w, double dt, int n_ste
 Status exec_full_to_sub(Plan* p, const void* u, void* f0, int B, void* stream, std::string* err);
 Status exec_sub_to_full(Plan* p, const void* f0, void* u, int B, void* stream, std::string* err);
 // Legacy block plan (plan_cfft): per-block DFTs of the packed real-space ASU.
+constexpr int kBlockLineElems = 1024;  // elements of the lines one CTA of the block transform stages
+constexpr int kBlockMaxLen = 4096;     // longest block edge
+constexpr int kBlockSmemMax = (2 * kBlockMaxLen + kBlockMaxLen) * 16;
 struct BlockPlan {
   int n_blocks = 0;
   long long total = 0;  // elements over all blocks
@@ -124,6 +127,8 @@ struct BlockPlan {
   void* d_dims = nullptr;
   void* d_off = nullptr;
   void* d_work = nullptr;
+  void* d_items = nullptr;  // per axis: int4 (block, first line, lines, 0) work items
+  int item_off[3] = {0, 0, 0}, n_items[3] = {0, 0, 0}, max_len[3] = {0, 0, 0};
 };
 Status block_plan_create(int n_blocks, const int32_t* dims, int precision, BlockPlan** out, std::string* err);
 void block_plan_destroy(BlockPlan* bp);

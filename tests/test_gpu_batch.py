@@ -98,3 +98,27 @@ def test_multiplan_graph_replay(cf, prep):
     assert step.graph is not None and step.kernels_per_run > 0
     for plan, _, _ in outs:
         plan.close()
+
+
+def test_autotune_path_picks_a_working_decomposition(cf, O, prep, tmp_path):
+    # Im-3m 32^3: the centring fold, the plain stride-2 path and the Q-matrix steps all
+    # apply; whichever the tuner keeps must give the default plan's spectra and steps.
+    N = (32, 32, 32)
+    p = prep(229, N, seed=4)
+    path, tu, ms = cf.autotune_path(p["spec"], p["ops_s"], N=N, precision=4, batch=4, op="mixed", n_steps=6,
+                                    ds=0.01, reps=2, cache_path=str(tmp_path / "t.json"),
+                                    knobs=(("lanes", (1, 2)),))
+    assert path in cf.batch.PATHS and ms > 0
+    ref = cf.KRFFTPlan(p["spec"], p["ops_s"], precision=4, max_batch=4, ds=0.01)
+    plan = cf.KRFFTPlan(p["spec"], p["ops_s"], precision=4, max_batch=4, ds=0.01, path=path, tuning=tu)
+    f0 = O.pack_stride(p["u"], plan.L)
+    x = torch.tensor(np.ascontiguousarray(f0.transpose(2, 1, 0)), dtype=torch.float32, device="cuda")
+    x = x[None].repeat(4, 1, 1, 1).contiguous()
+    assert rel_err(plan.forward(x).cpu().numpy(), ref.forward(x).cpu().numpy()) < 1e-5
+    w = 0.1 * x
+    qa, qb = x.clone(), x.clone()
+    ref.step_diffusion(qa, w, 0.01, 6)
+    plan.step_diffusion(qb, w, 0.01, 6)
+    assert rel_err(qb.cpu().numpy(), qa.cpu().numpy()) < 1e-5
+    ref.close()
+    plan.close()

@@ -46,9 +46,9 @@ def _targets(O, oops, N, nsamp):
     return 0.1 * t
 
 
-@pytest.mark.parametrize("sg", [229, 230, 221])
-def test_sno_forward_matches_oracle(cf, O, sg):
-    N = (16, 16, 16)
+@pytest.mark.parametrize("sg,n", [(229, 16), (230, 16), (221, 16), (230, 32), (229, 32)])
+def test_sno_forward_matches_oracle(cf, O, sg, n):
+    N = (n, n, n)
     plan, shift, oops, a = _case(cf, O, sg, N)
     model = cf.SpectralNeuralOperator()
     p = S.unflatten(model.get_params().astype(np.float64))
