@@ -249,34 +249,53 @@ __global__ void __launch_bounds__(128) k_sno_gemm(GemmArgs a) {
     phase ^= 1u;
     tc_fence_after();
 
-    // epilogue: row p = p0 + 32 warp + lane holds its N accumulators
-    float acc[N];
-#pragma unroll
-    for (int c0 = 0; c0 < N; c0 += 32) tc_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + c0, acc + c0);
+    // epilogue: row p = p0 + 32 warp + lane reads its accumulators 32 columns at a time
+    // (at most 32 accumulator registers live) and applies the fused operations
     const int p = p0 + warp * 32 + lane;
     const size_t base = static_cast<size_t>(s) * N * a.P + p;
-    if constexpr (EPI == kEpiGelu || EPI == kEpiLinear) {
+    float o0 = 0.f, o1 = 0.f;
+    if constexpr (EPI == kEpiProjTrain || EPI == kEpiProjInfer) {
+      o0 = __ldg(a.b2);
+      o1 = __ldg(a.b2 + 1);
+    }
 #pragma unroll
-      for (int c = 0; c < N; ++c) {
-        const size_t o = base + static_cast<size_t>(c) * a.P;
-        const float z = acc[c] + __ldg(a.bias + c) + __ldg(a.add + o);
-        if constexpr (EPI == kEpiGelu) {
-          a.out0[o] = z;
-          a.out1[o] = gelu_f(z);
-        } else {
-          a.out1[o] = z;
+    for (int c0 = 0; c0 < N; c0 += 32) {
+      float acc[32];
+      tc_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + c0, acc);
+      if constexpr (EPI == kEpiGelu || EPI == kEpiLinear) {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+          const int c = c0 + i;
+          const size_t o = base + static_cast<size_t>(c) * a.P;
+          const float z = acc[i] + __ldg(a.bias + c) + __ldg(a.add + o);
+          if constexpr (EPI == kEpiGelu) {
+            a.out0[o] = z;
+            a.out1[o] = gelu_f(z);
+          } else {
+            a.out1[o] = z;
+          }
+        }
+      } else if constexpr (EPI == kEpiProjTrain || EPI == kEpiProjInfer) {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+          const int c = c0 + i;
+          const float hp = acc[i] + __ldg(a.bias + c);
+          if constexpr (EPI == kEpiProjTrain) a.out0[base + static_cast<size_t>(c) * a.P] = hp;
+          const float h = gelu_f(hp);
+          o0 = fmaf(__bfloat162float(a.w2[c]), h, o0);
+          o1 = fmaf(__bfloat162float(a.w2[N + c]), h, o1);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+          const size_t o = base + static_cast<size_t>(c0 + i) * a.P;
+          float g = acc[i] + (a.add ? __ldg(a.add + o) : 0.0f);
+          if constexpr (EPI == kEpiBwdGelu) g *= gelu_grad_f(__ldg(a.zprev + o));
+          a.out0[o] = g;
         }
       }
-    } else if constexpr (EPI == kEpiProjTrain || EPI == kEpiProjInfer) {
-      float o0 = __ldg(a.b2), o1 = __ldg(a.b2 + 1);
-#pragma unroll
-      for (int c = 0; c < N; ++c) {
-        const float hp = acc[c] + __ldg(a.bias + c);
-        if constexpr (EPI == kEpiProjTrain) a.out0[base + static_cast<size_t>(c) * a.P] = hp;
-        const float h = gelu_f(hp);
-        o0 = fmaf(__bfloat162float(a.w2[c]), h, o0);
-        o1 = fmaf(__bfloat162float(a.w2[N + c]), h, o1);
-      }
+    }
+    if constexpr (EPI == kEpiProjTrain || EPI == kEpiProjInfer) {
       const size_t ob = static_cast<size_t>(s) * 2 * a.P + p;
       if constexpr (EPI == kEpiProjTrain) {
         a.out1[ob] = o0;
@@ -285,14 +304,6 @@ __global__ void __launch_bounds__(128) k_sno_gemm(GemmArgs a) {
         const float chiN = a.prm.chiN[s], f = a.prm.f[s];
         a.out1[ob] = chiN * (1.0f - f) + chiN * o0;
         a.out1[ob + a.P] = chiN * f + chiN * o1;
-      }
-    } else {
-#pragma unroll
-      for (int c = 0; c < N; ++c) {
-        const size_t o = base + static_cast<size_t>(c) * a.P;
-        float g = acc[c] + (a.add ? __ldg(a.add + o) : 0.0f);
-        if constexpr (EPI == kEpiBwdGelu) g *= gelu_grad_f(__ldg(a.zprev + o));
-        a.out0[o] = g;
       }
     }
     tc_fence_before();
