@@ -1029,6 +1029,7 @@ Status check_status_word(SnoCtx* c, cudaStream_t st, std::string* err) {
   SNO_CUDA(cudaMemcpyAsync(&h, c->status, sizeof(int), cudaMemcpyDeviceToHost, st), "SNO status read");
   SNO_CUDA(cudaStreamSynchronize(st), "SNO synchronise");
   if (h != 0) {
+    cudaMemsetAsync(c->status, 0, sizeof(int), st);  // reported once; the next call starts clean
     *err = "a tensor-core completion wait of the SNO ran out of time";
     return Status::kTimeout;
   }
