@@ -11,6 +11,7 @@ and reach the same free energy (|dF| <= 1e-7).
 """
 import os
 
+import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
@@ -59,3 +60,36 @@ def test_held_out_draws_64(cf, sg, chiN, f):
     assert a["converged"] and b["converged"]
     assert abs(a["F"] - b["F"]) <= 1e-7, (a["F"], b["F"])
     assert learned_s <= 0.5 * plain_s, (plain_s, learned_s, a, b)
+
+
+def test_prediction_is_grid_independent(cf):
+    # The network's inputs are functions of physical position and its spectral weights are
+    # indexed by Miller index, so its predictions on 64^3 (the training grid) and 96^3 are
+    # samples of one field: their low-order Fourier coefficients, with each grid's origin
+    # shift removed, agree (to the discretisation of the pointwise nonlinearity).
+    from crystallographicfft_b200 import warmstart as ws
+
+    coeffs = []
+    for n in (64, 96):
+        gg = ws.GroupGrid(230, n)
+        plan = cf.KRFFTPlan(gg.spec, gg.ops, N=gg.N, precision=4, max_batch=32)
+        model = cf.SpectralNeuralOperator()
+        model.load(WEIGHTS)
+        ctx = model.bind(plan, 230, gg.shift, 1)
+        w = ctx.predict([(20.0, 0.4)])[0]
+        F = plan.forward(w.contiguous()).cpu().numpy()  # (2, n_spec): w_A, w_B
+        idx = np.asarray(gg.spec.idx)
+        hc = np.where(idx >= n - n // 2, idx - n, idx)
+        low = {}
+        for i, h in enumerate(hc):
+            if np.dot(h, h) <= 12:
+                phase = np.exp(-2j * np.pi * np.dot(h, np.asarray(gg.shift)))
+                low[tuple(int(v) for v in h)] = F[0, i] * phase / n ** 3
+        coeffs.append(low)
+        for o in (ctx, model, plan):
+            o.close()
+    common = sorted(set(coeffs[0]) & set(coeffs[1]))
+    assert len(common) >= 3
+    a = np.array([coeffs[0][h] for h in common])
+    b = np.array([coeffs[1][h] for h in common])
+    assert np.max(np.abs(a - b)) <= 2e-2 * np.max(np.abs(a)), (common, a, b)
