@@ -7,8 +7,9 @@ FP32 with the centring fold, batched fields resident in HBM.
 One step = one forward + backward KRFFT over B fields (f0 -> spectral ASU -> f0).
 The default workload is the headline line; after its timed region it also measures the
 metric's second half, the SCFT time-to-tolerance of the Ia-3d 96^3 gyroid from the
-learned warm start and from the plain start, attached as `scft_ia3d96` (--no-scft skips
-it); --workload selects a secondary single-GPU
+learned warm start and from the plain start, attached as `scft_ia3d96`, and the
+secondary workloads below, attached as `secondary` (--no-attach, alias --no-scft, skips
+both); --workload selects a secondary single-GPU
 measurement (the SCFT time-to-tolerance of an AB diblock in Ia-3d at 96^3 from the
 learned warm start and from the plain start; one training step of the warm-start
 network; Pmmm 64^3 FP64 forward + backward; the Ia-3d 96^3 FP32 diffusion contour step;
@@ -473,7 +474,7 @@ def run_ours(args):
             line["cpu_baseline"] = {"error": repr(exc)}
     # The metric's second half (SCFT time-to-tolerance, learned start vs plain start),
     # measured after the headline's timed region: two timed pairs of solves.
-    if rank == 0 and world == 1 and not args.no_scft:
+    if rank == 0 and world == 1 and not args.no_attach:
         try:
             line["scft_ia3d96"] = dict(metric=SCFT_WORKLOAD, unit="s", config=scft_config(),
                                        **scft_summary(scft_learned_vs_plain(2, 1)))
@@ -494,11 +495,39 @@ def run_ours(args):
         except (OSError, ValueError):
             pass
     plan.close()
+    if rank == 0 and world == 1 and not args.no_attach:
+        line["secondary"] = secondary_lines(args)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+SECONDARY = ("pmmm64", "ia3d96-step", "mixed")
+
+
+def secondary_lines(args):
+    """The secondary workloads, each measured as `--workload NAME` measures it (its own
+    CUDA events, with this run's steps and warm-up), summarised for the headline line.
+    The mixed batch's autotuner starts from an empty cache unless --tune-cache names one."""
+    import tempfile
+
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        cache = args.tune_cache or os.path.join(tmp, "tuning.json")
+        for name in SECONDARY:
+            try:
+                t0 = time.perf_counter()
+                ln = measure_workload(name, args.steps, args.warmup, cache)
+                out[name] = {"metric": ln["metric"], "value": ln["value"], "unit": ln["unit"],
+                             "ms_per_step": ln["ms_per_step"], "dtype": ln["dtype"], "fields": ln["config"]["fields"],
+                             "roofline_frac": ln["roofline"]["frac"], "gpu_launches": ln["gpu_launches"],
+                             "sm_mhz": ln["clocks"].get("sm_mhz"), "clock_reasons": ln["clocks"].get("reasons"),
+                             "wall_s": round(time.perf_counter() - t0, 1)}
+            except Exception as exc:  # reported, never required by the headline
+                out[name] = {"error": repr(exc)}
+    return out
 
 
 # ----------------------------------------------------------------------------- other workloads
@@ -672,10 +701,16 @@ def _field_bytes(plan, rs):
 
 def run_workload(args):
     """Secondary measurements (one GPU): the same device-event timing as the main arm."""
+    print(json.dumps(measure_workload(args.workload, args.steps, args.warmup, args.tune_cache)), flush=True)
+
+
+def measure_workload(name, steps, warmup, tune_cache=None):
+    """One secondary workload (WORKLOADS[name]) timed by CUDA events over `steps` steps
+    after `warmup` untimed ones; returns its JSON line."""
     import torch
 
     cf = load_package()
-    W = WORKLOADS[args.workload]
+    W = WORKLOADS[name]
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(0)
     rs = W["precision"]
@@ -700,7 +735,7 @@ def run_workload(args):
             # decomposition per plan as well (autotune_path) timed each plan alone and made the
             # overlapped one-graph step slower (49.2 against 46.0 us per field), so it is not used
             tu, tms = cf.autotune_plan(spec, ops_s, N=N, precision=rs, batch=count, op="mixed", n_steps=50,
-                                       ds=0.01, cache_path=args.tune_cache)
+                                       ds=0.01, cache_path=tune_cache)
             tunings.append({"group": sg, "N": n, "fields": count, "tuning": tu, "tuned_ms": round(tms, 4)})
             plan = cf.KRFFTPlan(spec, ops_s, precision=rs, max_batch=count, ds=0.01, tuning=tu)
             q = symmetric_fields(cf, torch, ops_s, N, plan.L, count, seed=sg * 1000 + n, device=dev).to(rdt).contiguous()
@@ -744,7 +779,7 @@ def run_workload(args):
             for r in runs:
                 r()
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
     clocks = ClockSampler(0)
@@ -753,14 +788,14 @@ def run_workload(args):
     cf.LIB.cfft_launch_count(1)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    for _ in range(args.steps):
+    for _ in range(steps):
         step()
     e1.record()
     torch.cuda.synchronize()
     launches = int(cf.LIB.cfft_launch_count(1))
     if W["op"] == "mixed":
-        launches = int(step.kernels_per_run) * args.steps  # replayed graph: the kernels it holds
-    ms_step = e0.elapsed_time(e1) / args.steps
+        launches = int(step.kernels_per_run) * steps  # replayed graph: the kernels it holds
+    ms_step = e0.elapsed_time(e1) / steps
     clk = clocks.stop()
     peaks = {}
     try:
@@ -771,9 +806,9 @@ def run_workload(args):
     alg = sum(j[5] for j in jobs)
     achieved = alg / (ms_step * 1e-3) / 1e9
     line = {"metric": f"{W['desc']}: us per field", "value": ms_step * 1000.0 / fields, "unit": UNIT, "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False,
+            "steps": steps, "warmup": warmup, "ms_per_step": ms_step, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if rs == 4 else "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "description": W["desc"], "fields": fields,
+            "config": {"workload": name, "description": W["desc"], "fields": fields,
                        "plans": [{"N": list(j[0].N), "centering": j[0].centering, "centered": j[0].centered,
                                   "fields": j[4]} for j in jobs]},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
@@ -782,7 +817,11 @@ def run_workload(args):
     if W["op"] == "mixed":
         line["config"]["tuning"] = tunings
         line["config"]["launch"] = "one CUDA graph per step (MultiPlanStep) over one stream per plan"
-    print(json.dumps(line), flush=True)
+        step.graph = None  # the graph goes before the plans whose buffers it replays
+    torch.cuda.synchronize()
+    for j in jobs:
+        j[0].close()
+    return line
 
 
 def main():
@@ -794,8 +833,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end timing (profiling runs)")
-    ap.add_argument("--no-scft", action="store_true",
-                    help="skip the SCFT learned-vs-plain comparison attached to the headline line")
+    ap.add_argument("--no-attach", "--no-scft", dest="no_attach", action="store_true",
+                    help="skip what the headline line carries after its timed region: the SCFT learned-vs-plain "
+                         "comparison and the secondary workload lines (profiling runs)")
     ap.add_argument("--tune-cache", default=None, help="autotuner cache file (default ~/.cache/cfft_b200/tuning.json)")
     ap.add_argument("--workload", default="im3m128", choices=["im3m128", "scft-ia3d96", "sno-train"] + sorted(WORKLOADS),
                     help="im3m128 is the headline line; the others are secondary single-GPU measurements")
