@@ -9,8 +9,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
+#include <map>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include <cooperative_groups.h>
@@ -1523,19 +1525,30 @@ constexpr bool bwd_tma_fits() {
   else return tma_groups<BwdTmaShape<T, H, CT>>() >= 2;
 }
 // Persistent grid of a bulk-copy plane kernel: every SM's resident CTAs, or fewer when
-// the tasks run out (occupancy looked up once per kernel instantiation).
+// the tasks run out.  The resident count is looked up once per kernel and device (the
+// kernels of different H share a function type, so the cache is keyed by address) under
+// a lock, since plans may be executed from several host threads.
 template <typename K>
 int tma_grid(K kernel, int threads, size_t smem, int ntasks, int ng) {
-  static int per_sm = -1, sms = 0;
-  if (per_sm < 0) {
-    int dev = 0, occ = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem) != cudaSuccess) occ = 1;
-    per_sm = occ < 1 ? 1 : occ;
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, int> resident;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int cap = 1;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
+    auto it = resident.find(key);
+    if (it == resident.end()) {
+      int occ = 0, sms = 0;
+      if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 1;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, threads, smem) != cudaSuccess) occ = 1;
+      it = resident.emplace(key, std::max(1, occ) * std::max(1, sms)).first;
+    }
+    cap = it->second;
   }
   const int need = (ntasks + ng - 1) / ng;
-  return std::max(1, std::min(need, per_sm * sms));
+  return std::max(1, std::min(need, cap));
 }
 
 // Workspace slots per CTA of the fused z FFT + gather: 4, or 2 with CFFT_ZR_SLOTS=2
