@@ -43,6 +43,44 @@ bool check_shift_invariance(const std::vector<SymOp>& ops, const double* shift, 
   return true;
 }
 
+// True when the affine operations x -> R x + t (mod n, first dim axes) contain the
+// identity and are closed under composition.  The orbit of x is then exactly
+// {R x + t}, and one pass of the operations over x replaces the closure walk that
+// applies every operation to every orbit member.  Matrices are compared entry by
+// entry and translations mod n, so a list that is closed only as maps on the grid
+// counts as open and keeps the walk (same result, more work).
+static bool affine_ops_form_group(const std::vector<SymOp>& ops, const int* n, int dim) {
+  auto same = [&](const int (&R)[3][3], const long* t, const SymOp& o) {
+    for (int i = 0; i < dim; ++i) {
+      if (floor_mod(t[i] - o.t[i], n[i]) != 0) return false;
+      for (int j = 0; j < dim; ++j)
+        if (R[i][j] != o.R[i][j]) return false;
+    }
+    return true;
+  };
+  int I[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  const long zero[3] = {0, 0, 0};
+  bool has_id = false;
+  for (const auto& o : ops) has_id = has_id || same(I, zero, o);
+  if (!has_id) return false;
+  for (const auto& a : ops)
+    for (const auto& b : ops) {
+      int R[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      long t[3] = {0, 0, 0};
+      for (int i = 0; i < dim; ++i) {
+        t[i] = a.t[i];
+        for (int k = 0; k < dim; ++k) t[i] += static_cast<long>(a.R[i][k]) * b.t[k];
+        for (int j = 0; j < dim; ++j)
+          for (int k = 0; k < dim; ++k) R[i][j] += a.R[i][k] * b.R[k][j];
+      }
+      bool found = false;
+      for (const auto& c : ops)
+        if (same(R, t, c)) { found = true; break; }
+      if (!found) return false;
+    }
+  return true;
+}
+
 // _count_special_positions_fast (src/asu.jl:372-438): number of orbits shorter than |ops|.
 int count_special_positions_fast(const int* N, int dim, const std::vector<SymOp>& ops) {
   const int n1 = N[0], n2 = dim > 1 ? N[1] : 1, n3 = dim > 2 ? N[2] : 1;
@@ -51,11 +89,30 @@ int count_special_positions_fast(const int* N, int dim, const std::vector<SymOp>
   std::vector<long> orbit;
   int sp = 0;
   const int n[3] = {n1, n2, n3};
+  const bool closed = affine_ops_form_group(ops, n, dim);
   for (long lin = 0; lin < total; ++lin) {
     if (visited[lin]) continue;
     orbit.clear();
     orbit.push_back(lin);
     visited[lin] = 1;
+    if (closed) {  // the orbit is {g x}: one pass of the operations
+      long rem = lin;
+      int x[3];
+      x[0] = rem % n1; rem /= n1; x[1] = rem % n2; x[2] = rem / n2;
+      long size = 1;
+      for (const auto& op : ops) {
+        long li = 0, stride = 1;
+        for (int d = 0; d < 3; ++d) {
+          long s = (d < dim) ? op.t[d] : 0;
+          for (int j = 0; j < 3; ++j) s += op.R[d][j] * x[j];
+          li += floor_mod(s, n[d]) * stride;
+          stride *= n[d];
+        }
+        if (!visited[li]) { visited[li] = 1; ++size; }
+      }
+      if (size < static_cast<long>(ops.size())) ++sp;
+      continue;
+    }
     for (size_t w = 0; w < orbit.size(); ++w) {
       long rem = orbit[w];
       int x[3];
@@ -168,13 +225,65 @@ std::vector<SymOp> dual_ops(const std::vector<SymOp>& ops) {
   return out;
 }
 
+// The distinct rotation parts of a list of operations (centring copies share one R).
+static std::vector<SymOp> distinct_rotations(const std::vector<SymOp>& ops) {
+  std::vector<SymOp> out;
+  for (const auto& op : ops) {
+    bool dup = false;
+    for (const auto& o : out) {
+      bool same = true;
+      for (int i = 0; i < 3 && same; ++i)
+        for (int j = 0; j < 3 && same; ++j) same = o.R[i][j] == op.R[i][j];
+      if (same) { dup = true; break; }
+    }
+    if (!dup) out.push_back(op);
+  }
+  return out;
+}
+
+// True when the rotations contain the identity and are closed under multiplication
+// (a point group).  Then the orbit of k is exactly {R k}, with no closure walk.
+static bool rotations_form_group(const std::vector<SymOp>& rots) {
+  bool has_id = false;
+  for (const auto& r : rots) has_id = has_id || is_identity_R(r);
+  if (!has_id) return false;
+  for (const auto& a : rots)
+    for (const auto& b : rots) {
+      int p[3][3];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          p[i][j] = 0;
+          for (int k = 0; k < 3; ++k) p[i][j] += a.R[i][k] * b.R[k][j];
+        }
+      bool found = false;
+      for (const auto& c : rots) {
+        bool same = true;
+        for (int i = 0; i < 3 && same; ++i)
+          for (int j = 0; j < 3 && same; ++j) same = c.R[i][j] == p[i][j];
+        if (same) { found = true; break; }
+      }
+      if (!found) return false;
+    }
+  return true;
+}
+
 // calc_spectral_asu (src/spectral_indexing.jl:22-176): orbit representatives of the
 // dual point group (smallest column-major index), with the stabiliser-phase
 // extinction filter, sorted lexicographically by (h1, h2, h3).
+//
+// The reference grows each orbit by a closure walk that applies every operation to
+// every member, O(N^3 |G|).  When the distinct dual rotations form a group (always,
+// for a space group's operations) the walk is replaced by one pass of the distinct
+// rotations over the first unvisited index: scanning in increasing order, that index
+// is the smallest member of its orbit (a smaller member would have marked the whole
+// orbit already), and the orbit is {R k}.  The result is identical and the cost is
+// about N^3.  Operation lists that are not closed keep the closure walk.
 std::vector<SpecPoint> calc_spectral_asu(const std::vector<SymOp>& ops, const int* N, int dim) {
   const int n[3] = {N[0], dim > 1 ? N[1] : 1, dim > 2 ? N[2] : 1};
   const long total = static_cast<long>(n[0]) * n[1] * n[2];
   const std::vector<SymOp> rec = dual_ops(ops);
+  const std::vector<SymOp> rots = distinct_rotations(rec);
+  const bool closed = rotations_form_group(rots);
   std::vector<char> visited(total, 0);
   std::vector<SpecPoint> pts;
   std::vector<long> work;
@@ -183,13 +292,11 @@ std::vector<SpecPoint> calc_spectral_asu(const std::vector<SymOp>& ops, const in
     visited[lin] = 1;
     int orbit = 1;
     long min_lin = lin;
-    work.clear();
-    work.push_back(lin);
-    for (size_t w = 0; w < work.size(); ++w) {
-      long r2 = work[w];
+    if (closed) {
       int kk[3];
-      kk[0] = r2 % n[0]; r2 /= n[0]; kk[1] = r2 % n[1]; kk[2] = r2 / n[1];
-      for (const auto& op : rec) {
+      long r2 = lin;
+      kk[0] = static_cast<int>(r2 % n[0]); r2 /= n[0]; kk[1] = static_cast<int>(r2 % n[1]); kk[2] = static_cast<int>(r2 / n[1]);
+      for (const auto& op : rots) {
         long li = 0, stride = 1;
         for (int d = 0; d < 3; ++d) {
           long s = 0;
@@ -200,8 +307,29 @@ std::vector<SpecPoint> calc_spectral_asu(const std::vector<SymOp>& ops, const in
         if (!visited[li]) {
           visited[li] = 1;
           ++orbit;
-          work.push_back(li);
-          if (li < min_lin) min_lin = li;
+        }
+      }
+    } else {
+      work.clear();
+      work.push_back(lin);
+      for (size_t w = 0; w < work.size(); ++w) {
+        long r2 = work[w];
+        int kk[3];
+        kk[0] = r2 % n[0]; r2 /= n[0]; kk[1] = r2 % n[1]; kk[2] = r2 / n[1];
+        for (const auto& op : rec) {
+          long li = 0, stride = 1;
+          for (int d = 0; d < 3; ++d) {
+            long s = 0;
+            for (int j = 0; j < 3; ++j) s += op.R[d][j] * kk[j];
+            li += floor_mod(s, n[d]) * stride;
+            stride *= n[d];
+          }
+          if (!visited[li]) {
+            visited[li] = 1;
+            ++orbit;
+            work.push_back(li);
+            if (li < min_lin) min_lin = li;
+          }
         }
       }
     }
@@ -709,11 +837,22 @@ std::vector<AsuPoint> calc_asu(const std::vector<SymOp>& ops_in, const int* N_in
       const long total = static_cast<long>(st.n[0]) * st.n[1] * st.n[2];
       std::vector<char> seen(total, 0);
       std::vector<long> orbit;
+      const bool closed = affine_ops_form_group(st.ops, st.n, dim);
       for (long lin = 0; lin < total; ++lin) {
         if (seen[lin]) continue;
         orbit.assign(1, lin);
         seen[lin] = 1;
-        for (size_t w = 0; w < orbit.size(); ++w) {
+        if (closed) {  // the orbit is {g x}: one pass of the operations
+          const int x[3] = {static_cast<int>(lin % st.n[0]), static_cast<int>((lin / st.n[0]) % st.n[1]),
+                            static_cast<int>(lin / (static_cast<long>(st.n[0]) * st.n[1]))};
+          for (const auto& op : st.ops) {
+            int y[3] = {0, 0, 0};
+            apply(op, x, st.n, y);
+            const long li = y[0] + static_cast<long>(st.n[0]) * (y[1] + static_cast<long>(st.n[1]) * y[2]);
+            if (!seen[li]) { seen[li] = 1; orbit.push_back(li); }
+          }
+        }
+        for (size_t w = closed ? orbit.size() : 0; w < orbit.size(); ++w) {
           long r = orbit[w];
           int x[3] = {static_cast<int>(r % st.n[0]), static_cast<int>((r / st.n[0]) % st.n[1]),
                       static_cast<int>(r / (static_cast<long>(st.n[0]) * st.n[1]))};

@@ -66,3 +66,33 @@ def test_pack_asu_interleaved_gamma0(cf, O):
     assert np.array_equal(b.data, u[::2, ::2, ::2]) and b.orbit is None
     c = cf.pack_asu_interleaved(u, N, ops_s, L=(2, 2, 2), asu_only=False)
     assert sum(len(b.orbit.members) for b in c.dim_blocks[3]) == 8
+
+
+def test_calc_asu_and_special_positions_all_groups(cf, O):
+    # calc_asu (src/asu.jl:216-324) and _count_special_positions_fast (src/asu.jl:372-438)
+    # for every space group and plane group on the oracle's shifted operations, and at
+    # the unshifted ones (special positions on the grid): bit-exact against the oracle.
+    # The library walks each orbit once when the operations are closed on the grid.
+    # 8^3 for every group whose translations are in quarters and halves, 6^3 for the
+    # trigonal and hexagonal ones (thirds and sixths)
+    for dim, groups in ((3, range(1, 231)), (2, range(1, 18))):
+        for sg in groups:
+            n = 6 if (dim == 3 and 143 <= sg <= 194) or (dim == 2 and sg >= 13) else 8
+            N = (n,) * dim
+            oops = O.get_ops(sg, dim, N)
+            _, oops_s = O.find_optimal_shift(oops, N)
+            for ops in (oops, oops_s):
+                lib_ops = [cf.SymOp(op.R, op.t) for op in ops]
+                assert cf.count_special_positions(N, lib_ops) == O.count_special_positions_fast(N, ops), (dim, sg)
+            pts = cf.calc_asu(N, [cf.SymOp(op.R, op.t) for op in oops_s])
+            want = O.calc_asu_points(N, oops_s)
+            assert [(tuple(p.idx), tuple(p.depth), p.multiplicity) for p in pts] == want, (dim, sg)
+
+
+def test_calc_asu_large_grid(cf, O):
+    # Im-3m 24^3: the orbits' sizes add up to the grid and match the oracle
+    N = (24, 24, 24)
+    oops_s = O.find_optimal_shift(O.get_ops(229, 3, N), N)[1]
+    pts = cf.calc_asu(N, [cf.SymOp(op.R, op.t) for op in oops_s])
+    assert sum(p.multiplicity for p in pts) == 24 ** 3
+    assert [(tuple(p.idx), tuple(p.depth), p.multiplicity) for p in pts] == O.calc_asu_points(N, oops_s)

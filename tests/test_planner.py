@@ -201,3 +201,44 @@ def test_all_17_plane_groups(cf):
         ops = cf.get_ops(sg, 2, (12, 12))
         assert len({op.R for op in ops}) == order, sg
         assert len(ops) == order * (2 if sg in (5, 9) else 1), sg
+
+
+def test_spectral_asu_all_groups_vs_oracle(cf, O):
+    # calc_spectral_asu (src/spectral_indexing.jl:22-176) for every space group and
+    # plane group on the oracle's own operations: representatives and multiplicities
+    # bit-exact.  The library walks each orbit once with the group's distinct rotations.
+    for dim, groups, N in ((3, range(1, 231), (24, 24, 24)), (2, range(1, 18), (24, 24))):
+        for sg in groups:
+            oops = O.get_ops(sg, dim, N)
+            _, oops_s = O.find_optimal_shift(oops, N)
+            spec = cf.calc_spectral_asu([cf.SymOp(op.R, op.t) for op in oops_s], dim, N)
+            ospec = O.calc_spectral_asu(oops_s, dim, N)
+            assert np.array_equal(spec.idx, ospec.idx), (dim, sg)
+            assert np.array_equal(spec.mult, ospec.mult), (dim, sg)
+
+
+def test_spectral_asu_large_grids_vs_oracle(cf, O):
+    # the sizes of the bench and SCFT workloads: Im-3m 128^3, Ia-3d 96^3, Fd-3m 64^3
+    for sg, n in ((229, 128), (230, 96), (227, 64)):
+        N = (n, n, n)
+        oops = O.get_ops(sg, 3, N)
+        _, oops_s = O.find_optimal_shift(oops, N)
+        spec = cf.calc_spectral_asu([cf.SymOp(op.R, op.t) for op in oops_s], 3, N)
+        ospec = O.calc_spectral_asu(oops_s, 3, N)
+        assert np.array_equal(spec.idx, ospec.idx) and np.array_equal(spec.mult, ospec.mult), sg
+
+
+def test_spectral_asu_open_operation_list(cf):
+    # An operation list that is not closed ({I, 4-fold about z} without its powers) keeps
+    # the reference's closure walk, so its orbits are those of the cyclic group it
+    # generates; with t = 0 no point is extinct either way.
+    I = ((1, 0, 0), (0, 1, 0), (0, 0, 1))
+    R4 = ((0, -1, 0), (1, 0, 0), (0, 0, 1))
+    R2 = ((-1, 0, 0), (0, -1, 0), (0, 0, 1))
+    R4i = ((0, 1, 0), (-1, 0, 0), (0, 0, 1))
+    N = (12, 12, 6)
+    t0 = (0, 0, 0)
+    open_list = cf.calc_spectral_asu([cf.SymOp(I, t0), cf.SymOp(R4, t0)], 3, N)
+    group = cf.calc_spectral_asu([cf.SymOp(R, t0) for R in (I, R4, R2, R4i)], 3, N)
+    assert np.array_equal(open_list.idx, group.idx) and np.array_equal(open_list.mult, group.mult)
+    assert int(np.sum(group.mult)) == 12 * 12 * 6
