@@ -4,11 +4,13 @@
 // integer table (spectral-ASU points, multiplicities, L, M, fold offsets) is
 // identical to the reference's.
 #include <algorithm>
+#include <atomic>
 #include <climits>
 #include <cmath>
 #include <complex>
 #include <numeric>
 #include <set>
+#include <thread>
 
 #include "cfft_internal.h"
 
@@ -721,7 +723,11 @@ Status build_q_tables(const PlanTables& T, const double* lattice, double ds, std
   if (T.L[0] * T.L[1] * T.L[2] != d) { *err = "parity classes do not match the representatives"; return Status::kInvalid; }
   Q->assign(static_cast<size_t>(d) * Mvol * 2, 0.0);
   gather->assign(static_cast<size_t>(d) * Mvol, 0);
-  for (long q = 0; q < Mvol; ++q) {
+  // Fibers are independent: contiguous ranges of q go to host threads, each fiber's
+  // entries are computed exactly as in a serial pass.
+  std::atomic<bool> singular{false};
+  auto fibers = [&](long q0, long q1) {
+  for (long q = q0; q < q1 && !singular.load(std::memory_order_relaxed); ++q) {
     const long qv[3] = {q % T.M[0], (q / T.M[0]) % T.M[1], q / (static_cast<long>(T.M[0]) * T.M[1])};
     cd Bm[8][8];
     double Kv[8];
@@ -757,7 +763,7 @@ Status build_q_tables(const PlanTables& T, const double* lattice, double ds, std
       int piv = c;
       for (int i = c + 1; i < d; ++i)
         if (std::abs(Mx[i][c]) > std::abs(Mx[piv][c])) piv = i;
-      if (std::abs(Mx[piv][c]) < 1e-12) { *err = "singular alias matrix B"; return Status::kInvalid; }
+      if (std::abs(Mx[piv][c]) < 1e-12) { singular = true; return; }
       if (piv != c)
         for (int j = 0; j <= d; ++j) std::swap(Mx[c][j], Mx[piv][j]);
       for (int i = c + 1; i < d; ++i) {
@@ -786,6 +792,15 @@ Status build_q_tables(const PlanTables& T, const double* lattice, double ds, std
       (*gather)[static_cast<size_t>(b) * Mvol + q] = static_cast<int32_t>(g);
     }
   }
+  };
+  const long nthreads = std::max(1L, std::min<long>(std::min(16u, std::max(1u, std::thread::hardware_concurrency())),
+                                                    Mvol / 4096));
+  std::vector<std::thread> pool;
+  const long per = (Mvol + nthreads - 1) / nthreads;
+  for (long k = 1; k < nthreads; ++k) pool.emplace_back(fibers, std::min(Mvol, k * per), std::min(Mvol, (k + 1) * per));
+  fibers(0, std::min(Mvol, per));
+  for (auto& th : pool) th.join();
+  if (singular) { *err = "singular alias matrix B"; return Status::kInvalid; }
   return Status::kOk;
 }
 
