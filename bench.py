@@ -227,6 +227,34 @@ def cpu_reference_sample(budget_s=12.0):
             "sample": f"{len(times)} single fields of Im-3m 128^3 FP64 (median), numpy/pocketfft single thread"}
 
 
+def cpu_fullgrid_fft_sample(budget_s=4.0, workers=1):
+    """The full-grid baseline the reference's benches time beside the KRFFT
+    (test/bench_centered_scft.jl:53-81, test/bench_m7_forward_backward.jl:59-62): an
+    in-place complex FP64 FFT of the whole N^3 grid, forward then inverse, here with
+    scipy.fft (pocketfft) on `workers` threads.  Median us per field."""
+    import scipy.fft as sf
+
+    u = np.random.default_rng(1).standard_normal((NEDGE,) * 3).astype(np.complex128)
+    x = u.copy()
+
+    def one():
+        y = sf.fftn(x, workers=workers, overwrite_x=True)
+        return sf.ifftn(y, workers=workers, overwrite_x=True)
+
+    one()
+    times, t_end = [], time.perf_counter() + budget_s
+    while time.perf_counter() < t_end or len(times) < 3:
+        x[...] = u
+        t0 = time.perf_counter()
+        one()
+        times.append(time.perf_counter() - t0)
+        if len(times) >= 30:
+            break
+    return {"value": float(np.median(times)) * 1e6, "unit": UNIT, "cores": workers,
+            "sample": f"{len(times)} complex FP64 {NEDGE}^3 fftn + ifftn (median), scipy.fft pocketfft, "
+                      f"{workers} thread(s)"}
+
+
 def cpu_reference_throughput(steps, warmup):
     """All host cores: one forked worker per core (no GPU in this process), each running
     whole fields; one step = one field per worker.  Returns us per field (wall time of
@@ -472,6 +500,12 @@ def run_ours(args):
             line["cpu_baseline"] = cpu_reference_sample(budget_s=12.0)
         except Exception as exc:  # the baseline is reported, never required
             line["cpu_baseline"] = {"error": repr(exc)}
+        try:
+            cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+            line["cpu_fullgrid_fft"] = {"single_thread": cpu_fullgrid_fft_sample(4.0, 1),
+                                        "all_cores": cpu_fullgrid_fft_sample(4.0, cores)}
+        except Exception as exc:
+            line["cpu_fullgrid_fft"] = {"error": repr(exc)}
     # The metric's second half (SCFT time-to-tolerance, learned start vs plain start),
     # measured after the headline's timed region: two timed pairs of solves.
     if rank == 0 and world == 1 and not args.no_attach:

@@ -50,3 +50,16 @@ def test_reference_arm_is_silent_on_other_ranks():
                         "--warmup", "0"], env=env, capture_output=True, text=True, timeout=180, cwd=ROOT)
     assert r.returncode == 0, r.stderr
     assert r.stdout.strip() == ""
+
+
+def test_fullgrid_fft_baseline_sample():
+    # the full-grid complex FFT baseline reported beside cpu_baseline: a positive median
+    # over at least three timed fields, with its thread count
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("bench_under_test_fft", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    r = bench.cpu_fullgrid_fft_sample(budget_s=0.1, workers=2)
+    assert r["value"] > 0 and r["cores"] == 2 and r["unit"] == bench.UNIT
+    assert r["sample"].startswith(("3 ", "4 ", "5 ")) or int(r["sample"].split()[0]) >= 3
