@@ -420,6 +420,18 @@ cfft_status cfft_sno_get_grads(cfft_sno model, float* host) {
   return ret(cfft::sno_get_grads(reinterpret_cast<cfft::SnoModel*>(model), host, &err), err);
 }
 
+cfft_status cfft_sno_grads_device(cfft_sno model, void* dst, void* stream) {
+  if (!model || !dst) return ret(Status::kInvalid, "null argument");
+  std::string err;
+  return ret(cfft::sno_grads_device(reinterpret_cast<cfft::SnoModel*>(model), dst, stream, &err), err);
+}
+
+cfft_status cfft_sno_apply_grads(cfft_sno model, const void* grads, double lr, void* stream) {
+  if (!model) return ret(Status::kInvalid, "null argument");
+  std::string err;
+  return ret(cfft::sno_apply_grads(reinterpret_cast<cfft::SnoModel*>(model), grads, lr, stream, &err), err);
+}
+
 cfft_status cfft_sno_bind(cfft_sno model, cfft_plan plan, int group_slot, const double* shift, int max_samples,
                           cfft_sno_ctx* ctx) {
   if (!model || !plan || !shift || !ctx) return ret(Status::kInvalid, "null argument");

@@ -1036,7 +1036,41 @@ Status check_status_word(SnoCtx* c, cudaStream_t st, std::string* err) {
   return Status::kOk;
 }
 
+// One Adam step from the model's gradient buffer, then the BF16 working copies.
+Status adam_step(SnoModel* m, double lr, cudaStream_t st, std::string* err) {
+  m->t += 1;
+  const SnoConfig& k = m->cfg;
+  const float c1 = static_cast<float>(1.0 - std::pow(k.beta1, static_cast<double>(m->t)));
+  const float c2 = static_cast<float>(1.0 - std::pow(k.beta2, static_cast<double>(m->t)));
+  k_sno_adam<<<grid_for(LP::total, 256), 256, 0, st>>>(m->w, m->g, m->m, m->v, LP::total, static_cast<float>(lr),
+                                                       static_cast<float>(k.beta1), static_cast<float>(k.beta2),
+                                                       static_cast<float>(k.eps), static_cast<float>(k.weight_decay),
+                                                       c1, c2);
+  k_sno_to_bf16<<<grid_for(BL::total, 256), 256, 0, st>>>(m->w, m->wb);
+  add_launches(2);
+  SNO_CUDA(cudaGetLastError(), "SNO optimiser launch");
+  return Status::kOk;
+}
+
 }  // namespace
+
+Status sno_grads_device(const SnoModel* m, void* dst, void* stream, std::string* err) {
+  SNO_CUDA(cudaMemcpyAsync(dst, m->g, LP::total * sizeof(float), cudaMemcpyDeviceToDevice,
+                           static_cast<cudaStream_t>(stream)),
+           "SNO gradient copy");
+  return Status::kOk;
+}
+
+Status sno_apply_grads(SnoModel* m, const void* grads, double lr, void* stream, std::string* err) {
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (grads && grads != m->g)
+    SNO_CUDA(cudaMemcpyAsync(m->g, grads, LP::total * sizeof(float), cudaMemcpyDeviceToDevice, st),
+             "SNO gradient upload");
+  Status s = adam_step(m, lr, st, err);
+  if (s != Status::kOk) return s;
+  SNO_CUDA(cudaStreamSynchronize(st), "SNO optimiser");
+  return Status::kOk;
+}
 
 Status sno_predict(SnoCtx* c, const double* params, int S, void* w_out, void* stream, std::string* err) {
   if (!c || !params || !w_out || S < 1 || S > c->S) { *err = "invalid SNO predict arguments"; return Status::kInvalid; }
@@ -1056,19 +1090,7 @@ Status sno_train(SnoCtx* c, const double* params, int S, const void* w_target, d
   if (s != Status::kOk) return s;
   if ((s = backward_t(c, prm, S, static_cast<const float*>(w_target), st, err)) != Status::kOk) return s;
   SnoModel* m = c->model;
-  if (step) {
-    m->t += 1;
-    const SnoConfig& k = m->cfg;
-    const float c1 = static_cast<float>(1.0 - std::pow(k.beta1, static_cast<double>(m->t)));
-    const float c2 = static_cast<float>(1.0 - std::pow(k.beta2, static_cast<double>(m->t)));
-    k_sno_adam<<<grid_for(LP::total, 256), 256, 0, st>>>(m->w, m->g, m->m, m->v, LP::total, static_cast<float>(lr),
-                                                         static_cast<float>(k.beta1), static_cast<float>(k.beta2),
-                                                         static_cast<float>(k.eps), static_cast<float>(k.weight_decay),
-                                                         c1, c2);
-    k_sno_to_bf16<<<grid_for(BL::total, 256), 256, 0, st>>>(m->w, m->wb);
-    add_launches(2);
-    SNO_CUDA(cudaGetLastError(), "SNO optimiser launch");
-  }
+  if (step && (s = adam_step(m, lr, st, err)) != Status::kOk) return s;
   if (loss) {
     double h = 0.0;
     SNO_CUDA(cudaMemcpyAsync(&h, c->loss, sizeof(double), cudaMemcpyDeviceToHost, st), "SNO loss read");

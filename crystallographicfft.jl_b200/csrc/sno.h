@@ -47,6 +47,8 @@ void sno_model_destroy(SnoModel* m);
 Status sno_set_params(SnoModel* m, const float* host, std::string* err);
 Status sno_get_params(const SnoModel* m, float* host, std::string* err);
 Status sno_get_grads(const SnoModel* m, float* host, std::string* err);
+Status sno_grads_device(const SnoModel* m, void* dst, void* stream, std::string* err);
+Status sno_apply_grads(SnoModel* m, const void* grads, double lr, void* stream, std::string* err);
 
 // A model bound to one FP32 KRFFT plan (cubic group, P = M^3 a multiple of 128) for up
 // to max_samples samples per call; group_slot is the one-hot slot (0 Im-3m, 1 Ia-3d,

@@ -34,6 +34,8 @@ _SIGS = {
     "cfft_sno_set_params": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "cfft_sno_get_params": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     "cfft_sno_get_grads": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "cfft_sno_grads_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "cfft_sno_apply_grads": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p]),
     "cfft_sno_bind": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                      ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
     "cfft_sno_unbind": (ctypes.c_int, [ctypes.c_void_p]),
@@ -84,6 +86,30 @@ class SpectralNeuralOperator:
         out = np.empty(N_PARAMS, dtype=np.float32)
         check(LIB.cfft_sno_get_grads(self._h, out.ctypes.data))
         return out
+
+    def grads_device(self, out=None):
+        """Gradients of the last train_step as a float32 CUDA tensor (N_PARAMS), copied on
+        the current stream: the buffer a data-parallel step averages over ranks."""
+        torch = _torch()
+        if out is None:
+            out = torch.empty(N_PARAMS, dtype=torch.float32, device="cuda")
+        elif out.numel() != N_PARAMS or out.dtype != torch.float32 or not (out.is_cuda and out.is_contiguous()):
+            raise CFFTError(1, f"out must be a contiguous float32 CUDA tensor of {N_PARAMS} entries")
+        check(LIB.cfft_sno_grads_device(self._h, ctypes.c_void_p(out.data_ptr()),
+                                        ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+        return out
+
+    def apply_grads(self, grads=None, lr=None):
+        """One Adam step from `grads` (float32 CUDA tensor of N_PARAMS) or, with None, from
+        the gradients of the last train_step."""
+        torch = _torch()
+        ptr = None
+        if grads is not None:
+            if grads.numel() != N_PARAMS or grads.dtype != torch.float32 or not (grads.is_cuda and grads.is_contiguous()):
+                raise CFFTError(1, f"grads must be a contiguous float32 CUDA tensor of {N_PARAMS} entries")
+            ptr = ctypes.c_void_p(grads.data_ptr())
+        check(LIB.cfft_sno_apply_grads(self._h, ptr, float(self.lr if lr is None else lr),
+                                       ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
 
     def save(self, path):
         """Weights as BF16 bits (the precision the network computes with) in an .npy file."""
@@ -153,6 +179,26 @@ class SNOContext:
                                  self._stream()))
         return loss.value
 
+    def train_step_data_parallel(self, params, w_target, n_total, dist, lr=None, grad_buf=None):
+        """One data-parallel training step over the ranks of a process group (one GPU
+        per rank): this rank's samples (params, w_target; possibly none) out of n_total
+        in the global mini-batch.  The local gradient of the mean loss is weighted by the
+        rank's share of the samples, summed over the ranks by one all-reduce, and every
+        rank applies the same Adam step.  Returns the global mean loss."""
+        torch = _torch()
+        a = np.asarray(params, dtype=np.float64).reshape(-1, 2)
+        n_local = a.shape[0]
+        g = grad_buf if grad_buf is not None else torch.empty(N_PARAMS + 1, dtype=torch.float32, device="cuda")
+        if n_local:
+            loss = self.train_step(a, w_target, lr=lr, step=False)
+            self.model.grads_device(g[:N_PARAMS])
+        else:
+            loss = 0.0
+            g[:N_PARAMS].zero_()
+        total_loss = allreduce_mean_grads(g, loss, n_local, n_total, dist)
+        self.model.apply_grads(g[:N_PARAMS], lr=lr)
+        return total_loss
+
     def close(self):
         if getattr(self, "_h", None):
             LIB.cfft_sno_unbind(self._h)
@@ -163,3 +209,25 @@ class SNOContext:
             self.close()
         except Exception:
             pass
+
+
+def shard_of(indices, rank, world):
+    """This rank's slice of a global mini-batch (every world-th sample from `rank`)."""
+    return indices[rank::world]
+
+
+def sample_share(n_local, n_total):
+    """Weight of a rank's mean-loss gradient in the global mean: its share of the samples."""
+    return float(n_local) / float(n_total) if n_total else 0.0
+
+
+def allreduce_mean_grads(buf, loss, n_local, n_total, dist):
+    """buf = [gradient of this rank's mean loss | one spare entry].  Weights the gradient
+    by the rank's share of the samples, puts the weighted loss in the spare entry and
+    sums the buffer over the ranks with one all-reduce, so buf[:-1] becomes the gradient
+    of the global mean loss on every rank.  Returns the global mean loss."""
+    w = sample_share(n_local, n_total)
+    buf[:-1].mul_(w)
+    buf[-1] = loss * w
+    dist.all_reduce(buf)
+    return float(buf[-1].item())

@@ -2,6 +2,11 @@
 
     python crystallographicfft.jl_b200/train_warmstart.py --out WEIGHTS.npy --report REPORT.json
 
+or, data parallel on G GPUs of one node (one process per GPU, NCCL):
+
+    python -m torch.distributed.run --nnodes=1 --nproc-per-node G --master-addr 127.0.0.1 \
+        crystallographicfft.jl_b200/train_warmstart.py --out WEIGHTS.npy --report REPORT.json
+
 1. Training and held-out sets: AB diblock melts (b = 1, Ns = 100, cubic cell 3.8 b sqrt(N))
    with (chiN, f) drawn uniformly from [12, 30] x [0.30, 0.50], solved by the library's
    SCFT driver at 64^3 from the seeded plain start to a residual of 1e-4, for Ia-3d
@@ -66,13 +71,29 @@ def main():
     cf = _load_package()
     from crystallographicfft_b200 import warmstart as ws
 
+    # Under torchrun (one process per GPU) the data solves are split over the GPUs and the
+    # training is data parallel (one NCCL all-reduce of the gradients per step); rank 0
+    # saves the weights and runs the evaluation.
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(minutes=20))
+    gen = ws.generate if dist is None else (lambda gg, d, **kw: ws.generate_sharded(gg, d, dist, **kw))
+
     t_start = time.time()
     logs = []
 
     def log(msg):
         line = f"[{time.time() - t_start:7.1f}s] {msg}"
         logs.append(line)
-        print(line, flush=True)
+        if rank == 0:
+            print(line, flush=True)
 
     def parse(spec):
         return [(int(g), int(c)) for g, c in (x.split(":") for x in spec.split(","))]
@@ -84,14 +105,14 @@ def main():
     data = {}
     for k, (g, cnt) in enumerate(train_spec if a.weights is None else []):
         d = ws.draws(cnt, seed=1000 + k)
-        fld, st, tm = ws.generate(grids[g], d, threads=a.threads, log=log, max_iter=caps.get(g, 1000))
+        fld, st, tm = gen(grids[g], d, threads=a.threads, log=log, max_iter=caps.get(g, 1000))
         ok = np.array([s["err"] < 1e-3 for s in st])
         data[g] = dict(params=d[ok], fields=fld[torch.as_tensor(np.nonzero(ok)[0], device="cuda")].contiguous(),
                        F=np.array([s["F"] for s in st])[ok], seconds=float(np.sum(tm)), dropped=int((~ok).sum()))
     tests = {}
     for k, (g, cnt) in enumerate(test_spec):
         d = ws.draws(cnt, seed=2000 + k)
-        fld, st, tm = ws.generate(grids[g], d, threads=a.threads, log=log, max_iter=caps.get(g, 1000))
+        fld, st, tm = gen(grids[g], d, threads=a.threads, log=log, max_iter=caps.get(g, 1000))
         tests[g] = dict(params=d, fields=fld, states=st)
     gen_s = time.time() - t_start
     log(f"data generated in {gen_s:.1f} s")
@@ -106,19 +127,28 @@ def main():
             sets.append((ctxs[g], data[g]["params"], data[g]["fields"]))
     t0 = time.time()
     if a.weights is None:
-        hist = ws.train(model, sets, a.epochs, batch=a.batch, lr=a.lr, log=log, max_seconds=a.train_seconds)
-        log(f"trained {a.epochs} epochs in {time.time() - t0:.1f} s, final loss {hist[-1]:.3e}")
-        os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
-        model.save(a.out)
+        hist = ws.train(model, sets, a.epochs, batch=a.batch, lr=a.lr, log=log, max_seconds=a.train_seconds,
+                        dist=dist)
+        log(f"trained {a.epochs} epochs in {time.time() - t0:.1f} s on {world} GPU(s), final loss {hist[-1]:.3e}")
+        if rank == 0:
+            os.makedirs(os.path.dirname(os.path.abspath(a.out)), exist_ok=True)
+            model.save(a.out)
     else:
         model.load(a.weights)
         hist = [float("nan")]
     train_s = time.time() - t0
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+        if rank != 0:  # the evaluation runs on rank 0 alone
+            for o in list(ctxs.values()) + list(plans.values()) + [model]:
+                o.close()
+            return
 
     # held-out: field error of the prediction
     report = dict(grid=a.grid, weights=a.weights or a.out, train={str(g): dict(n=int(len(v["params"])), dropped=v["dropped"],
                                                    solve_seconds=v["seconds"]) for g, v in data.items()},
-                  epochs=a.epochs, batch=a.batch, lr=a.lr, loss_history=[float(x) for x in hist[::5]] + [float(hist[-1])],
+                  epochs=a.epochs, batch=a.batch, lr=a.lr, gpus=world, loss_history=[float(x) for x in hist[::5]] + [float(hist[-1])],
                   generate_seconds=gen_s, train_seconds=train_s, params=int(cf.sno.N_PARAMS))
     held = []
     for g, t in tests.items():

@@ -4,9 +4,11 @@ reference counterpart).
 - `GroupGrid`: a group on a grid with its seeded plain start (Gaussian-filtered noise
   symmetrised over the group, the same noise for every (chiN, f)).
 - `generate`: converged fields of draws (chiN, f) from the plain start, solved on
-  several host threads: the training and held-out sets.
+  several host threads: the training and held-out sets (`generate_sharded` splits the
+  draws over the GPUs of a process group and gathers the results).
 - `train`: Adam over shuffled mini-batches of one group at a time (contexts of one
-  model bound to each group's plan), cosine learning-rate decay.
+  model bound to each group's plan), cosine learning-rate decay; optionally data
+  parallel over the ranks of a process group (one gradient all-reduce per step).
 - `time_to_tol`: FP32 iterations to a switch residual, then FP64 to the tolerance,
   from the plain start (simple mixing first, `PLAIN`) or from a prediction (Anderson
   mixing from the first iteration, `WARM`), timed with CUDA events.
@@ -19,6 +21,7 @@ import time
 
 import numpy as np
 
+from . import sno
 from . import symmetry as sym
 from ._lib import CFFTError
 from .plans import _torch
@@ -116,16 +119,58 @@ def generate(gg, draws, tol=1e-4, schedule=None, max_iter=1000, threads=8, log=N
     return out, states, times
 
 
+def gather_rows(local, extra, n, dist):
+    """Reassemble rows computed round-robin over the ranks (rank r holds rows r, r + world,
+    ...): `local` is this rank's tensor of rows and `extra` a list of per-row Python
+    objects.  Returns the n rows in order and the n objects, on every rank."""
+    torch = _torch()
+    world, rank = dist.get_world_size(), dist.get_rank()
+    n_max = (n + world - 1) // world
+    pad = torch.zeros((n_max,) + tuple(local.shape[1:]), dtype=local.dtype, device=local.device)
+    pad[: local.shape[0]] = local
+    bufs = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(bufs, pad)
+    objs = [None] * world
+    dist.all_gather_object(objs, list(extra))
+    out = torch.empty((n,) + tuple(local.shape[1:]), dtype=local.dtype, device=local.device)
+    rows = [None] * n
+    for r in range(world):
+        idx = list(range(r, n, world))
+        if idx:
+            out[torch.as_tensor(idx, device=local.device)] = bufs[r][: len(idx)]
+        for j, i in enumerate(idx):
+            rows[i] = objs[r][j]
+    return out, rows
+
+
+def generate_sharded(gg, draws_, dist, **kw):
+    """`generate` with the draws split round-robin over the ranks of a process group (one
+    GPU per rank): every rank solves its share and receives all fields, states and times."""
+    world, rank = dist.get_world_size(), dist.get_rank()
+    mine = draws_[rank::world]
+    fld, st, tm = generate(gg, mine, **kw)
+    out, rows = gather_rows(fld, list(zip(st, tm)), len(draws_), dist)
+    return out, [r[0] for r in rows], [r[1] for r in rows]
+
+
 def draws(n, seed, chiN_range=(12.0, 30.0), f_range=(0.30, 0.50)):
     rng = np.random.default_rng(seed)
     return np.stack([rng.uniform(*chiN_range, n), rng.uniform(*f_range, n)], axis=1)
 
 
-def train(model, sets, epochs, batch=16, lr=1e-3, lr_final=1e-5, seed=0, log=None, max_seconds=None):
+def train(model, sets, epochs, batch=16, lr=1e-3, lr_final=1e-5, seed=0, log=None, max_seconds=None, dist=None):
     """sets: list of (ctx, params (n, 2), fields tensor (n, 2, M...)).  Cosine learning-rate
     decay from lr to lr_final; one mini-batch of one group per step.  Returns the mean
-    loss of each epoch; stops after the epoch that passes max_seconds."""
+    loss of each epoch; stops after the epoch that passes max_seconds.
+
+    With `dist` (torch.distributed, one GPU per rank, every rank holding the same sets)
+    each mini-batch is split over the ranks and the gradients are averaged by one
+    all-reduce per step (SpectralNeuralOperator's data-parallel step); every rank draws
+    the same shuffles from `seed`, so the ranks agree on the batches and the weights."""
     torch = _torch()
+    world = dist.get_world_size() if dist is not None else 1
+    rank = dist.get_rank() if dist is not None else 0
+    gbuf = torch.empty(sno.N_PARAMS + 1, dtype=torch.float32, device="cuda") if world > 1 else None
     t0 = time.time()
     rng = np.random.default_rng(seed)
     steps_per_epoch = sum((len(p) + batch - 1) // batch for _, p, _ in sets)
@@ -141,8 +186,14 @@ def train(model, sets, epochs, batch=16, lr=1e-3, lr_final=1e-5, seed=0, log=Non
         for si, idx in jobs:
             ctx, p, fld = sets[si]
             cur = lr_final + 0.5 * (lr - lr_final) * (1 + np.cos(np.pi * k / max(total - 1, 1)))
-            sel = torch.as_tensor(idx, device="cuda")
-            acc += ctx.train_step(p[idx], fld.index_select(0, sel).contiguous(), lr=cur)
+            if world > 1:
+                mine = sno.shard_of(idx, rank, world)
+                sel = torch.as_tensor(mine, device="cuda")
+                acc += ctx.train_step_data_parallel(p[mine], fld.index_select(0, sel).contiguous(), len(idx), dist,
+                                                    lr=cur, grad_buf=gbuf)
+            else:
+                sel = torch.as_tensor(idx, device="cuda")
+                acc += ctx.train_step(p[idx], fld.index_select(0, sel).contiguous(), lr=cur)
             k += 1
         hist.append(acc / len(jobs))
         if log and (ep % 10 == 0 or ep == epochs - 1):

@@ -343,6 +343,15 @@ cfft_status cfft_sno_set_params(cfft_sno model, const float* host);
 cfft_status cfft_sno_get_params(cfft_sno model, float* host);
 /* Gradients of the last cfft_sno_train call (host copy, parameter order). */
 cfft_status cfft_sno_get_grads(cfft_sno model, float* host);
+/* Data-parallel training over several GPUs (one process per GPU): each rank calls
+ * cfft_sno_train with step = 0 on its own samples, copies the gradients into a device
+ * buffer of cfft_sno_param_count() floats with cfft_sno_grads_device, averages that
+ * buffer over the ranks (an NCCL all-reduce), and then applies one Adam step from it
+ * with cfft_sno_apply_grads (grads = NULL uses the model's own gradient buffer).
+ * cfft_sno_train with step != 0 equals cfft_sno_train with step = 0 followed by
+ * cfft_sno_apply_grads(model, NULL, lr).  cfft_sno_apply_grads synchronises the stream. */
+cfft_status cfft_sno_grads_device(cfft_sno model, void* dst, void* stream);
+cfft_status cfft_sno_apply_grads(cfft_sno model, const void* grads, double lr, void* stream);
 /* Binds the model to a plan: shift is the fractional origin shift of the plan's
  * operations (find_optimal_shift), so the input features are the same functions of
  * position on every grid. */

@@ -63,3 +63,23 @@ def test_fullgrid_fft_baseline_sample():
     r = bench.cpu_fullgrid_fft_sample(budget_s=0.1, workers=2)
     assert r["value"] > 0 and r["cores"] == 2 and r["unit"] == bench.UNIT
     assert r["sample"].startswith(("3 ", "4 ", "5 ")) or int(r["sample"].split()[0]) >= 3
+
+
+def test_warmstart_data_parallel_host_logic_two_gloo_ranks():
+    # the warm-start network's data-parallel step on CPU ranks: share-weighted gradients
+    # of the ranks' shards sum to the full mini-batch gradient and mean loss (also when a
+    # rank has no sample), and round-robin generated rows come back in order
+    port = _free_port()
+    procs = []
+    for rank in range(2):
+        env = dict(os.environ, RANK=str(rank), WORLD_SIZE="2", MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, os.path.join(ROOT, "tests", "dp_worker.py")], env=env,
+                                      stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    for p in procs:
+        out, err = p.communicate(timeout=180)
+        assert p.returncode == 0, err
+        o = json.loads(out.strip().splitlines()[-1])
+        assert o["grad_err"] < 1e-12 and o["loss_err"] < 1e-12
+        assert o["grad1_err"] < 1e-12 and o["loss1_err"] < 1e-12
+        assert o["rows"] == [[10.0 * i, i + 0.5] for i in range(5)]
+        assert o["objs"] == [f"row{i}" for i in range(5)]

@@ -115,3 +115,63 @@ def test_sno_training_reduces_loss_and_save_load(cf, O, tmp_path):
     assert np.max(np.abs(after - before)) <= 2e-2 * np.max(np.abs(before))
     for o in (ctx, ctx2, model, m2, plan):
         o.close()
+
+
+
+def _adam_first_step(w, g, lr, b1=0.9, b2=0.999, eps=1e-8):
+    """Adam's first step from zero moments (cfft_sno_create's defaults, no weight decay)."""
+    m = (1 - b1) * g / (1 - b1)
+    v = (1 - b2) * g * g / (1 - b2)
+    return w - lr * m / (np.sqrt(v) + eps)
+
+
+def test_sno_split_step_and_data_parallel_step(cf, O):
+    # cfft_sno_grads_device copies the gradients of the last train call; cfft_sno_apply_grads
+    # takes one Adam step from a caller's gradient buffer; the data-parallel step on a
+    # one-rank NCCL group (share 1, all-reduce of one rank) takes that step from the
+    # all-reduced buffer.  Each is checked against Adam's first step on the host from the
+    # exact gradients used (the gradient reductions use atomics, so two separate runs
+    # may differ in the last bits).
+    import datetime
+    import socket
+
+    import torch.distributed as dist
+
+    N = (16, 16, 16)
+    lr = 1e-3
+    plan, shift, oops, a = _case(cf, O, 229, N)
+    t = _targets(O, oops, N, 2)
+    w_t = np.stack([np.stack(S.w_from_output(t[s], c, f)) for s, (c, f) in enumerate(PARAMS)])
+    wt_dev = torch.tensor(_to_sub(w_t, plan.L), dtype=torch.float32, device="cuda")
+
+    m1 = cf.SpectralNeuralOperator(lr=lr)
+    c1 = m1.bind(plan, 229, shift, 2)
+    w0 = m1.get_params().astype(np.float64)
+    loss1 = c1.train_step(PARAMS, wt_dev, step=False)
+    g = m1.grads_device()
+    assert np.array_equal(g.cpu().numpy(), m1.grads())
+    g_used = (0.5 * g).contiguous()  # any caller buffer, not the model's own gradients
+    m1.apply_grads(g_used)
+    want = _adam_first_step(w0, g_used.cpu().numpy().astype(np.float64), lr)
+    assert np.max(np.abs(m1.get_params() - want)) <= 1e-6 * lr + 1e-7 * np.max(np.abs(w0))
+
+    m2 = cf.SpectralNeuralOperator(lr=lr)
+    c2 = m2.bind(plan, 229, shift, 2)
+    assert np.array_equal(m2.get_params(), w0.astype(np.float32))  # seeded initial weights
+    buf = torch.empty(cf.sno.N_PARAMS + 1, dtype=torch.float32, device="cuda")
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        loss2 = c2.train_step_data_parallel(PARAMS, wt_dev, len(PARAMS), dist, grad_buf=buf)
+        torch.cuda.synchronize()
+    finally:
+        dist.destroy_process_group()
+    assert abs(loss2 - loss1) <= 1e-5 * abs(loss1)
+    assert abs(float(buf[-1]) - loss2) <= 1e-6 * abs(loss2)
+    want2 = _adam_first_step(w0, buf[:-1].cpu().numpy().astype(np.float64), lr)
+    assert np.max(np.abs(m2.get_params() - want2)) <= 1e-6 * lr + 1e-7 * np.max(np.abs(w0))
+    for o in (c1, c2, m1, m2, plan):
+        o.close()
