@@ -50,89 +50,54 @@ def _check_spec(plan, spec):
         raise CFFTError(1, "spectral ASU does not belong to this plan")
 
 
-def plan_krfft_recursive(spec, ops_shifted, **kw):
-    """plan_krfft_recursive (src/recursive_blocks.jl:64-145)."""
-    return VariantKRFFTPlan("recursive", spec, ops_shifted, **kw)
+# The forward variants by their reference names.  Each row: plan constructor (with its
+# reference lines), execute function (with its reference lines), and whether the execute
+# function takes the spectral indexing as the reference's does.  Every one computes the
+# spectral-ASU spectrum of a full-grid field on the batched subgrid pipeline; the names
+# exist so that a caller of the reference finds them.
+_FORWARD = [
+    ("recursive", "plan_krfft_recursive", "src/recursive_blocks.jl:64-145",
+     "execute_recursive_krfft", "src/recursive_blocks.jl:323-331", True),
+    ("sparse", "plan_krfft_sparse", "src/recursive_blocks.jl:514-630",
+     "execute_sparse_krfft", "src/recursive_blocks.jl:631-670", True),
+    ("selective", "plan_krfft_selective", "src/recursive_blocks.jl:756-889",
+     "execute_selective_krfft", "src/recursive_blocks.jl:890-957", True),
+    ("g0asu", "plan_krfft_g0asu", "src/recursive_blocks.jl:1034-1245",
+     "execute_g0asu_krfft", "src/recursive_blocks.jl:1246-1312", True),
+    ("g0asu_general", "plan_krfft_g0asu_general", "src/recursive_blocks.jl:1378-1553",
+     "execute_general_g0asu_krfft", "src/recursive_blocks.jl:1554-1588", True),
+    ("fractal", "plan_fractal_krfft", "src/fractal_krfft.jl:678-723",
+     "execute_fractal_krfft", "src/fractal_krfft.jl:869-901", False),
+    ("fractal_v2", "plan_fractal_krfft_v2", "src/fractal_krfft.jl:1021-1171",
+     "execute_fractal_krfft_v2", "src/fractal_krfft.jl:1228-1279", False),
+    ("fractal_v3", "plan_fractal_krfft_v3", "src/fractal_krfft_v3.jl:205-380",
+     "execute_fractal_krfft_v3", "src/fractal_krfft_v3.jl:381-452", False),
+]
 
 
-def execute_recursive_krfft(plan, spec, u):
-    """execute_recursive_krfft! (src/recursive_blocks.jl:323-331): spectrum on the ASU."""
-    _check_spec(plan, spec)
-    return plan.execute(u)
+def _forward_pair(kind, plan_name, plan_cite, exec_name, exec_cite, takes_spec):
+    def make(spec, ops_shifted, **kw):
+        return VariantKRFFTPlan(kind, spec, ops_shifted, **kw)
+
+    if takes_spec:
+        def run(plan, spec, u):
+            _check_spec(plan, spec)
+            return plan.execute(u)
+    else:
+        def run(plan, u):
+            return plan.execute(u)
+
+    make.__name__, run.__name__ = plan_name, exec_name
+    make.__doc__ = f"{plan_name} ({plan_cite}): a VariantKRFFTPlan on the device path."
+    run.__doc__ = f"{exec_name}! ({exec_cite}): the spectrum on the spectral ASU of the full-grid field u."
+    return make, run
 
 
-def plan_krfft_sparse(spec, ops_shifted, **kw):
-    """plan_krfft_sparse (src/recursive_blocks.jl:514-630)."""
-    return VariantKRFFTPlan("sparse", spec, ops_shifted, **kw)
-
-
-def execute_sparse_krfft(plan, spec, u):
-    """execute_sparse_krfft! (src/recursive_blocks.jl:631-670)."""
-    _check_spec(plan, spec)
-    return plan.execute(u)
-
-
-def plan_krfft_selective(spec, ops_shifted, **kw):
-    """plan_krfft_selective (src/recursive_blocks.jl:756-889)."""
-    return VariantKRFFTPlan("selective", spec, ops_shifted, **kw)
-
-
-def execute_selective_krfft(plan, spec, u):
-    """execute_selective_krfft! (src/recursive_blocks.jl:890-957)."""
-    _check_spec(plan, spec)
-    return plan.execute(u)
-
-
-def plan_krfft_g0asu(spec, ops_shifted, **kw):
-    """plan_krfft_g0asu (src/recursive_blocks.jl:1034-1245; cubic P3c or the general path)."""
-    return VariantKRFFTPlan("g0asu", spec, ops_shifted, **kw)
-
-
-def execute_g0asu_krfft(plan, spec, u):
-    """execute_g0asu_krfft! (src/recursive_blocks.jl:1246-1312)."""
-    _check_spec(plan, spec)
-    return plan.execute(u)
-
-
-def plan_krfft_g0asu_general(spec, ops_shifted, **kw):
-    """plan_krfft_g0asu_general (src/recursive_blocks.jl:1378-1553)."""
-    return VariantKRFFTPlan("g0asu_general", spec, ops_shifted, **kw)
-
-
-def execute_general_g0asu_krfft(plan, spec, u):
-    """execute_general_g0asu_krfft! (src/recursive_blocks.jl:1554-1588)."""
-    _check_spec(plan, spec)
-    return plan.execute(u)
-
-
-def plan_fractal_krfft(spec, ops_shifted, **kw):
-    """plan_fractal_krfft (src/fractal_krfft.jl:678-723)."""
-    return VariantKRFFTPlan("fractal", spec, ops_shifted, **kw)
-
-
-def execute_fractal_krfft(plan, u):
-    """execute_fractal_krfft! (src/fractal_krfft.jl:869-901): spectrum on the ASU."""
-    return plan.execute(u)
-
-
-def plan_fractal_krfft_v2(spec, ops_shifted, **kw):
-    """plan_fractal_krfft_v2 (src/fractal_krfft.jl:1021-1171)."""
-    return VariantKRFFTPlan("fractal_v2", spec, ops_shifted, **kw)
-
-
-def execute_fractal_krfft_v2(plan, u):
-    """execute_fractal_krfft_v2! (src/fractal_krfft.jl:1228-1279)."""
-    return plan.execute(u)
-
-
-def plan_fractal_krfft_v3(spec, ops_shifted, **kw):
-    """plan_fractal_krfft_v3 (src/fractal_krfft_v3.jl:205-380)."""
-    return VariantKRFFTPlan("fractal_v3", spec, ops_shifted, **kw)
-
-
-def execute_fractal_krfft_v3(plan, u):
-    """execute_fractal_krfft_v3! (src/fractal_krfft_v3.jl:381-452)."""
-    return plan.execute(u)
+for _row in _FORWARD:
+    _make, _run = _forward_pair(*_row)
+    globals()[_make.__name__] = _make
+    globals()[_run.__name__] = _run
+del _row, _make, _run
 
 
 class G0ASUBackwardPlan:
