@@ -88,6 +88,8 @@ def _load():
         "cfft_block_backward": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
         "cfft_calc_asu": (c_int, [c_int, ctypes.POINTER(c_int), c_int, c_int32_p, c_int32_p, c_int,
                                   ctypes.POINTER(c_int), c_int32_p, c_int32_p, c_int32_p]),
+        "cfft_fractal_tree": (c_int, [c_int, ctypes.POINTER(c_int), c_int, c_int32_p, c_int32_p, c_int, c_int,
+                                      ctypes.POINTER(c_int), ctypes.POINTER(c_int), c_int32_p]),
         "cfft_subgrid_spectrum": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
         "cfft_plan_rep_ops": (c_int, [c_void_p, c_int32_p, c_int32_p]),
         "cfft_plan_backward_tables": (c_int, [c_void_p, c_int32_p, c_int32_p, c_int32_p]),

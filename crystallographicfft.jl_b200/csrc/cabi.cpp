@@ -284,6 +284,28 @@ cfft_status cfft_calc_asu(int dim, const int* N, int n_ops, const int32_t* R, co
   return CFFT_OK;
 }
 
+cfft_status cfft_fractal_tree(int dim, const int* N, int n_ops, const int32_t* R, const int32_t* t, int flags, int cap,
+                              int* n_leaves, int* n_inner, int32_t* leaves) {
+  if (!n_leaves || !n_inner) return ret(Status::kInvalid, "null argument");
+  std::string err;
+  int n[3];
+  std::vector<cfft::SymOp> ops;
+  if (!read_N(dim, N, n, &err) || !read_ops(dim, n_ops, R, t, &ops, &err)) return ret(Status::kInvalid, err);
+  if (flags < 0 || flags > 3) return ret(Status::kInvalid, "flags must be 0..3");
+  std::vector<cfft::TreeLeaf> lv;
+  cfft::fractal_tree(ops, n, dim, flags, &lv, n_inner);
+  *n_leaves = static_cast<int>(lv.size());
+  if (!leaves) return CFFT_OK;
+  if (cap < *n_leaves) return ret(Status::kInvalid, "capacity too small for the tree's leaves");
+  for (size_t k = 0; k < lv.size(); ++k)
+    for (int d = 0; d < 3; ++d) {
+      leaves[9 * k + d] = lv[k].n[d];
+      leaves[9 * k + 3 + d] = lv[k].scale[d];
+      leaves[9 * k + 6 + d] = lv[k].offset[d];
+    }
+  return CFFT_OK;
+}
+
 cfft_status cfft_plan_q_tables(cfft_plan plan, double* Q, int32_t* gather) {
   if (!plan) return ret(Status::kInvalid, "null plan");
   const auto* p = reinterpret_cast<cfft::Plan*>(plan);

@@ -4,6 +4,7 @@
 // integer table (spectral-ASU points, multiplicities, L, M, fold offsets) is
 // identical to the reference's.
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <climits>
 #include <cmath>
@@ -948,6 +949,255 @@ std::vector<AsuPoint> calc_asu(const std::vector<SymOp>& ops_in, const int* N_in
     return std::lexicographical_compare(a.idx, a.idx + 3, b.idx, b.idx + 3);
   });
   return out;
+}
+
+// ---------------------------------------------------------------------------------
+// Recursive parity tree of the fractal KRFFT plans (build_recursive_tree and
+// collect_leaves, src/fractal_krfft.jl:133-636).  A node splits the dimensions whose
+// parity every diagonal operation preserves into even and odd sectors; sectors related
+// by an operation of the half-grid-shifted group (t' = t + (I - R)/2 mod N, rounded
+// half to even as the reference rounds it) share one representative child, which keeps
+// the operations that map its sector to itself, rewritten in its own coordinates:
+// R' = S^-1 R S, t' = S^-1 (R p + t - p).  A node whose operations are all pure
+// translations splits into its alive (non-extinct) sectors, each a leaf.
+namespace {
+
+struct TreeOp {
+  int R[3][3];
+  long t[3];
+};
+struct TreeNode {
+  int n[3], scale[3], offset[3];
+  std::vector<TreeOp> ops;
+  std::vector<int> children;
+  bool leaf = false;
+};
+
+long round_half_even_twice(long x2) {  // round(x2 / 2), ties to even
+  const long q = (x2 >= 0) ? x2 / 2 : -((-x2 + 1) / 2);  // floor(x2 / 2)
+  if (x2 - 2 * q == 0) return q;
+  return (q % 2 == 0) ? q : q + 1;
+}
+
+bool tree_identity(const int (&R)[3][3], int D) {
+  for (int i = 0; i < D; ++i)
+    for (int j = 0; j < D; ++j)
+      if (R[i][j] != (i == j ? 1 : 0)) return false;
+  return true;
+}
+
+}  // namespace
+
+void fractal_tree(const std::vector<SymOp>& ops_in, const int* N, int D, int flags, std::vector<TreeLeaf>* leaves,
+                  int* n_inner) {
+  const bool child_shifted_t = flags & 1, centering_split = !(flags & 2);
+  std::vector<TreeNode> nodes(1);
+  for (int d = 0; d < 3; ++d) {
+    nodes[0].n[d] = d < D ? N[d] : 1;
+    nodes[0].scale[d] = 1;
+    nodes[0].offset[d] = 0;
+  }
+  for (const auto& op : ops_in) {
+    TreeOp o{};
+    for (int i = 0; i < 3; ++i) {
+      o.t[i] = i < D ? op.t[i] : 0;
+      for (int j = 0; j < 3; ++j) o.R[i][j] = (i < D && j < D) ? op.R[i][j] : (i == j);
+    }
+    nodes[0].ops.push_back(o);
+  }
+  std::vector<int> stack{0};
+  while (!stack.empty()) {
+    const int id = stack.back();
+    stack.pop_back();
+    int cN[3];
+    for (int d = 0; d < 3; ++d) cN[d] = nodes[id].n[d];
+    bool zero = false;
+    for (int d = 0; d < D; ++d) zero = zero || cN[d] == 0;
+    if (zero) { nodes[id].leaf = true; continue; }
+    const std::vector<TreeOp> ops = nodes[id].ops;  // copy: nodes may grow below
+    bool nontrivial = false;
+    for (const auto& o : ops) nontrivial = nontrivial || !tree_identity(o.R, D);
+    if (!nontrivial) {
+      // centring translations only (_setup_centering_split!, src/fractal_krfft.jl:535-604)
+      std::vector<std::array<long, 3>> cent;
+      for (const auto& o : ops) {
+        std::array<long, 3> tm{0, 0, 0};
+        bool any = false;
+        for (int d = 0; d < D; ++d) { tm[d] = floor_mod(o.t[d], cN[d]); any = any || tm[d] != 0; }
+        if (any) cent.push_back(tm);
+      }
+      bool big = true;
+      for (int d = 0; d < D; ++d) big = big && cN[d] >= 2;
+      if (!(centering_split && !cent.empty() && big)) { nodes[id].leaf = true; continue; }
+      std::vector<int> split;
+      for (int d = 0; d < D; ++d)
+        if (cN[d] >= 2 && cN[d] % 2 == 0) split.push_back(d);
+      std::set<std::array<long, 3>> group{{0, 0, 0}};
+      std::vector<std::array<long, 3>> queue{{0, 0, 0}};
+      for (const auto& t : cent)
+        if (group.insert(t).second) queue.push_back(t);
+      while (!queue.empty()) {
+        const auto g = queue.back();
+        queue.pop_back();
+        for (const auto& t : cent) {
+          std::array<long, 3> h{0, 0, 0};
+          for (int d = 0; d < D; ++d) h[d] = floor_mod(g[d] + t[d], cN[d]);
+          if (group.insert(h).second) queue.push_back(h);
+        }
+      }
+      const int nsec = 1 << split.size();
+      for (int bits = 0; bits < nsec; ++bits) {
+        int p[3] = {0, 0, 0};
+        for (size_t k = 0; k < split.size(); ++k) p[split[k]] = (bits >> k) & 1;
+        double re = 0.0, im = 0.0;
+        for (const auto& tau : group) {
+          double ph = 0.0;
+          for (int d = 0; d < D; ++d) ph += static_cast<double>(p[d]) * tau[d] / cN[d];
+          re += std::cos(2.0 * M_PI * ph);
+          im -= std::sin(2.0 * M_PI * ph);
+        }
+        if (std::hypot(re, im) < 0.5) continue;  // extinct sector
+        TreeNode c;
+        for (int d = 0; d < 3; ++d) {
+          const bool sp = std::find(split.begin(), split.end(), d) != split.end();
+          c.n[d] = sp ? cN[d] / 2 : cN[d];
+          c.scale[d] = nodes[id].scale[d] * (sp ? 2 : 1);
+          c.offset[d] = nodes[id].scale[d] * p[d] + nodes[id].offset[d];
+        }
+        c.leaf = true;
+        nodes.push_back(c);
+        nodes[id].children.push_back(static_cast<int>(nodes.size()) - 1);
+      }
+      continue;
+    }
+    // splittable dimensions (find_split_dims, src/fractal_krfft.jl:159-186)
+    std::vector<int> split;
+    for (int d = 0; d < D; ++d) {
+      if (cN[d] % 2 != 0 || cN[d] <= 1) continue;
+      bool ok = true;
+      for (const auto& o : ops) {
+        bool diag = true;
+        for (int i = 0; i < D && diag; ++i)
+          for (int j = 0; j < D && diag; ++j)
+            if (i != j && o.R[i][j] != 0) diag = false;
+        if (!diag) continue;
+        if (floor_mod(o.t[d], 2) != 0 || floor_mod(o.R[d][d] + o.t[d], 2) != 1) { ok = false; break; }
+      }
+      if (ok) split.push_back(d);
+    }
+    bool all_small = true;
+    for (int d = 0; d < D; ++d) all_small = all_small && cN[d] <= 1;
+    if (split.empty() || all_small) { nodes[id].leaf = true; continue; }
+    const int nsec = 1 << split.size();
+    std::vector<std::array<int, 3>> par(nsec);
+    for (int bits = 0; bits < nsec; ++bits) {
+      par[bits] = {0, 0, 0};
+      for (size_t k = 0; k < split.size(); ++k) par[bits][split[k]] = (bits >> k) & 1;
+    }
+    auto in_split = [&](int d) { return std::find(split.begin(), split.end(), d) != split.end(); };
+    // half-grid-shifted translations (shift_ops_half_grid, src/fractal_krfft.jl:262-283)
+    std::vector<std::array<long, 3>> tsh(ops.size());
+    for (size_t k = 0; k < ops.size(); ++k)
+      for (int d = 0; d < 3; ++d) {
+        if (d >= D) { tsh[k][d] = 0; continue; }
+        long x2 = 2 * ops[k].t[d];
+        for (int j = 0; j < D; ++j) x2 += (d == j ? 1 : 0) - ops[k].R[d][j];
+        tsh[k][d] = round_half_even_twice(floor_mod(x2, 2L * cN[d]));
+      }
+    auto image = [&](size_t k, const std::array<int, 3>& p, int* img) {
+      for (int d = 0; d < D; ++d) {
+        long s = tsh[k][d];
+        for (int j = 0; j < D; ++j) s += static_cast<long>(ops[k].R[d][j]) * p[j];
+        img[d] = static_cast<int>(floor_mod(s, 2));
+      }
+    };
+    // sector orbits (find_sector_orbits, src/fractal_krfft.jl:203-250)
+    auto sector_of = [&](const int* img) {
+      int bits = 0;
+      for (size_t k = 0; k < split.size(); ++k) bits |= img[split[k]] << k;
+      return bits;
+    };
+    std::vector<int> orbit_rep(nsec);
+    std::vector<char> visited(nsec, 0);
+    for (int i = 0; i < nsec; ++i) orbit_rep[i] = i;
+    for (int i = 0; i < nsec; ++i) {
+      if (visited[i]) continue;
+      visited[i] = 1;
+      for (size_t k = 0; k < ops.size(); ++k) {
+        int img[3] = {0, 0, 0};
+        image(k, par[i], img);
+        const int j = sector_of(img);  // non-split dimensions are ignored
+        if (!visited[j]) { visited[j] = 1; orbit_rep[j] = i; }
+      }
+    }
+    std::vector<int> reps(orbit_rep.begin(), orbit_rep.end());
+    std::sort(reps.begin(), reps.end());
+    reps.erase(std::unique(reps.begin(), reps.end()), reps.end());
+    int S[3];
+    for (int d = 0; d < 3; ++d) S[d] = in_split(d) ? 2 : 1;
+    for (int ri : reps) {
+      const auto& p = par[ri];
+      TreeNode c;
+      for (int d = 0; d < 3; ++d) {
+        c.n[d] = in_split(d) ? cN[d] / 2 : cN[d];
+        c.scale[d] = nodes[id].scale[d] * S[d];
+        c.offset[d] = nodes[id].scale[d] * p[d] + nodes[id].offset[d];
+      }
+      for (size_t k = 0; k < ops.size(); ++k) {
+        int img[3] = {0, 0, 0};
+        image(k, p, img);
+        bool self = true;
+        for (int d : split) self = self && img[d] == p[d];
+        if (!self) continue;
+        TreeOp o{};
+        bool valid = true;
+        for (int i = 0; i < 3 && valid; ++i) {
+          for (int j = 0; j < 3; ++j) {
+            const long rv = static_cast<long>(ops[k].R[i][j]) * S[j];
+            if (rv % S[i] != 0) { valid = false; break; }
+            o.R[i][j] = static_cast<int>(rv / S[i]);
+          }
+          if (!valid || i >= D) { o.t[i] = 0; continue; }
+          long tv = (child_shifted_t ? tsh[k][i] : ops[k].t[i]) - p[i];
+          for (int j = 0; j < D; ++j) tv += static_cast<long>(ops[k].R[i][j]) * p[j];
+          if (tv % S[i] != 0) { valid = false; break; }
+          o.t[i] = tv / S[i];
+        }
+        if (!valid) continue;
+        bool dup = false;  // _deduplicate_ops: exact (R, t)
+        for (const auto& e : c.ops) {
+          bool same = true;
+          for (int i = 0; i < 3 && same; ++i) {
+            same = e.t[i] == o.t[i];
+            for (int j = 0; j < 3 && same; ++j) same = e.R[i][j] == o.R[i][j];
+          }
+          if (same) { dup = true; break; }
+        }
+        if (!dup) c.ops.push_back(o);
+      }
+      nodes.push_back(std::move(c));
+      const int cid = static_cast<int>(nodes.size()) - 1;
+      nodes[id].children.push_back(cid);
+      stack.push_back(cid);
+    }
+  }
+  // collect_leaves: depth first, children in order
+  leaves->clear();
+  *n_inner = 0;
+  std::vector<int> order{0};
+  while (!order.empty()) {
+    const int id = order.back();
+    order.pop_back();
+    const TreeNode& nd = nodes[id];
+    if (nd.leaf) {
+      TreeLeaf l{};
+      for (int d = 0; d < 3; ++d) { l.n[d] = nd.n[d]; l.scale[d] = nd.scale[d]; l.offset[d] = nd.offset[d]; }
+      leaves->push_back(l);
+      continue;
+    }
+    ++*n_inner;
+    for (auto it = nd.children.rbegin(); it != nd.children.rend(); ++it) order.push_back(*it);
+  }
 }
 
 }  // namespace cfft

@@ -121,6 +121,25 @@ def find_optimal_shift(ops, N):
     return shift[:dim], shifted
 
 
+def fractal_tree(ops, N, *, flags=0):
+    """build_recursive_tree + collect_leaves (src/fractal_krfft.jl:300-636) in the
+    library's plan layer.  Returns (leaves, n_inner): leaves is an int32 array
+    (n_leaves, 3, 3) of [grid size, stride, offset] per leaf in collect_leaves order.
+    flags: 0 = the current source; 1 = child translations from the half-grid-shifted
+    operations, 2 = no centring split (3 = both, the construction of the reference's
+    tree survey)."""
+    dim = ops[0].dim
+    R, t = _pack(ops)
+    Nc = _Nc(N, dim)
+    n, inner = ctypes.c_int(0), ctypes.c_int(0)
+    check(LIB.cfft_fractal_tree(dim, Nc, len(ops), _ptr(R), _ptr(t), int(flags), 0, ctypes.byref(n),
+                                ctypes.byref(inner), None))
+    out = np.zeros((n.value, 9), dtype=np.int32)
+    check(LIB.cfft_fractal_tree(dim, Nc, len(ops), _ptr(R), _ptr(t), int(flags), n.value, ctypes.byref(n),
+                                ctypes.byref(inner), _ptr(out)))
+    return out.reshape(n.value, 3, 3)[:, :, :dim], int(inner.value)
+
+
 def count_special_positions(N, ops) -> int:
     """_count_special_positions_fast (src/asu.jl:372-438)."""
     dim = ops[0].dim

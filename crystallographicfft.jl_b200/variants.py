@@ -28,15 +28,58 @@ from ._lib import CFFTError
 from .plans import PATH_AUTO, PATH_M2, KRFFTPlan, _is_tensor, _torch, fullgrid_to_subgrid
 
 
-class VariantKRFFTPlan:
-    """A variant forward plan (spectral ASU from the full grid) on the device path."""
+class FractalLeaf:
+    """A leaf of the recursive parity tree: its grid, and the stride and offset at which
+    it samples the full grid (FractalNode, src/fractal_krfft.jl:32-98)."""
 
-    def __init__(self, kind, spec, ops_shifted, *, precision=8, max_batch=1, path=PATH_AUTO):
+    def __init__(self, subgrid_N, scale, offset):
+        self.subgrid_N, self.scale, self.offset = tuple(subgrid_N), tuple(scale), tuple(offset)
+        self.is_leaf = True
+
+
+class FractalTree:
+    """build_recursive_tree (src/fractal_krfft.jl:300-520), built by the library's plan
+    layer: its leaves in collect_leaves order and the number of inner nodes."""
+
+    def __init__(self, N, ops, flags=0):
+        arr, self.n_inner = sym.fractal_tree(ops, N, flags=flags)
+        self.N = tuple(N)
+        self.leaves = [FractalLeaf(a[0], a[1], a[2]) for a in arr]
+        self.n_leaves = len(self.leaves)
+
+    def fft_points(self):
+        """Total FFT points of the leaves (the volume the tree transforms)."""
+        return int(sum(np.prod(l.subgrid_N) for l in self.leaves))
+
+
+def build_recursive_tree(N, ops):
+    """build_recursive_tree(N, ops) (src/fractal_krfft.jl:300-520)."""
+    return FractalTree(tuple(N), ops)
+
+
+calc_asu_tree = build_recursive_tree  # src/fractal_krfft.jl:946
+
+
+def collect_leaves(tree):
+    """collect_leaves (src/fractal_krfft.jl:622-636)."""
+    return list(tree.leaves)
+
+
+class VariantKRFFTPlan:
+    """A variant forward plan (spectral ASU from the full grid) on the device path.  The
+    fractal kinds also hold the reference's plan-time tree (tree, n_leaves, n_inner,
+    like FractalCFFTPlan, src/fractal_krfft.jl:104-114); the transform itself runs on the
+    batched subgrid pipeline."""
+
+    def __init__(self, kind, spec, ops_shifted, *, precision=8, max_batch=1, path=PATH_AUTO, device=True):
         self.kind = kind
         self.spec = spec
-        self.plan = KRFFTPlan(spec, ops_shifted, precision=precision, max_batch=max_batch, path=path)
+        self.plan = KRFFTPlan(spec, ops_shifted, precision=precision, max_batch=max_batch, path=path, device=device)
         self.n_spec = self.plan.n_spec
         self.N = tuple(spec.N)
+        if kind.startswith("fractal"):
+            self.tree = FractalTree(self.N, ops_shifted)
+            self.n_leaves, self.n_inner = self.tree.n_leaves, self.tree.n_inner
 
     def execute(self, u):
         return self.plan.forward(fullgrid_to_subgrid(self.plan, u))

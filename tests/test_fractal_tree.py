@@ -15,6 +15,7 @@ default.
 import json
 import os
 
+import numpy as np
 import pytest
 
 from oracle import fractal_tree as FT
@@ -67,3 +68,74 @@ def test_reference_tree_assertions(O):
         for l in leaves:
             assert all(o < s for o, s in zip(l.offset, l.scale))
             assert all(n * s == 16 for n, s in zip(l.subgrid_N, l.scale))
+
+
+def _oracle_leaves(O, N, ops, **kw):
+    return [(l.subgrid_N, l.scale, l.offset) for l in FT.collect_leaves(FT.build_recursive_tree(N, ops, **kw))]
+
+
+def _oracle_inner(node):
+    return 0 if node.is_leaf else 1 + sum(_oracle_inner(c) for c in node.children)
+
+
+def _lib_leaves(cf, N, ops, flags):
+    arr, inner = cf.fractal_tree([cf.SymOp(op.R, op.t) for op in ops], N, flags=flags)
+    return [tuple(tuple(int(v) for v in a[k]) for k in range(3)) for a in arr], inner
+
+
+@pytest.mark.parametrize("sg", [2, 16, 20, 22, 47, 70, 123, 136, 141, 195, 196, 200, 216, 221, 225, 227, 229, 230])
+def test_library_tree_equals_oracle(cf, O, sg):
+    # the library's plan-layer tree, leaf by leaf (grid, stride, offset, in collect_leaves
+    # order), for the current source and for the survey's construction, on the unshifted
+    # and the shifted operations
+    N = (32, 32, 32)
+    ops = O.get_ops(sg, 3, N)
+    for o in (ops, O.find_optimal_shift(ops, N)[1]):
+        for flags, kw in ((0, {}), (3, dict(child_shifted_t=True, centering_split=False))):
+            got, inner = _lib_leaves(cf, N, o, flags)
+            assert got == _oracle_leaves(O, N, o, **kw), (sg, flags)
+            assert inner == _oracle_inner(FT.build_recursive_tree(N, o, **kw)), (sg, flags)
+
+
+def test_library_tree_reproduces_reference_survey(cf, O):
+    bad = []
+    for sg, row in _survey().items():
+        lib_ops = cf.get_ops(int(sg), 3, N64)
+        arr, _ = cf.fractal_tree(lib_ops, N64, flags=3)
+        ratio = 64 ** 3 / float(sum(int(a[0][0]) * int(a[0][1]) * int(a[0][2]) for a in arr))
+        if round(ratio, 1) != row["ratio"]:
+            bad.append(sg)
+    assert not bad, bad
+
+
+def test_fractal_plan_tree(cf, O):
+    # FractalCFFTPlan's n_leaves / n_inner (src/fractal_krfft.jl:104-114) on the plan; the
+    # P1 tree is a single leaf (test/test_fractal_krfft.jl:69-80)
+    N = (16, 16, 16)
+    ops = O.get_ops(221, 3, N)
+    lib_ops = [cf.SymOp(op.R, op.t) for op in ops]
+    tree = cf.build_recursive_tree(N, lib_ops)
+    assert [(l.subgrid_N, l.scale, l.offset) for l in cf.collect_leaves(tree)] == _oracle_leaves(O, N, ops)
+    assert tree.fft_points() == sum(int(np.prod(l[0])) for l in _oracle_leaves(O, N, ops))
+    ident = [cf.SymOp(((1, 0, 0), (0, 1, 0), (0, 0, 1)), (0, 0, 0))]
+    p1 = cf.calc_asu_tree((8, 8, 8), ident)
+    assert p1.n_leaves == 1 and p1.n_inner == 0 and p1.leaves[0].subgrid_N == (8, 8, 8)
+
+
+def test_fractal_variant_plans_hold_the_tree(cf, O):
+    # plan_fractal_krfft / _v2 / _v3 carry the tree of the operations they were given
+    # (host-only plans: the tables, not the device path)
+    N = (16, 16, 16)
+    oops = O.get_ops(221, 3, N)  # unshifted, as test/test_fractal_krfft.jl passes them
+    ops_s = [cf.SymOp(op.R, op.t) for op in oops]
+    spec = cf.calc_spectral_asu(ops_s, 3, N)
+    want = _oracle_leaves(O, N, oops)
+    inner = _oracle_inner(FT.build_recursive_tree(N, oops))
+    for make in (cf.plan_fractal_krfft, cf.plan_fractal_krfft_v2, cf.plan_fractal_krfft_v3):
+        plan = make(spec, ops_s, device=False)
+        assert plan.n_leaves == len(want) and plan.n_inner == inner
+        assert [(l.subgrid_N, l.scale, l.offset) for l in plan.tree.leaves] == want
+        plan.close()
+    plan = cf.plan_krfft_g0asu(spec, ops_s, device=False)
+    assert not hasattr(plan, "tree")
+    plan.close()
