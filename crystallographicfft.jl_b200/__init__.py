@@ -8,6 +8,7 @@ from ._lib import LIB, CFFTError, LIB_PATH  # noqa: F401
 from .symmetry import (  # noqa: F401
     SymOp, SpectralIndexing, apply_op, auto_L, available_groups, calc_spectral_asu, check_shift_invariance,
     count_special_positions, detect_centering_type, dual_ops, find_optimal_shift, fractal_tree, get_k_vector, get_ops,
+    shift_ops_half_grid,
     strip_centering, MIRROR_ADAPTATION_TABLE, MirrorAdaptationEntry, get_mirror_adaptation, needs_basis_change,
     needs_dct_path,
 )
@@ -24,7 +25,7 @@ from .plans import (  # noqa: F401
 
 from .variants import (  # noqa: F401
     FractalLeaf, FractalTree, G0ASUBackwardPlan, StagedPm3mPlan, VariantKRFFTPlan, build_recursive_tree,
-    calc_asu_tree, collect_leaves, execute_fractal_krfft, execute_fractal_krfft_v2,
+    calc_asu_tree, collect_leaves, tree_summary, execute_fractal_krfft, execute_fractal_krfft_v2,
     execute_fractal_krfft_v3, execute_g0asu_ikrfft, execute_g0asu_krfft, execute_general_g0asu_krfft,
     execute_recursive_krfft, execute_selective_krfft, execute_sparse_krfft, execute_staged, execute_staged_full,
     lookup_full_spectrum, plan_fractal_krfft, plan_fractal_krfft_v2, plan_fractal_krfft_v3, plan_krfft_g0asu,

@@ -297,12 +297,14 @@ cfft_status cfft_fractal_tree(int dim, const int* N, int n_ops, const int32_t* R
   *n_leaves = static_cast<int>(lv.size());
   if (!leaves) return CFFT_OK;
   if (cap < *n_leaves) return ret(Status::kInvalid, "capacity too small for the tree's leaves");
-  for (size_t k = 0; k < lv.size(); ++k)
+  for (size_t k = 0; k < lv.size(); ++k) {
     for (int d = 0; d < 3; ++d) {
-      leaves[9 * k + d] = lv[k].n[d];
-      leaves[9 * k + 3 + d] = lv[k].scale[d];
-      leaves[9 * k + 6 + d] = lv[k].offset[d];
+      leaves[10 * k + d] = lv[k].n[d];
+      leaves[10 * k + 3 + d] = lv[k].scale[d];
+      leaves[10 * k + 6 + d] = lv[k].offset[d];
     }
+    leaves[10 * k + 9] = lv[k].depth;
+  }
   return CFFT_OK;
 }
 

@@ -967,7 +967,7 @@ struct TreeOp {
   long t[3];
 };
 struct TreeNode {
-  int n[3], scale[3], offset[3];
+  int n[3], scale[3], offset[3], depth = 0;
   std::vector<TreeOp> ops;
   std::vector<int> children;
   bool leaf = false;
@@ -1065,6 +1065,7 @@ void fractal_tree(const std::vector<SymOp>& ops_in, const int* N, int D, int fla
           c.offset[d] = nodes[id].scale[d] * p[d] + nodes[id].offset[d];
         }
         c.leaf = true;
+        c.depth = nodes[id].depth + 1;
         nodes.push_back(c);
         nodes[id].children.push_back(static_cast<int>(nodes.size()) - 1);
       }
@@ -1175,6 +1176,7 @@ void fractal_tree(const std::vector<SymOp>& ops_in, const int* N, int D, int fla
         }
         if (!dup) c.ops.push_back(o);
       }
+      c.depth = nodes[id].depth + 1;
       nodes.push_back(std::move(c));
       const int cid = static_cast<int>(nodes.size()) - 1;
       nodes[id].children.push_back(cid);
@@ -1192,6 +1194,7 @@ void fractal_tree(const std::vector<SymOp>& ops_in, const int* N, int D, int fla
     if (nd.leaf) {
       TreeLeaf l{};
       for (int d = 0; d < 3; ++d) { l.n[d] = nd.n[d]; l.scale[d] = nd.scale[d]; l.offset[d] = nd.offset[d]; }
+      l.depth = nd.depth;
       leaves->push_back(l);
       continue;
     }

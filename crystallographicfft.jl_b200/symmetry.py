@@ -12,7 +12,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._lib import LIB, check
+from ._lib import LIB, CFFTError, check
 
 CENTERING_NAMES = {0: "P", 1: "C", 2: "A", 3: "I", 4: "F"}
 
@@ -123,8 +123,9 @@ def find_optimal_shift(ops, N):
 
 def fractal_tree(ops, N, *, flags=0):
     """build_recursive_tree + collect_leaves (src/fractal_krfft.jl:300-636) in the
-    library's plan layer.  Returns (leaves, n_inner): leaves is an int32 array
-    (n_leaves, 3, 3) of [grid size, stride, offset] per leaf in collect_leaves order.
+    library's plan layer.  Returns (leaves, depths, n_inner): leaves is an int32 array
+    (n_leaves, 3, dim) of [grid size, stride, offset] per leaf in collect_leaves order,
+    depths the leaves' depths below the root.
     flags: 0 = the current source; 1 = child translations from the half-grid-shifted
     operations, 2 = no centring split (3 = both, the construction of the reference's
     tree survey)."""
@@ -134,10 +135,26 @@ def fractal_tree(ops, N, *, flags=0):
     n, inner = ctypes.c_int(0), ctypes.c_int(0)
     check(LIB.cfft_fractal_tree(dim, Nc, len(ops), _ptr(R), _ptr(t), int(flags), 0, ctypes.byref(n),
                                 ctypes.byref(inner), None))
-    out = np.zeros((n.value, 9), dtype=np.int32)
+    out = np.zeros((n.value, 10), dtype=np.int32)
     check(LIB.cfft_fractal_tree(dim, Nc, len(ops), _ptr(R), _ptr(t), int(flags), n.value, ctypes.byref(n),
                                 ctypes.byref(inner), _ptr(out)))
-    return out.reshape(n.value, 3, 3)[:, :, :dim], int(inner.value)
+    return out[:, :9].reshape(n.value, 3, 3)[:, :, :dim], out[:, 9].copy(), int(inner.value)
+
+
+def shift_ops_half_grid(ops, N):
+    """shift_ops_half_grid (src/fractal_krfft.jl:262-283): the operations with the grid
+    origin moved by half a grid step, t' = t + (I - R) b mod N with b = 1/2 in every
+    dimension.  The fractal plans of the reference expect fields symmetric under these.
+    Raises when a translation becomes fractional (e.g. hexagonal rotations), which the
+    grid-unit operations here cannot hold."""
+    out = []
+    for op in ops:
+        D, R = op.dim, op.Rm
+        t2 = [2 * int(op.t[d]) + sum((1 if d == j else 0) - int(R[d, j]) for j in range(D)) for d in range(D)]
+        if any(v % 2 for v in t2):
+            raise CFFTError(1, "shift_ops_half_grid: a shifted translation is not on the grid")
+        out.append(SymOp(op.R, tuple((v // 2) % N[d] for d, v in enumerate(t2))))
+    return out
 
 
 def count_special_positions(N, ops) -> int:

@@ -42,9 +42,10 @@ class FractalTree:
     layer: its leaves in collect_leaves order and the number of inner nodes."""
 
     def __init__(self, N, ops, flags=0):
-        arr, self.n_inner = sym.fractal_tree(ops, N, flags=flags)
+        arr, depths, self.n_inner = sym.fractal_tree(ops, N, flags=flags)
         self.N = tuple(N)
         self.leaves = [FractalLeaf(a[0], a[1], a[2]) for a in arr]
+        self.depths = [int(d) for d in depths]
         self.n_leaves = len(self.leaves)
 
     def fft_points(self):
@@ -63,6 +64,12 @@ calc_asu_tree = build_recursive_tree  # src/fractal_krfft.jl:946
 def collect_leaves(tree):
     """collect_leaves (src/fractal_krfft.jl:622-636)."""
     return list(tree.leaves)
+
+
+def tree_summary(tree):
+    """tree_summary (src/fractal_krfft.jl:653-667): leaves, inner nodes, deepest leaf."""
+    return dict(n_gp_leaves=tree.n_leaves, n_sp_nodes=tree.n_inner,
+                max_depth=max(tree.depths) if tree.depths else 0)
 
 
 class VariantKRFFTPlan:

@@ -121,9 +121,10 @@ cfft_status cfft_block_backward(cfft_block_plan plan, const void* in, void* out,
 /* build_recursive_tree + collect_leaves (src/fractal_krfft.jl:300-636): the recursive
  * parity tree that the fractal plans (plan_fractal_krfft, src/fractal_krfft.jl:678-723;
  * plan_fractal_krfft_v2/v3) are built on, from the operations (R row-major n_ops x 9,
- * t n_ops x 3, grid units).  leaves receives n_leaves x 9 int32 (grid size[3],
- * stride[3], offset[3] in the full grid) in collect_leaves order, *n_inner the number
- * of inner nodes; call with leaves = NULL to query *n_leaves.  flags = 0 follows the
+ * t n_ops x 3, grid units).  leaves receives n_leaves x 10 int32 (grid size[3],
+ * stride[3], offset[3] in the full grid, depth below the root) in collect_leaves
+ * order, *n_inner the number of inner nodes; call with leaves = NULL to query
+ * *n_leaves.  flags = 0 follows the
  * current source; bit 0 takes child translations from the half-grid-shifted
  * operations and bit 1 skips the centring split (the construction of the reference
  * version that wrote its tree survey, test/debug_tree_output.log). */

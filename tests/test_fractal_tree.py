@@ -79,7 +79,7 @@ def _oracle_inner(node):
 
 
 def _lib_leaves(cf, N, ops, flags):
-    arr, inner = cf.fractal_tree([cf.SymOp(op.R, op.t) for op in ops], N, flags=flags)
+    arr, _, inner = cf.fractal_tree([cf.SymOp(op.R, op.t) for op in ops], N, flags=flags)
     return [tuple(tuple(int(v) for v in a[k]) for k in range(3)) for a in arr], inner
 
 
@@ -101,7 +101,7 @@ def test_library_tree_reproduces_reference_survey(cf, O):
     bad = []
     for sg, row in _survey().items():
         lib_ops = cf.get_ops(int(sg), 3, N64)
-        arr, _ = cf.fractal_tree(lib_ops, N64, flags=3)
+        arr, _, _ = cf.fractal_tree(lib_ops, N64, flags=3)
         ratio = 64 ** 3 / float(sum(int(a[0][0]) * int(a[0][1]) * int(a[0][2]) for a in arr))
         if round(ratio, 1) != row["ratio"]:
             bad.append(sg)
@@ -139,3 +139,27 @@ def test_fractal_variant_plans_hold_the_tree(cf, O):
     plan = cf.plan_krfft_g0asu(spec, ops_s, device=False)
     assert not hasattr(plan, "tree")
     plan.close()
+
+
+def _oracle_depths(node, d=0):
+    return [d] if node.is_leaf else [x for c in node.children for x in _oracle_depths(c, d + 1)]
+
+
+def test_tree_summary_and_half_grid_shift(cf, O):
+    # tree_summary (src/fractal_krfft.jl:653-667) and shift_ops_half_grid
+    # (src/fractal_krfft.jl:262-283), against the oracle
+    N = (16, 16, 16)
+    for sg in (47, 136, 200, 221, 229):
+        oops = O.get_ops(sg, 3, N)
+        lib = [cf.SymOp(op.R, op.t) for op in oops]
+        root = FT.build_recursive_tree(N, oops)
+        s = cf.tree_summary(cf.build_recursive_tree(N, lib))
+        assert s == dict(n_gp_leaves=len(FT.collect_leaves(root)), n_sp_nodes=_oracle_inner(root),
+                         max_depth=max(_oracle_depths(root)))
+        sh = cf.shift_ops_half_grid(lib, N)
+        want = FT._shift_half(FT._ops_int(oops, 3), N, 3)
+        assert [tuple(op.t) for op in sh] == [tuple(v % n for v, n in zip(t, N)) for _, t in want]
+        assert [op.R for op in sh] == [op.R for op in lib]
+    hexa = [cf.SymOp(op.R, op.t) for op in O.get_ops(168, 3, (12, 12, 12))]
+    with pytest.raises(cf.CFFTError):
+        cf.shift_ops_half_grid(hexa, (12, 12, 12))
