@@ -557,8 +557,11 @@ def plan_diffusion(N, lattice, sg_num, dim, ds, *, method="qfused", precision=8,
     subgrid solver.  The reference's :matrix branch (a dense real-ASU x spectral-ASU
     transform and its pseudo-inverse, src/diffusion_solver.jl:20-80) is a host-side
     dense solve outside the KRFFT path this library accelerates, and is refused, as is
-    the :krfft branch, which calls a plan_krfft(real_asu, spec_asu, ops) signature that
-    the reference's own krfft.jl does not define."""
+    the :krfft branch: the legacy solver on the mode-B plan_krfft(real_asu, spec_asu,
+    ops) of src/krfft.jl:119-389 (an FFT of every orbit block of a stride-2 packing,
+    recombined by a sparse matrix and its adjoint, map_fft! / map_ifft!), whose scale the
+    reference derived empirically (src/diffusion_solver.jl:93-160).  :qfused computes the
+    same contour step on one subgrid."""
     method = str(method).lstrip(":")
     if method == "qfused":
         ops = sym.get_ops(sg_num, dim, N)

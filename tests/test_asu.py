@@ -96,3 +96,26 @@ def test_calc_asu_large_grid(cf, O):
     pts = cf.calc_asu(N, [cf.SymOp(op.R, op.t) for op in oops_s])
     assert sum(p.multiplicity for p in pts) == 24 ** 3
     assert [(tuple(p.idx), tuple(p.depth), p.multiplicity) for p in pts] == O.calc_asu_points(N, oops_s)
+
+
+def test_pack_asu_interleaved_mode_b_cases(cf):
+    # test/test_packing_mode_b.jl: P4 at L = 2 packs 6 orbit subgrids, each u[range] with
+    # stride 2 starting at its representative; Pmmm packs 8 independent subgrids that
+    # cover the grid.  That file calls the default, but the reference's source keeps
+    # only the Gamma_0 orbit by default (asu_only = true, src/pack_asu.jl:113-143), so the
+    # counts it asserts are those of asu_only = false.
+    N = (16, 16, 16)
+    u = np.random.default_rng(0).standard_normal(N) + 1j * np.random.default_rng(1).standard_normal(N)
+    c = cf.pack_asu_interleaved(u, N, cf.get_ops(75, 3, N), L=(2, 2, 2), asu_only=False)
+    blocks = c.dim_blocks[3]
+    assert len(blocks) == 6
+    for b in blocks:
+        assert b.orbit is not None
+        assert np.array_equal(b.data, u[tuple(slice(r.start, None, r.step) for r in b.range)])
+        assert [r.start for r in b.range] == list(b.orbit.representative)
+        assert all(r.step == 2 for r in b.range)
+    c = cf.pack_asu_interleaved(u, N, cf.get_ops(47, 3, N), L=(2, 2, 2), asu_only=False)
+    blocks = c.dim_blocks[3]
+    assert len(blocks) == 8 and all(b.orbit.multiplicity == 1 for b in blocks)
+    assert sum(b.data.size for b in blocks) == 16 ** 3
+    assert len(cf.pack_asu_interleaved(u, N, cf.get_ops(75, 3, N), L=(2, 2, 2)).dim_blocks[3]) == 1

@@ -1,5 +1,6 @@
 """Legacy block path: plan_cfft + mul!/ldiv! (src/cfft_plan.jl, src/execution.jl) on the
-device block transform, mirroring test/runtests.jl:80-115 (CFFT round trip, p2mm) and
+device block transform, mirroring test/runtests.jl:80-115 and test/test_cfft.jl:74-110
+(CFFT round trip, p2mm) and
 checking every block against numpy's FFT."""
 import copy
 

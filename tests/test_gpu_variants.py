@@ -1,7 +1,8 @@
 """The reference's variant plans (recursive, sparse, selective, G0-ASU, general G0-ASU,
 G0-ASU backward, fractal v1-v3, staged Pm-3m) through their reference names on the
 device path, with the reference's own checks: test/runtests.jl:129-166,403-433,
-test/test_selective_g0.jl, test/test_general_g0_asu.jl, test/test_fractal_krfft.jl,
+test/test_selective_g0.jl, test/test_general_g0_asu.jl, test/test_g0_asu.jl,
+test/test_g0_asu_backward.jl, test/test_fractal_krfft.jl,
 test/test_staged_pm3m.jl (spectra against the full FFT of the same field)."""
 import numpy as np
 import pytest

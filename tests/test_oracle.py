@@ -71,7 +71,8 @@ def test_frequency_aliasing(O):
 
 
 def test_auto_L_pins(prep, O):
-    # test/runtests.jl:224 (Pmmm L = (2,2,2)); :394 (P2/m anisotropic)
+    # test/runtests.jl:224 (Pmmm L = (2,2,2)); :394 (P2/m anisotropic); test/test_auto_L.jl
+    # prints L for a list of groups and asserts nothing
     assert O.auto_L(prep(47, N16)["oops"]) == [2, 2, 2]
     assert O.auto_L(prep(10, N16)["oops"]) != [2, 2, 2]
 
@@ -93,7 +94,7 @@ def test_fold_fft_vs_direct(prep, O):
 
 
 def test_fold_unfold_identity(prep, O):
-    # test/runtests.jl:258-270 (1e-12)
+    # test/runtests.jl:258-270, test/test_m7_scft.jl:34-126 (1e-12)
     p = prep(229, N16)
     f0 = O.pack_stride(p["u"], [2, 2, 2])
     fp = O.plan_centering_fold("I", f0.shape)
@@ -103,7 +104,8 @@ def test_fold_unfold_identity(prep, O):
 
 @pytest.mark.parametrize("sg", [221, 225, 227, 229, 230, 47, 63, 70, 72, 10])
 def test_forward_vs_fft(prep, O, sg):
-    # test/runtests.jl:199-216 and :436-476 (centred / M2 forward vs fft(u) on the ASU)
+    # test/runtests.jl:199-216 and :436-476, test/test_krfft_fftw.jl:82-221,
+    # test/test_krfft_general.jl:13-160 (centred / M2 forward vs fft(u) on the ASU)
     p = prep(sg, N16)
     spec_o = O.calc_spectral_asu(p["oops"], 3, N16)
     plan = O.plan_krfft_centered(spec_o, p["oops"])
@@ -182,7 +184,7 @@ def test_m2q_vs_fullgrid(prep, O, sg):
 
 
 def test_m7_vs_m2q(prep, O):
-    # test/runtests.jl:273-287 (1e-12)
+    # test/runtests.jl:273-287, test/test_m7_scft.jl:131-162 (1e-12)
     p = prep(225, N16)
     plan = O.plan_m2_q_ops(p["oops"], N16, DS, LAT)
     f0 = O.pack_stride(p["u"], [2, 2, 2])
@@ -212,3 +214,17 @@ def test_m2_backward_first_row_is_alias_mean(prep, O):
         assert keep.any()
         # inv_w = x_a * sym_phase with |sym_phase| = 1  =>  |inv_w| = 1/d
         assert np.allclose(np.abs(b.inv_w[keep]), 1.0 / b.d, atol=1e-12)
+
+
+@pytest.mark.parametrize("sg", [47, 123, 136, 221, 10, 2, 230, 70, 69, 139, 227])
+def test_m2_backward_roundtrip(prep, O, sg):
+    # test/test_m2_backward.jl:69-156: plan_krfft + fft_reconstruct!, then
+    # execute_m2_backward!, recovers the symmetric field's subgrid (max error < 1e-10),
+    # for the P groups and the centred groups the reference lists (N = 16 here)
+    p = prep(sg, N16)
+    spec_o = O.calc_spectral_asu(p["oops"], 3, N16)
+    fwd = O.plan_krfft(spec_o, p["oops"])
+    bwd = O.plan_m2_backward(spec_o, p["oops"])
+    f0 = O.pack_stride(p["u"], O.auto_L(p["oops"]))
+    back = O.execute_m2_backward(bwd, O.fft_reconstruct(fwd, f0))
+    assert np.max(np.abs(np.real(back).reshape(f0.shape, order="F") - f0)) < 1e-10
