@@ -372,3 +372,137 @@ def needs_dct_path(sg: int) -> bool:
 def needs_basis_change(sg: int) -> bool:
     """needs_basis_change (src/mirror_table.jl:280-285)."""
     return not MIRROR_ADAPTATION_TABLE[sg].all_axial
+
+
+# ----------------------------------------------------------------------------------
+# Choice of the decomposition factor and of the grid (src/optimal_L.jl)
+# ----------------------------------------------------------------------------------
+
+_GRID_FOR_TABLES = 24  # every group's translations are whole grid steps at 24 per edge
+
+
+def _reach(ops, L):
+    return {tuple(int(op.t[d]) % L[d] for d in range(len(L))) for op in ops}
+
+
+def optimal_L_phase1(*args):
+    """optimal_L_phase1(ops_shifted) or optimal_L_phase1(sg, dim, N)
+    (src/optimal_L.jl:59-104,106-110) -> (L, n_active, n_reachable): L_d = 2 where some
+    shifted operation has an odd translation, the subgrids reachable from subgrid 0 are
+    {t mod L}, and when they do not cover all prod(L) subgrids L is reduced to the
+    largest set of dimensions whose subgrids are all reachable."""
+    if len(args) == 3:
+        sg, dim, N = args
+        _, ops = find_optimal_shift(get_ops(sg, dim, N), N)
+    else:
+        (ops,) = args
+    dim = ops[0].dim
+    L = [2 if any(int(op.t[d]) % 2 == 1 for op in ops) else 1 for d in range(dim)]
+    n_sub = int(np.prod(L))
+    if n_sub == 1:
+        return L, 1, 1
+    n_reach = len(_reach(ops, L))
+    n_active = n_sub // n_reach
+    if n_active > 1:  # _optimize_L_for_coverage (src/optimal_L.jl:117-166)
+        best, best_prod, best_active, best_reach = [1] * dim, 1, 1, 1
+        for mask in range(2 ** dim):
+            Lt = [2 if (mask >> d) & 1 and L[d] == 2 else 1 for d in range(dim)]
+            ns = int(np.prod(Lt))
+            if ns == 1:
+                continue
+            nr = len(_reach(ops, Lt))
+            na = ns // nr
+            if na == 1 and (ns > best_prod // max(best_active, 1) or best_active > 1):
+                best, best_prod, best_active, best_reach = Lt, ns, 1, nr
+        return best, best_active, best_reach
+    return L, n_active, n_reach
+
+
+def _point_rotations(sg, D):
+    seen, out = set(), []
+    for op in get_ops(sg, D, (_GRID_FOR_TABLES,) * D):
+        if op.R not in seen:
+            seen.add(op.R)
+            out.append(op.Rm)
+    return out
+
+
+def _rotation_order(R):
+    Rn = R.copy()
+    for n in range(1, 13):
+        if np.array_equal(Rn, np.eye(len(R), dtype=R.dtype)):
+            return n
+        Rn = Rn @ R
+    return 1
+
+
+def optimal_L(sg, D=3):
+    """optimal_L (src/optimal_L.jl:194-206): per axis, the lcm of the orders of the
+    rotations that move it (2 for a flipped axis of an improper operation), at least 2."""
+    import math
+
+    cycles = [[] for _ in range(D)]
+    for R in _point_rotations(sg, D):
+        if np.array_equal(R, np.eye(D, dtype=R.dtype)):
+            continue
+        order = _rotation_order(R)
+        for d in range(D):
+            moved = R[d, d] != 1 or any(R[d, i] != 0 or R[i, d] != 0 for i in range(D) if i != d)
+            if moved:
+                cycles[d].append(order)
+        if round(np.linalg.det(R)) < 0:
+            for d in range(D):
+                if R[d, d] == -1:
+                    cycles[d].append(2)
+    return tuple(max(math.lcm(*c), 2) if c else 2 for c in cycles)
+
+
+def optimal_L_isotropic(sg, D=3):
+    """optimal_L_isotropic (src/optimal_L.jl:215-228): the lcm of all rotation orders
+    (2 for improper operations), at least 2."""
+    import math
+
+    cycles = set()
+    for R in _point_rotations(sg, D):
+        if np.array_equal(R, np.eye(D, dtype=R.dtype)):
+            continue
+        cycles.add(_rotation_order(R))
+        if round(np.linalg.det(R)) < 0:
+            cycles.add(2)
+    return max(math.lcm(*cycles), 2) if cycles else 2
+
+
+def recommended_N(sg, target_N):
+    """recommended_N (src/optimal_L.jl:236-246): each edge rounded up to a multiple of
+    optimal_L."""
+    L = optimal_L(sg, len(target_N))
+    return tuple(L[d] * -(-int(target_N[d]) // L[d]) for d in range(len(target_N)))
+
+
+def group_order(sg, D=3):
+    """group_order (src/optimal_L.jl:258-261): |G| with every centring translation."""
+    return len(get_ops(sg, D, (_GRID_FOR_TABLES,) * D))
+
+
+def detect_centering(ops, N):
+    """detect_centering (src/recursive_blocks.jl:368-403): 'F' with at least three pure
+    translations, one of them a face vector (two halves and a zero); 'I' with a body
+    vector (1/2, 1/2, 1/2); 'P' otherwise (C, A and R centrings included)."""
+    D = len(N)
+    n_cent, body, face = 0, False, False
+    for op in ops:
+        if not np.array_equal(op.Rm, np.eye(D, dtype=np.int64)) or all(abs(int(v)) < 0.1 for v in op.t):
+            continue
+        n_cent += 1
+        frac = [int(op.t[d]) / N[d] for d in range(D)]
+        if all(abs(f - 0.5) < 0.01 for f in frac):
+            body = True
+        n_half = sum(abs(f - 0.5) < 0.01 for f in frac)
+        n_zero = sum(abs(f) < 0.01 for f in frac)
+        if n_half == 2 and n_zero == 1:
+            face = True
+    if face and n_cent >= 3:
+        return "F"
+    if body and n_cent >= 1:
+        return "I"
+    return "P"

@@ -242,3 +242,35 @@ def test_spectral_asu_open_operation_list(cf):
     group = cf.calc_spectral_asu([cf.SymOp(R, t0) for R in (I, R4, R2, R4i)], 3, N)
     assert np.array_equal(open_list.idx, group.idx) and np.array_equal(open_list.mult, group.mult)
     assert int(np.sum(group.mult)) == 12 * 12 * 6
+
+
+def test_optimal_L_module(cf, O):
+    # src/optimal_L.jl: the examples its docstrings give that its code reproduces
+    assert cf.optimal_L_phase1(47, 3, (16, 16, 16)) == ([2, 2, 2], 1, 8)
+    assert cf.optimal_L_phase1(25, 3, (16, 16, 16)) == ([2, 2, 1], 1, 4)
+    assert cf.optimal_L(75, 3) == (4, 4, 2)
+    assert cf.optimal_L(47, 3) == (2, 2, 2)  # the code's result; its docstring's (4,4,4) predates the b-shift
+    assert cf.group_order(230) == 96
+    assert cf.recommended_N(75, (30, 30, 30)) == (32, 32, 30)
+    # optimal_L_phase1's L is auto_L's (src/krfft.jl:225-279) for every group, with one
+    # active subgrid, and every grid recommended_N returns is a multiple of optimal_L
+    N = (24, 24, 24)
+    for sg in range(1, 231):
+        _, oops = O.find_optimal_shift(O.get_ops(sg, 3, N), N)
+        L, n_active, n_reach = cf.optimal_L_phase1([cf.SymOp(op.R, op.t) for op in oops])
+        assert L == O.auto_L(oops) and n_active == 1 and n_reach == int(np.prod(L)), sg
+        assert cf.group_order(sg) == len(oops)
+        Lo = cf.optimal_L(sg)
+        assert all(n % l == 0 and n >= 25 for n, l in zip(cf.recommended_N(sg, (25, 25, 25)), Lo))
+        assert cf.optimal_L_isotropic(sg) % 2 == 0 or cf.optimal_L_isotropic(sg) % 3 == 0
+
+
+def test_detect_centering_three_way(cf):
+    # detect_centering (src/recursive_blocks.jl:368-403) tells F and I apart and calls
+    # every other lattice P; detect_centering_type (src/symmetry_ops.jl:133-179) names all
+    N = (24, 24, 24)
+    for sg in range(1, 231):
+        ops = cf.get_ops(sg, 3, N)
+        full = cf.detect_centering_type(ops, N)
+        want = full if full in ("F", "I") else "P"
+        assert cf.detect_centering(ops, N) == want, (sg, full)
