@@ -9,7 +9,7 @@ from .symmetry import (  # noqa: F401
     SymOp, SpectralIndexing, apply_op, auto_L, available_groups, calc_spectral_asu, check_shift_invariance,
     count_special_positions, detect_centering_type, dual_ops, find_optimal_shift, fractal_tree, get_k_vector, get_ops,
     shift_ops_half_grid, optimal_L_phase1, optimal_L, optimal_L_isotropic, recommended_N, group_order,
-    detect_centering,
+    detect_centering, CenteringType, CentP, CentC, CentA, CentI, CentF, convert_op,
     strip_centering, MIRROR_ADAPTATION_TABLE, MirrorAdaptationEntry, get_mirror_adaptation, needs_basis_change,
     needs_dct_path,
 )

@@ -173,6 +173,34 @@ def auto_L(ops_shifted):
     return [int(v) for v in L][:dim]
 
 
+class CenteringType(str, __import__("enum").Enum):
+    """CenteringType (src/symmetry_ops.jl:122-131): the lattice centrings as the values
+    detect_centering_type returns, so that detect_centering_type(ops, N) == CentI."""
+
+    CentP = "P"
+    CentC = "C"
+    CentA = "A"
+    CentI = "I"
+    CentF = "F"
+
+
+CentP, CentC, CentA, CentI, CentF = (CenteringType.CentP, CenteringType.CentC, CenteringType.CentA,
+                                     CenteringType.CentI, CenteringType.CentF)
+
+
+def convert_op(R, t_frac, N) -> SymOp:
+    """convert_op (src/symmetry_ops.jl:38-49) for an operation given by its rotation and
+    fractional translation: the translation in grid units, round(t_frac * N), which must
+    lie within 1e-5 of a whole number of grid steps."""
+    D = len(N)
+    Rm = np.asarray(R, dtype=np.float64).reshape(D, D)
+    tg = np.asarray(t_frac, dtype=np.float64) * np.asarray(N, dtype=np.float64)
+    ti = np.rint(tg)
+    if not np.allclose(tg, ti, rtol=0.0, atol=1e-5):
+        raise CFFTError(1, f"convert_op: symmetry operation not commensurate with grid {tuple(N)}")
+    return SymOp(tuple(int(v) for v in np.rint(Rm).ravel()), tuple(int(v) for v in ti))
+
+
 def detect_centering_type(ops, N) -> str:
     """detect_centering_type (src/symmetry_ops.jl:133-179): 'P', 'C', 'A', 'I' or 'F'."""
     dim = ops[0].dim

@@ -274,3 +274,21 @@ def test_detect_centering_three_way(cf):
         full = cf.detect_centering_type(ops, N)
         want = full if full in ("F", "I") else "P"
         assert cf.detect_centering(ops, N) == want, (sg, full)
+
+
+def test_centering_enum_and_convert_op(cf):
+    # CenteringType (src/symmetry_ops.jl:122-131) compares with detect_centering_type's
+    # result; convert_op (src/symmetry_ops.jl:38-49) scales fractional translations
+    N = (16, 16, 16)
+    assert cf.detect_centering_type(cf.get_ops(229, 3, N), N) == cf.CentI
+    assert cf.detect_centering_type(cf.get_ops(225, 3, N), N) == cf.CentF
+    assert cf.detect_centering_type(cf.get_ops(47, 3, N), N) == cf.CentP
+    assert [c.value for c in cf.CenteringType] == ["P", "C", "A", "I", "F"]
+    op = cf.convert_op(((0, -1, 0), (1, 0, 0), (0, 0, 1)), (0.5, 0.0, 0.25), N)
+    assert op == cf.SymOp((0, -1, 0, 1, 0, 0, 0, 0, 1), (8, 0, 4))
+    with pytest.raises(cf.CFFTError):
+        cf.convert_op(np.eye(3), (1 / 3, 0, 0), N)
+    # every operation of the table is convert_op of its own fractional form
+    for sg in (2, 70, 167, 227, 230):
+        for o in cf.get_ops(sg, 3, (24, 24, 24)):
+            assert cf.convert_op(o.Rm, [v / 24 for v in o.t], (24, 24, 24)) == o
