@@ -79,6 +79,15 @@ def algorithmic_bytes_per_field(M, n_spec, real_bytes=4):
     return 2 * (real_bytes * int(np.prod(M)) + 2 * real_bytes * n_spec)
 
 
+def algorithmic_flops_per_field(n_ch, H, n_spec, d):
+    """FLOPs of a forward + backward, reported beside the byte roofline (not the bound):
+    n_ch complex FFTs of the H^3 channel grid each way at 5 n log2 n, and the d-tap
+    complex multiply-add of the reconstruct and of its inverse gather (8 flops a tap) at
+    each spectral point."""
+    vol = int(np.prod(H))
+    return 2 * n_ch * 5 * vol * float(np.log2(vol)) + 2 * d * 8 * n_spec
+
+
 # ----------------------------------------------------------------------------- clocks
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
@@ -475,6 +484,7 @@ def run_ours(args):
         kern = {"name": "k_plane_fwd_h" if top == 0 else "k_plane_bwd_h", "algorithmic_bytes": kb,
                 "ms": float(stage[top]), "achieved": ka, "frac": ka / hbm,
                 "note": "f0 bytes of the batch over the stage's CUDA-event time (chunks back to back on one stream)"}
+    flops_field = algorithmic_flops_per_field(plan.n_channels, plan.H, plan.n_spec, plan.info.n_rep)
     line = {
         "metric": METRIC, "value": us_field, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": False, "scaling": "weak",
@@ -489,7 +499,8 @@ def run_ours(args):
                      "peak_source": peak_src, "traffic": None,
                      "scope": "whole forward+backward per batch (6 launches per 64-field chunk); algorithmic bytes 2*(4*M^3 + 8*n_spec) per field",
                      "stage_ms": {n: float(v) for n, v in zip(names, stage)}, "dominant_stage": names[top],
-                     "dominant_kernel": kern},
+                     "dominant_kernel": kern, "flops_per_field": flops_field,
+                     "achieved_tflops": flops_field / (us_field * 1e-6) / 1e12},
         "latency_1field": lat,
         "gpu_launches": launches,
         "clocks": clk,

@@ -83,3 +83,15 @@ def test_warmstart_data_parallel_host_logic_two_gloo_ranks():
         assert o["grad1_err"] < 1e-12 and o["loss1_err"] < 1e-12
         assert o["rows"] == [[10.0 * i, i + 0.5] for i in range(5)]
         assert o["objs"] == [f"row{i}" for i in range(5)]
+
+
+def test_algorithmic_flops_of_the_headline():
+    # about 23 MFLOP per Im-3m 128^3 field: 4 channels of 32^3 both ways, 8 taps a point
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("bench_under_test_flops", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    f = bench.algorithmic_flops_per_field(4, (32, 32, 32), 22880, 8)
+    assert f == 2 * 4 * 5 * 32768 * 15 + 2 * 8 * 8 * 22880
+    assert 22e6 < f < 23e6
