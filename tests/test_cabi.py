@@ -37,3 +37,26 @@ def test_invalid_arguments(cf):
     assert lib.cfft_get_ops(229, 4, N, 0, ctypes.byref(n), None, None) == 1
     assert lib.cfft_forward(None, None, None, 1, None) == 1
     assert b"null" in lib.cfft_last_error() or lib.cfft_last_error()
+
+
+def test_fractal_tree_invalid_arguments(cf):
+    import numpy as np
+
+    lib = cf.LIB
+    N = (ctypes.c_int * 3)(8, 8, 8)
+    R = np.eye(3, dtype=np.int32).ravel()
+    t = np.zeros(3, dtype=np.int32)
+    Rp = R.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+    tp = t.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+    n, inner = ctypes.c_int(-1), ctypes.c_int(-1)
+    assert lib.cfft_fractal_tree(3, N, 1, Rp, tp, 0, 0, None, ctypes.byref(inner), None) == 1
+    assert lib.cfft_fractal_tree(4, N, 1, Rp, tp, 0, 0, ctypes.byref(n), ctypes.byref(inner), None) == 1
+    assert lib.cfft_fractal_tree(3, N, 0, Rp, tp, 0, 0, ctypes.byref(n), ctypes.byref(inner), None) == 1
+    assert lib.cfft_fractal_tree(3, N, 1, Rp, tp, 7, 0, ctypes.byref(n), ctypes.byref(inner), None) == 1
+    assert lib.cfft_fractal_tree(3, N, 1, Rp, tp, 0, 0, ctypes.byref(n), ctypes.byref(inner), None) == 0
+    assert n.value == 1 and inner.value == 0  # P1: the root is the only leaf
+    out = np.zeros(10, dtype=np.int32)
+    op = out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+    assert lib.cfft_fractal_tree(3, N, 1, Rp, tp, 0, 0, ctypes.byref(n), ctypes.byref(inner), op) == 1  # cap 0
+    assert lib.cfft_fractal_tree(3, N, 1, Rp, tp, 0, 1, ctypes.byref(n), ctypes.byref(inner), op) == 0
+    assert list(out) == [8, 8, 8, 1, 1, 1, 0, 0, 0, 0]
