@@ -12,6 +12,7 @@
 #include <numeric>
 #include <set>
 #include <thread>
+#include <unordered_map>
 
 #include "cfft_internal.h"
 
@@ -270,49 +271,142 @@ static bool rotations_form_group(const std::vector<SymOp>& rots) {
   return true;
 }
 
+// Stabiliser-phase extinction filter of calc_spectral_asu (src/spectral_indexing.jl:143-171):
+// a representative kr is kept when |sum over g with R_g kr = kr (mod N) of
+// exp(-2 pi i kr.t_g / N)| > 1e-5.
+static bool spectral_alive(const std::vector<SymOp>& ops, const std::vector<SymOp>& rec, const int* kr, const int* n,
+                           int dim) {
+  double sr = 0.0, si = 0.0;
+  for (size_t g = 0; g < rec.size(); ++g) {
+    bool stab = true;
+    for (int d = 0; d < 3 && stab; ++d) {
+      long s = 0;
+      for (int j = 0; j < 3; ++j) s += rec[g].R[d][j] * kr[j];
+      if ((s - kr[d]) % n[d] != 0) stab = false;
+    }
+    if (!stab) continue;
+    double phase = 0.0;
+    for (int d = 0; d < dim; ++d) phase += static_cast<double>(kr[d]) * ops[g].t[d] / n[d];
+    sr += std::cos(2.0 * M_PI * phase);
+    si -= std::sin(2.0 * M_PI * phase);
+  }
+  return std::hypot(sr, si) > 1e-5;
+}
+
+// Representatives of a closed point group without a visited array: k (column-major
+// index lin) is the smallest member of its orbit {R k} exactly when no rotation maps it
+// to a smaller index, which most points fail after one or two rotations.  The test is
+// arithmetic only, so it runs on host threads over ranges of lin; the orbit size (the
+// number of distinct images) and the extinction filter are evaluated at representatives.
+static std::vector<SpecPoint> spectral_asu_closed(const std::vector<SymOp>& ops, const std::vector<SymOp>& rec,
+                                                  const std::vector<SymOp>& rots, const int* n, int dim) {
+  const long total = static_cast<long>(n[0]) * n[1] * n[2];
+  std::vector<std::array<int, 9>> R;
+  for (const auto& r : rots) {
+    if (is_identity_R(r)) continue;
+    std::array<int, 9> a{};
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) a[3 * i + j] = r.R[i][j];
+    R.push_back(a);
+  }
+  // Rotation entries of crystallographic groups are small, so an image coordinate lies
+  // within a few multiples of N of [0, N) and is wrapped by adding or subtracting N.
+  int amax = 0;
+  for (const auto& a : R)
+    for (int v : a) amax = std::max(amax, std::abs(v));
+  const bool small = amax <= 2;
+  auto image = [&](const std::array<int, 9>& a, const int* k) {
+    long li = 0, stride = 1;
+    for (int d = 0; d < 3; ++d) {
+      long s = static_cast<long>(a[3 * d]) * k[0] + static_cast<long>(a[3 * d + 1]) * k[1] +
+               static_cast<long>(a[3 * d + 2]) * k[2];
+      if (small) {
+        while (s < 0) s += n[d];
+        while (s >= n[d]) s -= n[d];
+      } else {
+        s = floor_mod(s, n[d]);
+      }
+      li += s * stride;
+      stride *= n[d];
+    }
+    return li;
+  };
+  const long nthreads = std::max(1L, std::min<long>(std::min(16u, std::max(1u, std::thread::hardware_concurrency())),
+                                                    total / 65536));
+  std::vector<std::vector<SpecPoint>> part(nthreads);
+  auto work = [&](long t) {
+    const long l0 = total * t / nthreads, l1 = total * (t + 1) / nthreads;
+    std::vector<long> imgs;
+    // Move-to-front: the rotation that rejected the previous point is tried first, since
+    // neighbouring points are usually rejected by the same one.
+    std::vector<int> order(R.size());
+    std::iota(order.begin(), order.end(), 0);
+    for (long lin = l0; lin < l1; ++lin) {
+      const int k[3] = {static_cast<int>(lin % n[0]), static_cast<int>((lin / n[0]) % n[1]),
+                        static_cast<int>(lin / (static_cast<long>(n[0]) * n[1]))};
+      bool rep = true;
+      for (size_t i = 0; i < order.size(); ++i)
+        if (image(R[order[i]], k) < lin) {
+          rep = false;
+          if (i) std::swap(order[0], order[i]);
+          break;
+        }
+      if (!rep) continue;
+      imgs.assign(1, lin);
+      for (const auto& a : R) imgs.push_back(image(a, k));
+      std::sort(imgs.begin(), imgs.end());
+      const int mult = static_cast<int>(std::unique(imgs.begin(), imgs.end()) - imgs.begin());
+      if (!spectral_alive(ops, rec, k, n, dim)) continue;
+      SpecPoint p;
+      p.h[0] = k[0]; p.h[1] = k[1]; p.h[2] = k[2];
+      p.mult = mult;
+      part[t].push_back(p);
+    }
+  };
+  std::vector<std::thread> pool;
+  for (long t = 1; t < nthreads; ++t) pool.emplace_back(work, t);
+  work(0);
+  for (auto& th : pool) th.join();
+  std::vector<SpecPoint> pts;
+  for (auto& v : part) pts.insert(pts.end(), v.begin(), v.end());
+  return pts;
+}
+
 // calc_spectral_asu (src/spectral_indexing.jl:22-176): orbit representatives of the
 // dual point group (smallest column-major index), with the stabiliser-phase
 // extinction filter, sorted lexicographically by (h1, h2, h3).
 //
 // The reference grows each orbit by a closure walk that applies every operation to
 // every member, O(N^3 |G|).  When the distinct dual rotations form a group (always,
-// for a space group's operations) the walk is replaced by one pass of the distinct
-// rotations over the first unvisited index: scanning in increasing order, that index
-// is the smallest member of its orbit (a smaller member would have marked the whole
-// orbit already), and the orbit is {R k}.  The result is identical and the cost is
-// about N^3.  Operation lists that are not closed keep the closure walk.
+// for a space group's operations) the representatives are found directly
+// (spectral_asu_closed); the result is identical.  Operation lists that are not closed
+// keep the closure walk.  The last result is kept per host thread, so the query and the
+// fill call of the C ABI and the plan build on the same operations compute it once.
 std::vector<SpecPoint> calc_spectral_asu(const std::vector<SymOp>& ops, const int* N, int dim) {
   const int n[3] = {N[0], dim > 1 ? N[1] : 1, dim > 2 ? N[2] : 1};
+  thread_local std::vector<long> cache_key;
+  thread_local std::vector<SpecPoint> cache_pts;
+  std::vector<long> key{dim, n[0], n[1], n[2]};
+  for (const auto& op : ops) {
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) key.push_back(op.R[i][j]);
+    for (int i = 0; i < 3; ++i) key.push_back(op.t[i]);
+  }
+  if (key == cache_key) return cache_pts;
   const long total = static_cast<long>(n[0]) * n[1] * n[2];
   const std::vector<SymOp> rec = dual_ops(ops);
   const std::vector<SymOp> rots = distinct_rotations(rec);
-  const bool closed = rotations_form_group(rots);
-  std::vector<char> visited(total, 0);
   std::vector<SpecPoint> pts;
-  std::vector<long> work;
-  for (long lin = 0; lin < total; ++lin) {
-    if (visited[lin]) continue;
-    visited[lin] = 1;
-    int orbit = 1;
-    long min_lin = lin;
-    if (closed) {
-      int kk[3];
-      long r2 = lin;
-      kk[0] = static_cast<int>(r2 % n[0]); r2 /= n[0]; kk[1] = static_cast<int>(r2 % n[1]); kk[2] = static_cast<int>(r2 / n[1]);
-      for (const auto& op : rots) {
-        long li = 0, stride = 1;
-        for (int d = 0; d < 3; ++d) {
-          long s = 0;
-          for (int j = 0; j < 3; ++j) s += op.R[d][j] * kk[j];
-          li += floor_mod(s, n[d]) * stride;
-          stride *= n[d];
-        }
-        if (!visited[li]) {
-          visited[li] = 1;
-          ++orbit;
-        }
-      }
-    } else {
+  if (rotations_form_group(rots)) {
+    pts = spectral_asu_closed(ops, rec, rots, n, dim);
+  } else {
+    std::vector<char> visited(total, 0);
+    std::vector<long> work;
+    for (long lin = 0; lin < total; ++lin) {
+      if (visited[lin]) continue;
+      visited[lin] = 1;
+      int orbit = 1;
+      long min_lin = lin;
       work.clear();
       work.push_back(lin);
       for (size_t w = 0; w < work.size(); ++w) {
@@ -335,26 +429,10 @@ std::vector<SpecPoint> calc_spectral_asu(const std::vector<SymOp>& ops, const in
           }
         }
       }
-    }
-    int kr[3];
-    long rem = min_lin;
-    kr[0] = rem % n[0]; rem /= n[0]; kr[1] = rem % n[1]; kr[2] = rem / n[1];
-    // Extinction filter: |sum_{g in Stab(k)} exp(-2 pi i k.t_g / N)| > 1e-5.
-    double sr = 0.0, si = 0.0;
-    for (size_t g = 0; g < rec.size(); ++g) {
-      bool stab = true;
-      for (int d = 0; d < 3 && stab; ++d) {
-        long s = 0;
-        for (int j = 0; j < 3; ++j) s += rec[g].R[d][j] * kr[j];
-        if ((s - kr[d]) % n[d] != 0) stab = false;
-      }
-      if (!stab) continue;
-      double phase = 0.0;
-      for (int d = 0; d < dim; ++d) phase += static_cast<double>(kr[d]) * ops[g].t[d] / n[d];
-      sr += std::cos(2.0 * M_PI * phase);
-      si -= std::sin(2.0 * M_PI * phase);
-    }
-    if (std::hypot(sr, si) > 1e-5) {
+      int kr[3];
+      long rem = min_lin;
+      kr[0] = rem % n[0]; rem /= n[0]; kr[1] = rem % n[1]; kr[2] = rem / n[1];
+      if (!spectral_alive(ops, rec, kr, n, dim)) continue;
       SpecPoint p;
       p.h[0] = kr[0]; p.h[1] = kr[1]; p.h[2] = kr[2];
       p.mult = orbit;
@@ -366,6 +444,8 @@ std::vector<SpecPoint> calc_spectral_asu(const std::vector<SymOp>& ops, const in
     if (a.h[1] != b.h[1]) return a.h[1] < b.h[1];
     return a.h[2] < b.h[2];
   });
+  cache_key.swap(key);
+  cache_pts = pts;
   return pts;
 }
 
@@ -527,11 +607,13 @@ Status build_tables(const std::vector<SymOp>& shifted_ops, const int* N_in, int 
     T->offsets[0] = {0, 0, 0};
   }
 
-  // ---- reverse lookup over the full grid (src/krfft.jl:1183-1255) ----
+  // ---- reverse lookup (src/krfft.jl:1183-1255) ----
+  // For a full-grid frequency key, the entry of _build_spectral_reverse_lookup: the
+  // spectral point s whose orbit holds the key (direct) or its negative (conjugate),
+  // with the symmetry phase, the first writer winning in the reference's order (for
+  // each s: itself, then per operation j its image R_j^T h_s and the negative, then -h_s).
   const long n1 = N[0], n2 = N[1], n3 = N[2];
   const long total = n1 * n2 * n3;
-  std::vector<int32_t> rs(total, 0), rp(total, 0);
-  std::vector<char> rc(total, 0);
   auto lin = [&](long a, long b, long c) { return a + n1 * (b + n2 * c); };
   auto phase_num = [&](const int* h, const int* t) {
     long j = 0;
@@ -539,26 +621,108 @@ Status build_tables(const std::vector<SymOp>& shifted_ops, const int* N_in, int 
     return static_cast<int32_t>(floor_mod(j, P));
   };
   const int nspec = static_cast<int>(T->spec.size());
-  for (int s = 0; s < nspec; ++s) {
-    const int* h = T->spec[s].h;
-    long key = lin(h[0], h[1], h[2]);
-    if (!rs[key]) { rs[key] = s + 1; rp[key] = 0; rc[key] = 0; }
-    for (const auto& op : T->ops) {
-      long hr[3];
-      for (int d = 0; d < 3; ++d) {
-        long v = 0;
-        for (int d2 = 0; d2 < 3; ++d2) v += static_cast<long>(op.R[d2][d]) * h[d2];
-        hr[d] = floor_mod(v, N[d]);
+  const std::vector<SymOp> rev_rots = distinct_rotations(dual_ops(T->ops));
+  const bool rev_closed = rotations_form_group(rev_rots);
+  // Non-closed operation lists: the reference's dense table over the full grid.
+  std::vector<int32_t> rs, rp;
+  std::vector<char> rc;
+  if (!rev_closed) {
+    rs.assign(total, 0);
+    rp.assign(total, 0);
+    rc.assign(total, 0);
+    for (int s = 0; s < nspec; ++s) {
+      const int* h = T->spec[s].h;
+      long key = lin(h[0], h[1], h[2]);
+      if (!rs[key]) { rs[key] = s + 1; rp[key] = 0; rc[key] = 0; }
+      for (const auto& op : T->ops) {
+        long hr[3];
+        for (int d = 0; d < 3; ++d) {
+          long v = 0;
+          for (int d2 = 0; d2 < 3; ++d2) v += static_cast<long>(op.R[d2][d]) * h[d2];
+          hr[d] = floor_mod(v, N[d]);
+        }
+        const int32_t ph = phase_num(h, op.t);
+        key = lin(hr[0], hr[1], hr[2]);
+        if (!rs[key]) { rs[key] = s + 1; rp[key] = ph; rc[key] = 0; }
+        key = lin(floor_mod(-hr[0], n1), floor_mod(-hr[1], n2), floor_mod(-hr[2], n3));
+        if (!rs[key]) { rs[key] = s + 1; rp[key] = static_cast<int32_t>(floor_mod(-static_cast<long>(ph), P)); rc[key] = 1; }
       }
-      const int32_t ph = phase_num(h, op.t);
-      key = lin(hr[0], hr[1], hr[2]);
-      if (!rs[key]) { rs[key] = s + 1; rp[key] = ph; rc[key] = 0; }
-      key = lin(floor_mod(-hr[0], n1), floor_mod(-hr[1], n2), floor_mod(-hr[2], n3));
-      if (!rs[key]) { rs[key] = s + 1; rp[key] = static_cast<int32_t>(floor_mod(-static_cast<long>(ph), P)); rc[key] = 1; }
+      key = lin(floor_mod(-h[0], n1), floor_mod(-h[1], n2), floor_mod(-h[2], n3));
+      if (!rs[key]) { rs[key] = s + 1; rp[key] = 0; rc[key] = 1; }
     }
-    key = lin(floor_mod(-h[0], n1), floor_mod(-h[1], n2), floor_mod(-h[2], n3));
-    if (!rs[key]) { rs[key] = s + 1; rp[key] = 0; rc[key] = 1; }
   }
+  // Closed groups: each queried key is answered directly.  The spectral points are the
+  // smallest members of their orbits, so the candidates are s_d = the point at the
+  // orbit minimum of k (a direct entry) and s_c = that of -k (a conjugate entry); the
+  // smaller s wins, and within one s the first operation in list order.
+  std::unordered_map<long, int> spec_at;
+  if (rev_closed) {
+    spec_at.reserve(2 * static_cast<size_t>(nspec) + 1);
+    for (int s = 0; s < nspec; ++s) spec_at[lin(T->spec[s].h[0], T->spec[s].h[1], T->spec[s].h[2])] = s;
+  }
+  auto orbit_min = [&](const long* k) {
+    long best = LONG_MAX;
+    for (const auto& r : rev_rots) {
+      long v[3];
+      for (int d = 0; d < 3; ++d) {
+        long x = 0;
+        for (int j = 0; j < 3; ++j) x += static_cast<long>(r.R[d][j]) * k[j];
+        v[d] = floor_mod(x, N[d]);
+      }
+      best = std::min(best, lin(v[0], v[1], v[2]));
+    }
+    return best;
+  };
+  // (signed spectral index + 1 as in the dense table: 0 = absent, < 0 conjugate; phase)
+  auto lookup = [&](const long* k, int32_t* sgn, int32_t* ph) {
+    if (!rev_closed) {
+      const long key = lin(k[0], k[1], k[2]);
+      *sgn = rs[key] ? (rc[key] ? -rs[key] : rs[key]) : 0;
+      *ph = rs[key] ? rp[key] : 0;
+      return;
+    }
+    const long nk[3] = {floor_mod(-k[0], n1), floor_mod(-k[1], n2), floor_mod(-k[2], n3)};
+    auto find = [&](long key) {
+      auto it = spec_at.find(key);
+      return it == spec_at.end() ? -1 : it->second;
+    };
+    const int sd = find(orbit_min(k)), sc = find(orbit_min(nk));
+    if (sd < 0 && sc < 0) { *sgn = 0; *ph = 0; return; }
+    const long big = 4L * static_cast<long>(T->ops.size()) + 8;
+    // order of the first direct write of k by sd, and of the first conjugate write by sc
+    auto first_write = [&](int s, bool conj, int32_t* phase) -> long {
+      const int* h = T->spec[s].h;
+      if (!conj && h[0] == k[0] && h[1] == k[1] && h[2] == k[2]) { *phase = 0; return -1; }
+      for (size_t j = 0; j < T->ops.size(); ++j) {
+        const auto& op = T->ops[j];
+        long hr[3];
+        for (int d = 0; d < 3; ++d) {
+          long v = 0;
+          for (int d2 = 0; d2 < 3; ++d2) v += static_cast<long>(op.R[d2][d]) * h[d2];
+          hr[d] = floor_mod(conj ? -v : v, N[d]);
+        }
+        if (hr[0] == k[0] && hr[1] == k[1] && hr[2] == k[2]) {
+          const int32_t p0 = phase_num(h, op.t);
+          *phase = conj ? static_cast<int32_t>(floor_mod(-static_cast<long>(p0), P)) : p0;
+          return 2 * static_cast<long>(j) + (conj ? 1 : 0);
+        }
+      }
+      if (conj && floor_mod(-h[0], n1) == k[0] && floor_mod(-h[1], n2) == k[1] && floor_mod(-h[2], n3) == k[2]) {
+        *phase = 0;
+        return 2 * static_cast<long>(T->ops.size());
+      }
+      *phase = 0;
+      return big;  // not written by s (does not happen for a closed group)
+    };
+    int32_t pd = 0, pc = 0;
+    const long od = sd >= 0 ? first_write(sd, false, &pd) : big;
+    const long oc = sc >= 0 ? first_write(sc, true, &pc) : big;
+    const bool take_d = sd >= 0 && od < big && (sc < 0 || oc >= big || sd < sc || (sd == sc && od < oc));
+    if (take_d) { *sgn = sd + 1; *ph = pd; return; }
+    if (sc >= 0 && oc < big) { *sgn = -(sc + 1); *ph = pc; return; }
+    *sgn = 0;
+    *ph = 0;
+  };
 
   // ---- orbit structure on the M-grid under the even-translation subgroup ----
   // (src/centering_fold.jl:643-687, generalised to any L by s = t / L)
@@ -605,22 +769,35 @@ Status build_tables(const std::vector<SymOp>& shifted_ops, const int* N_in, int 
     seen[m] = 1;
     if (!alive) continue;
     T->orbit_rep.push_back(static_cast<int32_t>(m));
-    // d aliases h_a = q + M .* alpha_a, alpha enumerated with the first axis fastest.
-    for (int a = 0; a < d; ++a) {
-      int alpha[3];
-      int rem = a;
-      for (int dd = 0; dd < 3; ++dd) { alpha[dd] = rem % L[dd]; rem /= L[dd]; }
-      long hk[3];
-      for (int dd = 0; dd < 3; ++dd) hk[dd] = floor_mod(q[dd] + static_cast<long>(M[dd]) * alpha[dd], N[dd]);
-      const long key = lin(hk[0], hk[1], hk[2]);
-      if (rs[key]) {
-        T->inv_spec.push_back(rc[key] ? -rs[key] : rs[key]);
-        T->inv_phase.push_back(rp[key]);
-      } else {
-        T->inv_spec.push_back(0);
-        T->inv_phase.push_back(0);
+  }
+  // d aliases h_a = q + M .* alpha_a per representative, alpha with the first axis
+  // fastest; the lookups are independent and run on host threads.
+  const long n_orb_all = static_cast<long>(T->orbit_rep.size());
+  T->inv_spec.assign(static_cast<size_t>(n_orb_all) * d, 0);
+  T->inv_phase.assign(static_cast<size_t>(n_orb_all) * d, 0);
+  auto fill = [&](long o0, long o1) {
+    for (long o = o0; o < o1; ++o) {
+      long rr = T->orbit_rep[o];
+      long q[3];
+      q[0] = rr % M[0]; rr /= M[0]; q[1] = rr % M[1]; q[2] = rr / M[1];
+      for (int a = 0; a < d; ++a) {
+        int alpha[3];
+        int rem = a;
+        for (int dd = 0; dd < 3; ++dd) { alpha[dd] = rem % L[dd]; rem /= L[dd]; }
+        long hk[3];
+        for (int dd = 0; dd < 3; ++dd) hk[dd] = floor_mod(q[dd] + static_cast<long>(M[dd]) * alpha[dd], N[dd]);
+        lookup(hk, &T->inv_spec[o * d + a], &T->inv_phase[o * d + a]);
       }
     }
+  };
+  const long nth = rev_closed ? std::max(1L, std::min<long>(std::min(16u, std::max(1u, std::thread::hardware_concurrency())),
+                                                            n_orb_all / 2048))
+                              : 1;
+  {
+    std::vector<std::thread> pool;
+    for (long t = 1; t < nth; ++t) pool.emplace_back(fill, n_orb_all * t / nth, n_orb_all * (t + 1) / nth);
+    fill(0, n_orb_all / nth);
+    for (auto& th : pool) th.join();
   }
   // Order the representatives by the spectral index of their first alias so that
   // neighbouring device threads gather neighbouring spectrum entries.

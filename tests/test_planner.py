@@ -292,3 +292,30 @@ def test_centering_enum_and_convert_op(cf):
     for sg in (2, 70, 167, 227, 230):
         for o in cf.get_ops(sg, 3, (24, 24, 24)):
             assert cf.convert_op(o.Rm, [v / 24 for v in o.t], (24, 24, 24)) == o
+
+
+def test_backward_tables_all_groups_vs_oracle(cf, O):
+    # The plan's backward lookup (_build_spectral_reverse_lookup / _build_inv_recon_table!,
+    # src/krfft.jl:997-1255) for every space group at 12^3: per orbit representative and
+    # alias, the signed spectral index and the phase of the oracle's M2 inverse table.
+    # The library answers each lookup from the orbit minima of k and -k with the
+    # reference's first-writer order; the oracle builds the reference's dense table.
+    N = (12, 12, 12)
+    for sg in range(1, 231):
+        oops = O.find_optimal_shift(O.get_ops(sg, 3, N), N)[1]
+        ops_s = [cf.SymOp(op.R, op.t) for op in oops]
+        spec = cf.calc_spectral_asu(ops_s, 3, N)
+        plan = cf.KRFFTPlan(spec, ops_s, precision=8, device=False)
+        reps, s_tab, p_tab = plan.backward_tables()
+        ospec = O.calc_spectral_asu(oops, 3, N)
+        ob = O.plan_m2_backward(ospec, oops)
+        P = plan.info.P
+        for o, q in enumerate(reps):
+            for a in range(ob.d):
+                s = int(s_tab[o, a])
+                if s == 0:
+                    assert ob.inv_spec[a, q] < 0, (sg, o, a)
+                    continue
+                assert ob.inv_spec[a, q] == abs(s) - 1 and bool(ob.inv_conj[a, q]) == (s < 0), (sg, o, a)
+                assert abs(np.exp(2j * np.pi * p_tab[o, a] / P) / ob.d - ob.inv_w[a, q]) < 1e-12, (sg, o, a)
+        plan.close()
