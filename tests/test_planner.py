@@ -319,3 +319,27 @@ def test_backward_tables_all_groups_vs_oracle(cf, O):
                 assert ob.inv_spec[a, q] == abs(s) - 1 and bool(ob.inv_conj[a, q]) == (s < 0), (sg, o, a)
                 assert abs(np.exp(2j * np.pi * p_tab[o, a] / P) / ob.d - ob.inv_w[a, q]) < 1e-12, (sg, o, a)
         plan.close()
+
+
+@pytest.mark.parametrize("sg,n", [(229, 128), (230, 96), (47, 64), (221, 64), (227, 64)])
+def test_backward_tables_bench_sizes_vs_oracle(cf, O, sg, n):
+    # the backward tables the device path uses at the bench and SCFT sizes (Im-3m 128^3,
+    # Ia-3d 96^3, Pmmm / Pm-3m / Fd-3m 64^3), entry by entry against the oracle's dense
+    # M2 inverse table
+    N = (n, n, n)
+    oops = O.find_optimal_shift(O.get_ops(sg, 3, N), N)[1]
+    ops_s = [cf.SymOp(op.R, op.t) for op in oops]
+    spec = cf.calc_spectral_asu(ops_s, 3, N)
+    plan = cf.KRFFTPlan(spec, ops_s, precision=4, device=False)
+    reps, s_tab, p_tab = plan.backward_tables()
+    ob = O.plan_m2_backward(O.calc_spectral_asu(oops, 3, N), oops)
+    reps = np.asarray(reps)
+    s = np.asarray(s_tab)
+    os_, oc, ow = ob.inv_spec[:, reps].T, ob.inv_conj[:, reps].T, ob.inv_w[:, reps].T
+    assert np.all(os_[s == 0] < 0)
+    pres = s != 0
+    assert np.array_equal(os_[pres], np.abs(s[pres]) - 1)
+    assert np.array_equal(oc[pres].astype(bool), s[pres] < 0)
+    w = np.exp(2j * np.pi * np.asarray(p_tab) / plan.info.P) / ob.d
+    assert np.max(np.abs(w[pres] - ow[pres])) < 1e-12
+    plan.close()
