@@ -343,3 +343,32 @@ def test_backward_tables_bench_sizes_vs_oracle(cf, O, sg, n):
     w = np.exp(2j * np.pi * np.asarray(p_tab) / plan.info.P) / ob.d
     assert np.max(np.abs(w[pres] - ow[pres])) < 1e-12
     plan.close()
+
+
+def test_concurrent_plan_builds_match_serial(cf):
+    # Plans built from several host threads at once (as the warm-start data solves do)
+    # get the same tables as serial builds: the planner's per-thread ASU cache and its own
+    # worker threads do not mix results between callers.
+    import threading
+
+    cases = [(229, 32), (230, 48), (221, 32), (227, 32), (47, 32), (225, 32)]
+
+    def tables(sg, n):
+        N = (n, n, n)
+        _, ops_s = cf.find_optimal_shift(cf.get_ops(sg, 3, N), N)
+        spec = cf.calc_spectral_asu(ops_s, 3, N)
+        p = cf.KRFFTPlan(spec, ops_s, precision=4, device=False)
+        r = (np.asarray(spec.idx).copy(), *[np.asarray(x).copy() for x in p.backward_tables()])
+        p.close()
+        return r
+
+    serial = [tables(*c) for c in cases]
+    for _ in range(2):
+        res = [None] * len(cases)
+        ths = [threading.Thread(target=lambda i=i: res.__setitem__(i, tables(*cases[i]))) for i in range(len(cases))]
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        for got, want in zip(res, serial):
+            assert all(np.array_equal(a, b) for a, b in zip(got, want))
