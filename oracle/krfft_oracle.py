@@ -13,8 +13,10 @@ test/test_q_fused.jl), and (b) against the integer pins those tests hold
 (ASU sizes, centering classes, fold metadata, stripped op counts, auto-L).
 Its space-group operations come from its own Hall-symbol table (hall_groups.py),
 pinned to the reference's Crystalline-derived mirror/centring table
-(src/mirror_table.jl, tests/golden/mirror_table.json) and to the ITA group
-orders; nothing here loads the library under test.
+(src/mirror_table.jl, tests/golden/mirror_table.json), to the ITA group orders, and
+to the reference's own recursive-tree survey output (test/debug_tree_output.log,
+tests/golden/tree_survey_64.json, reproduced through fractal_tree.py for its 163
+groups); nothing here loads the library under test.
 
 Layout conventions follow the reference: grids are indexed [x, y, z] with x
 fastest in memory (Julia column-major == numpy order='F'); the oracle stores
