@@ -97,6 +97,10 @@ def _load():
         "cfft_update_kernel": (c_int, [c_void_p, ctypes.c_double, c_double_p]),
         "cfft_forward": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
         "cfft_backward": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+        "cfft_forward_plans": (c_int, [c_int, ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p),
+                                       ctypes.POINTER(c_void_p), ctypes.POINTER(c_int), c_void_p]),
+        "cfft_backward_plans": (c_int, [c_int, ctypes.POINTER(c_void_p), ctypes.POINTER(c_void_p),
+                                        ctypes.POINTER(c_void_p), ctypes.POINTER(c_int), c_void_p]),
         "cfft_scft_step": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
         "cfft_step_diffusion": (c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_double, c_int, c_int, c_void_p]),
         "cfft_fullgrid_to_subgrid": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),

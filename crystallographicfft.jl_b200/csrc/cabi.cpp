@@ -546,6 +546,32 @@ cfft_status cfft_backward(cfft_plan plan, const void* F, void* f0, int batch, vo
 cfft_status cfft_scft_step(cfft_plan plan, void* f0, int batch, void* stream) {
   CFFT_EXEC(cfft::exec_scft_step(p, f0, batch, stream, &err));
 }
+
+cfft_status cfft_forward_plans(int n_plans, const cfft_plan* plans, const void* const* f0, void* const* F,
+                               const int* batch, void* stream) {
+  if (n_plans < 1 || !plans || !f0 || !F || !batch) return ret(Status::kInvalid, "invalid plan array arguments");
+  for (int i = 0; i < n_plans; ++i) {
+    const cfft_status st = cfft_forward(plans[i], f0[i], F[i], batch[i], stream);
+    if (st != CFFT_OK) {
+      g_last_error = "plan " + std::to_string(i) + ": " + g_last_error;
+      return st;
+    }
+  }
+  return CFFT_OK;
+}
+
+cfft_status cfft_backward_plans(int n_plans, const cfft_plan* plans, const void* const* F, void* const* f0,
+                                const int* batch, void* stream) {
+  if (n_plans < 1 || !plans || !F || !f0 || !batch) return ret(Status::kInvalid, "invalid plan array arguments");
+  for (int i = 0; i < n_plans; ++i) {
+    const cfft_status st = cfft_backward(plans[i], F[i], f0[i], batch[i], stream);
+    if (st != CFFT_OK) {
+      g_last_error = "plan " + std::to_string(i) + ": " + g_last_error;
+      return st;
+    }
+  }
+  return CFFT_OK;
+}
 cfft_status cfft_step_diffusion(cfft_plan plan, void* q, const void* w, double dt, int n_steps, int batch,
                                 void* stream) {
   CFFT_EXEC(cfft::exec_step_diffusion(p, q, w, dt, n_steps, batch, stream, &err));

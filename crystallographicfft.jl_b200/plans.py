@@ -313,6 +313,39 @@ class KRFFTPlan:
 # ---------------------------------------------------------------------------
 
 
+def _plan_array_call(fn, plans, ins, outs, in_kind, out_kind, per):
+    n = len(plans)
+    if n < 1 or len(ins) != n or len(outs) != n:
+        raise CFFTError(1, "plans, inputs and outputs must be lists of the same non-zero length")
+    batch = []
+    for p, x, y in zip(plans, ins, outs):
+        p._check_tensor(x, in_kind)
+        p._check_tensor(y, out_kind)
+        batch.append(p._batch_of(x, per(p)))
+    hs = (ctypes.c_void_p * n)(*[p.handle.value for p in plans])
+    xs = (ctypes.c_void_p * n)(*[x.data_ptr() for x in ins])
+    ys = (ctypes.c_void_p * n)(*[y.data_ptr() for y in outs])
+    bs = (ctypes.c_int * n)(*batch)
+    check(fn(n, hs, xs, ys, bs, KRFFTPlan._stream()))
+    return outs
+
+
+def forward_plans(plans, fields, out=None):
+    """The forward transforms of several plans in one library call (cfft_forward_plans):
+    plans[i] on the CUDA tensor fields[i] (its subgrid batch), in list order on torch's
+    current stream.  Returns the spectra (new tensors unless `out` is given)."""
+    outs = list(out) if out is not None else [p._new_spec_tensor(p._batch_of(x, p.mvol), x)
+                                              for p, x in zip(plans, fields)]
+    return _plan_array_call(LIB.cfft_forward_plans, list(plans), list(fields), outs, "r", "c", lambda p: p.mvol)
+
+
+def backward_plans(plans, spectra, out=None):
+    """The backward transforms of several plans in one library call (cfft_backward_plans)."""
+    outs = list(out) if out is not None else [p._new_field_tensor(p._batch_of(F, p.n_spec), F)
+                                              for p, F in zip(plans, spectra)]
+    return _plan_array_call(LIB.cfft_backward_plans, list(plans), list(spectra), outs, "c", "r", lambda p: p.n_spec)
+
+
 def plan_krfft(spec, ops_shifted, *, precision=8, max_batch=1):
     """plan_krfft(spec, ops_shifted) auto-L variant (src/krfft.jl:301-389)."""
     return KRFFTPlan(spec, ops_shifted, precision=precision, max_batch=max_batch, path=PATH_M2)

@@ -222,6 +222,16 @@ cfft_status cfft_forward(cfft_plan plan, const void* f0, void* F, int batch, voi
  * src/krfft.jl:1269-1277): F -> f0 (real part). */
 cfft_status cfft_backward(cfft_plan plan, const void* F, void* f0, int batch, void* stream);
 
+/* Batched forms over an array of plans (no reference counterpart: a caller of the
+ * reference runs its plans one call each): plan i runs cfft_forward (cfft_backward) on
+ * batch[i] fields from f0[i] into F[i] (F[i] into f0[i]), the plans in array order on
+ * the one stream.  Each call is the single-plan call; the first failing plan stops the
+ * loop, and its status is returned with "plan i: " before its message. */
+cfft_status cfft_forward_plans(int n_plans, const cfft_plan* plans, const void* const* f0, void* const* F,
+                               const int* batch, void* stream);
+cfft_status cfft_backward_plans(int n_plans, const cfft_plan* plans, const void* const* F, void* const* f0,
+                                const int* batch, void* stream);
+
 /* execute_centered_scft! / execute_m2_scft! (src/centering_fold.jl:908-931,
  * src/q_fused_krfft.jl:989-1026): f0 <- IKRFFT(K . KRFFT(f0)), in place. */
 cfft_status cfft_scft_step(cfft_plan plan, void* f0, int batch, void* stream);

@@ -60,3 +60,26 @@ def test_fractal_tree_invalid_arguments(cf):
     assert lib.cfft_fractal_tree(3, N, 1, Rp, tp, 0, 0, ctypes.byref(n), ctypes.byref(inner), op) == 1  # cap 0
     assert lib.cfft_fractal_tree(3, N, 1, Rp, tp, 0, 1, ctypes.byref(n), ctypes.byref(inner), op) == 0
     assert list(out) == [8, 8, 8, 1, 1, 1, 0, 0, 0, 0]
+
+
+def test_plan_array_entry_points_validate_and_report(cf):
+    # cfft_forward_plans / cfft_backward_plans: argument checks, and the first failing
+    # plan's status with its index (host-only plans have no device state)
+    import numpy as np
+
+    lib = cf.LIB
+    N = (16, 16, 16)
+    _, ops_s = cf.find_optimal_shift(cf.get_ops(229, 3, N), N)
+    spec = cf.calc_spectral_asu(ops_s, 3, N)
+    plans = [cf.KRFFTPlan(spec, ops_s, precision=4, device=False) for _ in range(2)]
+    hs = (ctypes.c_void_p * 2)(*[p.handle.value for p in plans])
+    bufs = (ctypes.c_void_p * 2)(None, None)
+    batch = (ctypes.c_int * 2)(1, 1)
+    for fn in (lib.cfft_forward_plans, lib.cfft_backward_plans):
+        assert fn(0, hs, bufs, bufs, batch, None) == 1
+        assert fn(2, None, bufs, bufs, batch, None) == 1
+        assert fn(2, hs, bufs, bufs, None, None) == 1
+        assert fn(2, hs, bufs, bufs, batch, None) == 1
+        assert lib.cfft_last_error().startswith(b"plan 0: ")
+    for p in plans:
+        p.close()
