@@ -228,3 +228,28 @@ def test_m2_backward_roundtrip(prep, O, sg):
     f0 = O.pack_stride(p["u"], O.auto_L(p["oops"]))
     back = O.execute_m2_backward(bwd, O.fft_reconstruct(fwd, f0))
     assert np.max(np.abs(np.real(back).reshape(f0.shape, order="F") - f0)) < 1e-10
+
+
+def test_oracle_forward_and_roundtrip_all_groups(O):
+    # The oracle's own transforms for every space group at 12^3 (its table's operations,
+    # shifted by find_optimal_shift): the forward against numpy's full FFT on the spectral
+    # ASU (test/runtests.jl:199-216) and the backward round trip to the subgrid
+    # (test/test_m2_backward.jl, test/test_centered_backward.jl), each < 1e-9
+    N = (12, 12, 12)
+    bad = []
+    for sg in range(1, 231):
+        oops = O.find_optimal_shift(O.get_ops(sg, 3, N), N)[1]
+        spec = O.calc_spectral_asu(oops, 3, N)
+        u = O.make_symmetric(oops, N, seed=sg)
+        fwd = O.plan_krfft_centered(spec, oops)
+        if isinstance(fwd, O.CenteredPlan):
+            F = O.execute_centered_krfft(fwd, u)
+            f0 = O.pack_stride(u, [2, 2, 2])
+            back = O.execute_centered_ikrfft(O.plan_centered_ikrfft(spec, oops, fwd), F)
+        else:
+            F = O.execute_krfft(fwd, u)
+            f0 = O.pack_stride(u, O.auto_L(oops))
+            back = np.real(O.execute_m2_backward(O.plan_m2_backward(spec, oops), F)).reshape(f0.shape, order="F")
+        if np.max(np.abs(F - O.spectrum_on_asu(u, spec))) > 1e-9 or np.max(np.abs(back - f0)) > 1e-9:
+            bad.append(sg)
+    assert not bad, bad
