@@ -14,7 +14,7 @@ from .symmetry import (  # noqa: F401
     needs_dct_path,
 )
 from .plans import (  # noqa: F401
-    forward_plans, backward_plans,
+    forward_plans, backward_plans, plan_centering_fold, SubgridCenteringFoldPlan,
     DiffusionSolver, KRFFTPlan, PATH_AUTO, PATH_CENTERED, PATH_M2, PATH_M2Q, PATH_M7, execute_centered_ikrfft,
     execute_centered_krfft, execute_m2_q, execute_m7_scft, plan_m2_q, plan_m7_scft, PATH_FULLGRID,
     Diagonal, apply_diffusion_operator, calc_gradient_term, calc_matrix_q,

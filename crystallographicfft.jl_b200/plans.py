@@ -18,6 +18,7 @@ Array conventions
 from __future__ import annotations
 
 import ctypes
+from dataclasses import dataclass
 
 import numpy as np
 
@@ -311,6 +312,45 @@ class KRFFTPlan:
 # ---------------------------------------------------------------------------
 # Reference-named constructors and execute functions
 # ---------------------------------------------------------------------------
+
+
+# Alive parity offsets of the centring fold, in the reference's order (_alive_offsets,
+# src/centering_fold.jl:111-127); the plane kernels fold the channels in this order.
+_ALIVE_OFFSETS = {"I": [(0, 0, 0), (1, 1, 0), (1, 0, 1), (0, 1, 1)], "F": [(0, 0, 0), (1, 1, 1)],
+                  "C": [(0, 0, 0), (1, 1, 0), (0, 0, 1), (1, 1, 1)], "A": [(0, 0, 0), (0, 1, 1), (1, 0, 0), (1, 1, 1)]}
+
+
+@dataclass
+class SubgridCenteringFoldPlan:
+    """SubgridCenteringFoldPlan (src/centering_fold.jl:41-53): the fold's geometry.  The
+    channel buffers and FFT plans of the reference have no counterpart: the fold, the
+    channel FFTs and G0 assembly run fused in the library's plane kernels."""
+
+    centering: str
+    M: tuple
+    H: tuple
+    n_channels: int
+    offsets: list       # alive parity offsets per channel
+    twiddle_1d: list    # per channel, per dimension: e^{-2 pi i off_d n / M_d}, n < H_d
+    sign_table: list    # per channel, 8 signs (-1)^{off . e}, e = (ex, ey, ez), ex fastest
+
+
+def plan_centering_fold(centering, M):
+    """plan_centering_fold (src/centering_fold.jl:60-104) for centring I, F, C or A (a
+    string or a CenteringType) on a stride-2 subgrid M with even edges."""
+    c = getattr(centering, "value", centering)
+    if c not in _ALIVE_OFFSETS:
+        raise CFFTError(1, f"Centering fold not applicable for {c}")
+    M = tuple(int(m) for m in M)
+    if any(m % 2 for m in M):
+        raise CFFTError(1, "Subgrid dimensions must be even for centering fold")
+    H = tuple(m // 2 for m in M)
+    offs = _ALIVE_OFFSETS[c]
+    tw = [tuple(np.ones(H[d], dtype=np.complex128) if o[d] == 0 else
+                np.exp(-2j * np.pi * o[d] * np.arange(H[d]) / M[d]) for d in range(3)) for o in offs]
+    signs = [tuple(1 - 2 * ((o[0] * (i & 1) + o[1] * ((i >> 1) & 1) + o[2] * ((i >> 2) & 1)) & 1) for i in range(8))
+             for o in offs]
+    return SubgridCenteringFoldPlan(c, M, H, len(offs), list(offs), tw, signs)
 
 
 def _plan_array_call(fn, plans, ins, outs, in_kind, out_kind, per):

@@ -372,3 +372,25 @@ def test_concurrent_plan_builds_match_serial(cf):
             t.join()
         for got, want in zip(res, serial):
             assert all(np.array_equal(a, b) for a, b in zip(got, want))
+
+
+def test_plan_centering_fold_metadata(cf, O):
+    # plan_centering_fold (src/centering_fold.jl:60-104): test/test_centering_fold.jl:32-54
+    # pins the channel counts; offsets, twiddles and signs against the oracle's fold
+    for c, n_ch in (("F", 2), ("I", 4), ("C", 4), ("A", 4)):
+        M = (32, 24, 16)
+        p = cf.plan_centering_fold(c, M)
+        o = O.plan_centering_fold(c, M)
+        assert p.n_channels == n_ch == o.n_channels and p.H == o.H == (16, 12, 8)
+        assert p.offsets == o.offsets
+        for k, off in enumerate(p.offsets):
+            t = p.twiddle_1d[k]
+            full = t[0][:, None, None] * t[1][None, :, None] * t[2][None, None, :]
+            assert np.allclose(full, O._fold_twiddle(o, off), atol=1e-15)
+            assert p.sign_table[k] == tuple((-1) ** (off[0] * (i & 1) + off[1] * ((i >> 1) & 1) + off[2] * ((i >> 2) & 1))
+                                            for i in range(8))
+    assert cf.plan_centering_fold(cf.CentI, (8, 8, 8)).n_channels == 4
+    with pytest.raises(cf.CFFTError):
+        cf.plan_centering_fold("P", (8, 8, 8))
+    with pytest.raises(cf.CFFTError):
+        cf.plan_centering_fold("I", (8, 7, 8))
