@@ -54,16 +54,19 @@ def load_package():
     return mod
 
 
-# Sources of the transform path (plan tables, scheduling, kernels); the SCFT driver, the
-# warm-start network, the space-group table and the C ABI wrappers do not change its traffic.
+# What a DRAM-traffic figure measured by ncu depends on: the device side of the transform
+# path (kernels, launch scheduling, the table layouts they read) and the tables the plan
+# layer hands it for the measured plan.  The first is keyed by these sources; the plan
+# layer (planner.cpp) enters through the hash of the measured plan's tables instead, so
+# a faster planner that builds the same tables keeps the figure.  The SCFT driver, the
+# warm-start network, the space-group table and the C ABI wrappers do not change it.
 TRANSFORM_SOURCES = ("cfft_internal.h", "device_common.cuh", "exec.cu", "exec.h", "fast_api.h", "fast_kernels.cuh",
                      "fast_other_f32.cu", "fast_other_f64.cu", "fast_planes_f32.cu", "fast_planes_f64.cu",
-                     "planner.cpp", "tma_planes.cuh")
+                     "tma_planes.cuh")
 
 
 def kernel_source_sha():
-    """Hash of the transform path's native sources; a DRAM-traffic figure measured by ncu
-    applies to the build it was measured on only."""
+    """Hash of the transform path's device-side sources."""
     import hashlib
 
     h = hashlib.sha256()
@@ -71,6 +74,22 @@ def kernel_source_sha():
     for name in TRANSFORM_SOURCES:
         h.update(name.encode())
         h.update(open(os.path.join(csrc, name), "rb").read())
+    return h.hexdigest()[:16]
+
+
+def plan_table_sha(plan):
+    """Hash of the host tables a plan's kernels read: its geometry, spectral ASU,
+    representative operations and backward orbit tables."""
+    import hashlib
+
+    h = hashlib.sha256()
+    for v in (plan.L, plan.M, plan.H, (plan.n_spec, plan.n_channels, plan.info.n_rep, plan.info.P)):
+        h.update(np.asarray(v, dtype=np.int64).tobytes())
+    idx, mult = plan.spectral_asu()
+    for a in (idx, mult, *plan.backward_tables()):
+        h.update(np.ascontiguousarray(np.asarray(a, dtype=np.int64)).tobytes())
+    for op in plan.rep_ops():
+        h.update(np.asarray(op.R, dtype=np.int64).tobytes() + np.asarray(op.t, dtype=np.int64).tobytes())
     return h.hexdigest()[:16]
 
 
@@ -529,10 +548,12 @@ def run_ours(args):
     # of the native sources); null when the sources changed since the capture.
     traffic_file = os.path.join(ROOT, "profiles", "traffic_im3m128.json")
     line["roofline"]["kernel_source_sha"] = kernel_source_sha()
+    line["roofline"]["plan_table_sha"] = plan_table_sha(plan)
     if os.path.exists(traffic_file):
         try:
             tr = json.load(open(traffic_file))
-            if tr.get("kernel_source_sha") == line["roofline"]["kernel_source_sha"]:
+            if (tr.get("kernel_source_sha") == line["roofline"]["kernel_source_sha"]
+                    and tr.get("plan_table_sha") == line["roofline"]["plan_table_sha"]):
                 line["roofline"]["traffic"] = tr.get("bytes_per_field", 0) * B
                 line["roofline"]["traffic_note"] = tr.get("note")
             else:

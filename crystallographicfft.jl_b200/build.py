@@ -28,7 +28,8 @@ NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-rela
 HOST_SOURCES = ["spacegroups.cpp", "planner.cpp", "cabi.cpp"]
 # The fast-path kernels are split by stage group and precision so nvcc runs in parallel.
 DEVICE_SOURCES = ["exec.cu", "scft.cu", "sno.cu", "fast_planes_f32.cu", "fast_planes_f64.cu", "fast_other_f32.cu", "fast_other_f64.cu"]
-HEADERS = ["cfft_internal.h", "exec.h", "device_common.cuh", "fast_api.h", "fast_kernels.cuh", "tma_planes.cuh", "scft.h", "sno.h"]
+HEADERS = ["cfft_internal.h", "exec.h", "device_common.cuh", "fast_api.h", "fast_kernels.cuh", "tma_planes.cuh", "scft.h", "sno.h",
+           "fractal_tree.h"]
 
 
 def _newer(src_paths, target):

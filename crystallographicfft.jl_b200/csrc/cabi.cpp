@@ -9,6 +9,7 @@
 #include "fast_api.h"
 #include "scft.h"
 #include "sno.h"
+#include "fractal_tree.h"
 
 using cfft::Status;
 

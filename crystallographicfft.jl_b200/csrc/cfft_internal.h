@@ -101,16 +101,6 @@ struct AsuPoint {
   int mult;      // orbit size at the leaf
 };
 std::vector<AsuPoint> calc_asu(const std::vector<SymOp>& ops, const int* N, int dim);
-
-// A leaf of the fractal KRFFT's recursive parity tree: its grid, and the stride and
-// offset at which it samples the full grid.
-struct TreeLeaf {
-  int n[3], scale[3], offset[3], depth;
-};
-// build_recursive_tree + collect_leaves (src/fractal_krfft.jl:300-636).  flags bit 0:
-// child translations from the half-grid-shifted operations; bit 1: no centring split.
-void fractal_tree(const std::vector<SymOp>& ops, const int* N, int dim, int flags, std::vector<TreeLeaf>* leaves,
-                  int* n_inner);
 Status build_q_tables(const PlanTables& T, const double* lattice, double ds, std::vector<double>* Q,
                       std::vector<int32_t>* gather, std::string* err);
 

@@ -15,6 +15,7 @@
 #include <unordered_map>
 
 #include "cfft_internal.h"
+#include "fractal_tree.h"
 
 namespace cfft {
 
