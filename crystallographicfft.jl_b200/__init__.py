@@ -44,4 +44,4 @@ from .scft import SCFTSolver, initial_fields, plan_scft  # noqa: F401
 from .batch import MultiPlanStep, autotune_path, autotune_plan  # noqa: F401
 from .sno import GROUP_SLOTS, SNOContext, SpectralNeuralOperator  # noqa: F401
 
-__version__ = "0.2.0"
+__version__ = "0.3.0"

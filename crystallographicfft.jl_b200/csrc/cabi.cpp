@@ -623,7 +623,7 @@ const char* cfft_status_string(cfft_status s) {
 
 const char* cfft_last_error(void) { return g_last_error.c_str(); }
 
-int cfft_version(void) { return 100; }
+int cfft_version(void) { return 110; }
 
 int64_t cfft_launch_count(int reset) { return cfft::launch_count(reset != 0); }
 
