@@ -4,6 +4,8 @@ import ctypes
 import os
 import re
 
+import pytest
+
 from conftest import PKG_DIR, ROOT
 
 
@@ -81,5 +83,35 @@ def test_plan_array_entry_points_validate_and_report(cf):
         assert fn(2, hs, bufs, bufs, None, None) == 1
         assert fn(2, hs, bufs, bufs, batch, None) == 1
         assert lib.cfft_last_error().startswith(b"plan 0: ")
+    for p in plans:
+        p.close()
+
+
+def test_plan_array_python_wrappers_reach_the_library(cf, monkeypatch):
+    # forward_plans / backward_plans build their argument arrays and output tensors and
+    # call the library; with host-only plans (and the CUDA-tensor check lifted for CPU
+    # tensors) the call reaches cfft_forward_plans and returns plan 0's error
+    import torch
+
+    monkeypatch.setattr(cf.KRFFTPlan, "_check_tensor", lambda self, x, kind: None)
+    monkeypatch.setattr(cf.KRFFTPlan, "_stream", staticmethod(lambda: ctypes.c_void_p(None)))
+    plans, fields = [], []
+    for sg, n, prec, B in ((229, 16, 4, 3), (47, 16, 8, 1)):
+        N = (n, n, n)
+        _, ops_s = cf.find_optimal_shift(cf.get_ops(sg, 3, N), N)
+        spec = cf.calc_spectral_asu(ops_s, 3, N)
+        p = cf.KRFFTPlan(spec, ops_s, precision=prec, device=False)
+        plans.append(p)
+        dt = torch.float32 if prec == 4 else torch.float64
+        fields.append(torch.zeros(((B,) if B > 1 else ()) + tuple(reversed(p.M)), dtype=dt))
+    with pytest.raises(cf.CFFTError) as e:
+        cf.forward_plans(plans, fields)
+    assert "plan 0: " in str(e.value)
+    spectra = [torch.zeros((3, plans[0].n_spec), dtype=torch.complex64), torch.zeros(plans[1].n_spec, dtype=torch.complex128)]
+    with pytest.raises(cf.CFFTError) as e:
+        cf.backward_plans(plans, spectra)
+    assert "plan 0: " in str(e.value)
+    with pytest.raises(cf.CFFTError):
+        cf.forward_plans(plans, fields[:1])
     for p in plans:
         p.close()
