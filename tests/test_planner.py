@@ -394,3 +394,58 @@ def test_plan_centering_fold_metadata(cf, O):
         cf.plan_centering_fold("P", (8, 8, 8))
     with pytest.raises(cf.CFFTError):
         cf.plan_centering_fold("I", (8, 7, 8))
+
+
+def test_planner_on_random_subgroups_vs_oracle(cf, O):
+    # Closed groups outside the standard tables: subgroups generated by two operations of
+    # a random space group (seeded), shifted and planned; spectral ASU and backward tables
+    # against the oracle's (its dense first-writer table) at 12^3.
+    import random
+
+    rng = random.Random(7)
+    N = (12, 12, 12)
+    ident = O.SymOp((1, 0, 0, 0, 1, 0, 0, 0, 1), (0, 0, 0))
+
+    def compose(a, b):
+        Ra, Rb = np.array(a.R).reshape(3, 3), np.array(b.R).reshape(3, 3)
+        t = (Ra @ np.array(b.t) + np.array(a.t)) % 12
+        return O.SymOp(tuple(int(v) for v in (Ra @ Rb).ravel()), tuple(int(v) for v in t))
+
+    def closure(gens):
+        grp, frontier = {(ident.R, ident.t): ident}, [ident]
+        while frontier:
+            nxt = []
+            for a in frontier:
+                for b in gens:
+                    c = compose(a, b)
+                    if (c.R, c.t) not in grp:
+                        grp[(c.R, c.t)] = c
+                        nxt.append(c)
+            frontier = nxt
+        return sorted(grp.values(), key=lambda o: (o.R != ident.R, o.R, o.t))
+
+    checked = 0
+    for _ in range(40):
+        full = O.get_ops(rng.randint(1, 230), 3, N)
+        ops = closure(rng.sample(full, min(2, len(full))))
+        _, oops = O.find_optimal_shift(ops, N)
+        ops_s = [cf.SymOp(op.R, op.t) for op in oops]
+        spec = cf.calc_spectral_asu(ops_s, 3, N)
+        ospec = O.calc_spectral_asu(oops, 3, N)
+        assert np.array_equal(spec.idx, ospec.idx) and np.array_equal(spec.mult, ospec.mult)
+        try:
+            plan = cf.KRFFTPlan(spec, ops_s, precision=8, device=False)
+        except cf.CFFTError:
+            continue  # e.g. no representative for some parity class at this grid
+        reps, s_tab, p_tab = plan.backward_tables()
+        ob = O.plan_m2_backward(ospec, oops)
+        reps, s = np.asarray(reps), np.asarray(s_tab)
+        os_, oc, ow = ob.inv_spec[:, reps].T, ob.inv_conj[:, reps].T, ob.inv_w[:, reps].T
+        assert np.all(os_[s == 0] < 0)
+        pres = s != 0
+        assert np.array_equal(os_[pres], np.abs(s[pres]) - 1) and np.array_equal(oc[pres].astype(bool), s[pres] < 0)
+        w = np.exp(2j * np.pi * np.asarray(p_tab) / plan.info.P) / ob.d
+        assert np.max(np.abs(w[pres] - ow[pres]), initial=0.0) < 1e-12
+        plan.close()
+        checked += 1
+    assert checked >= 30
